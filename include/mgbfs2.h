@@ -1,0 +1,212 @@
+/*
+ * libmgbfs2 — C ABI of the B200-native exact BFS engine for implicit Cayley and
+ * permutation graphs.
+ *
+ * Conventions (kept from the reference's C ABI, cuda/mgbfs_cuda.h:10-19):
+ *   - every function returns int: 0 = success (or enqueued), a small positive
+ *     MGBFS2_* code, or MGBFS2_CUDA_BASE + cudaError_t;
+ *   - create functions take (char* error, size_t error_capacity) for a message;
+ *   - kernel-level entry points take caller-owned device pointers and a
+ *     `void* stream` (cudaStream_t, NULL = legacy default stream) and allocate
+ *     nothing; device-side failures land in a sticky uint32 error word
+ *     (reference: cuda/generic_visited.h:19);
+ *   - a graph handle is single-threaded: one caller at a time.
+ *
+ * Every entry point cites the reference interface it replaces.  Paths are
+ * relative to the TryDotAtwo/MultiGPUBFS tree.
+ */
+#ifndef MGBFS2_H
+#define MGBFS2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MGBFS2_API __attribute__((visibility("default")))
+#else
+#define MGBFS2_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  MGBFS2_OK = 0,
+  MGBFS2_INVALID_ARGUMENT = 1,
+  MGBFS2_UNSUPPORTED = 2,
+  MGBFS2_OUT_OF_MEMORY = 3,
+  MGBFS2_CAPACITY = 4,
+  MGBFS2_DEVICE_STATUS = 5,
+  MGBFS2_STATE = 6,
+  MGBFS2_NOT_FOUND = 7,
+  MGBFS2_CUDA_BASE = 1000
+};
+
+/* Graph description: the lossless schema-2 contract of
+ * multigpubfs/graph_definition.py:17-69 as plain arrays. */
+typedef struct {
+  uint32_t kind;                 /* 0 = permutation, 1 = int64 matrix */
+  uint32_t elements;             /* state length: degree, or rows * cols */
+  uint32_t rows, cols;           /* matrix shape; permutation: rows = degree, cols = 1 */
+  uint32_t generators;
+  const uint32_t* permutations;  /* generators x elements; child[i] = state[g[i]] */
+  const int64_t* matrices;       /* generators x rows x rows, row-major */
+  const uint32_t* moduli;        /* generators; 0 = plain int64 wrap, else 2..2^31 */
+  const int64_t* start;          /* elements */
+  uint64_t orbit_bound;          /* expected_max_unique_states, 0 = none */
+} mgbfs2_graph_desc;
+
+enum { MGBFS2_VISITED_AUTO = 0, MGBFS2_VISITED_BITMAP = 1, MGBFS2_VISITED_HASH = 2, MGBFS2_VISITED_HASH3 = 3 };
+enum { MGBFS2_DEDUP_AUTO = 0, MGBFS2_DEDUP_ATOMIC = 1, MGBFS2_DEDUP_WARP = 2, MGBFS2_DEDUP_SORT = 3,
+       MGBFS2_DEDUP_BUCKET = 4 };
+enum { MGBFS2_PLANNER_PLAIN = 0, MGBFS2_PLANNER_LEARNED = 1 };
+
+typedef struct {
+  uint32_t visited;        /* MGBFS2_VISITED_* */
+  uint32_t dedup;          /* MGBFS2_DEDUP_* */
+  uint64_t capacity;       /* max states per frontier, 0 = from the state bound */
+  uint64_t reserve_bytes;  /* device bytes never planned, 0 = 2 GiB */
+  uint32_t shards;         /* bucket shards for MGBFS2_DEDUP_BUCKET, 0 = 64 */
+  uint32_t block;          /* threads per block, 0 = tuned */
+  uint32_t planner;        /* MGBFS2_PLANNER_* */
+  uint32_t reserved;
+} mgbfs2_plan_request;
+
+typedef struct {
+  uint32_t visited, dedup;
+  uint32_t packed;          /* 1 = states are one packed uint64 word */
+  uint32_t bits_per_symbol; /* packed symbol width */
+  uint32_t key_words;       /* uint64 words per state */
+  uint32_t history_layers;  /* 1 = all visited retained, 3 = three-layer banks */
+  uint64_t capacity;        /* frontier capacity bound (states) */
+  uint64_t table_slots;     /* hash slots (all-visited table) */
+  uint64_t bitmap_bits;     /* rank-domain size of the bitmap */
+  uint64_t device_bytes;    /* fixed device allocation of the plan */
+  uint64_t state_bound;     /* certified orbit bound, 0 = unknown */
+  uint32_t shards, block;
+  uint32_t inverse_closed;
+  uint32_t planner;
+} mgbfs2_plan_info;
+
+typedef struct {
+  double max_seconds;          /* 0 = no deadline */
+  uint32_t max_layers;         /* 0 = no limit */
+  uint32_t reserved;
+  const volatile int32_t* cancel; /* optional; non-zero stops before the next layer */
+} mgbfs2_run_limits;
+
+enum { MGBFS2_REASON_FRONTIER_EXHAUSTED = 0, MGBFS2_REASON_DEADLINE = 1, MGBFS2_REASON_CANCELLED = 2,
+       MGBFS2_REASON_RESOURCE = 3, MGBFS2_REASON_LAYER_LIMIT = 4 };
+
+typedef struct {
+  uint32_t complete;     /* 1 = frontier exhausted */
+  uint32_t reason;       /* MGBFS2_REASON_* */
+  uint32_t fatal;        /* device ERR_* bits when reason = RESOURCE */
+  uint32_t layers;       /* entries in the layer table (depth 0 included) */
+  uint64_t states;       /* sum of layer sizes */
+  uint64_t successors;   /* successors generated */
+  double bfs_seconds;
+  uint32_t redo_layers;  /* layers recomputed after an exact overflow */
+  uint32_t kernel_launches;
+  uint64_t peak_device_bytes;
+  double device_seconds; /* CUDA-event time of the whole run on the engine stream */
+  double kernel_seconds; /* CUDA-event time summed over the layer-expansion kernels */
+} mgbfs2_status;
+
+/* Per-layer callback; return non-zero to stop (reason CANCELLED). */
+typedef int (*mgbfs2_layer_callback)(void* user, uint32_t depth, uint64_t size, double seconds);
+
+typedef struct mgbfs2_graph mgbfs2_graph;
+
+/* Replaces the `mgbfs graph` engine set-up: GenericNativeBfs::new,
+ * crates/mgbfs-runtime/src/generic_native.rs:69-98 (validation of
+ * graph_definition.py:46-69 included). */
+MGBFS2_API int mgbfs2_graph_create(const mgbfs2_graph_desc* desc, int device, mgbfs2_graph** out, char* error,
+                        size_t error_capacity);
+
+/* Replaces the plain planner GenericMemoryPlan::{with_storage, automatic_storage},
+ * crates/mgbfs-runtime/src/generic_memory.rs:36-49, and the `graph-info` admission
+ * verb, crates/mgbfs-cli/src/main.rs:54-84. */
+MGBFS2_API int mgbfs2_plan(mgbfs2_graph* graph, const mgbfs2_plan_request* request, mgbfs2_plan_info* plan);
+
+/* Replaces the layer loop of generic_run::run, crates/mgbfs-runtime/src/generic_run.rs:25-34,
+ * with GenericNativeBfs::advance, generic_native.rs:106-126 (one scalar readback per layer). */
+MGBFS2_API int mgbfs2_run(mgbfs2_graph* graph, const mgbfs2_run_limits* limits, mgbfs2_layer_callback callback,
+               void* user, mgbfs2_status* status);
+
+/* layer_sizes / layer_seconds of report.json, generic_run.rs:39. */
+MGBFS2_API int mgbfs2_layer_table(const mgbfs2_graph* graph, uint64_t* sizes, double* seconds, size_t capacity,
+                       size_t* count);
+
+/* states.json samples, generic_native.rs:129-144: which = 0 -> the deepest layer
+ * ("current", up to capacity_rows rows), which = 1 -> the layer before it when
+ * it holds fewer than 1000 states ("previous_small").  Rows are int64 labels,
+ * row-major, elements per row. */
+MGBFS2_API int mgbfs2_sample(mgbfs2_graph* graph, uint32_t which, int64_t* out, size_t capacity_rows, size_t* rows);
+
+/* Static message for a status code (reference: native_fault.rs error markers). */
+MGBFS2_API const char* mgbfs2_status_string(int code);
+
+MGBFS2_API void mgbfs2_destroy(mgbfs2_graph* graph);
+
+/* ------------------------------------------------------------------------ */
+/* Kernel-level entry points (caller-owned device buffers, no allocation).    */
+
+/* All successors of `count` parents: children[(p * generators + g) * elements + e].
+ * Parents and children are row-major int64 states.  Replaces
+ * mgbfs_generic_generate_i64 (cuda/generic_graph.h, kernel cuda/generic_graph.cu:7-36),
+ * whose planes are element-major; the int64 matrix action wraps before `% modulo`
+ * exactly as graph_definition.py:77-83. */
+MGBFS2_API int mgbfs2_successors_i64(uint32_t kind, uint32_t elements, uint32_t rows, uint32_t cols, uint32_t generators,
+                          const int64_t* parents, uint64_t count, const uint32_t* permutations,
+                          const int64_t* matrices, const uint32_t* moduli, int64_t* children,
+                          uint32_t* error, void* stream);
+
+/* Packed successors of one-word states (4/8/16/32-bit symbols):
+ * children[p * generators + g].  Device form of the packed transitions of
+ * scripts/cpu_small_bfs.py:21-27 for arbitrary permutation generators. */
+MGBFS2_API int mgbfs2_successors_packed(uint32_t degree, uint32_t bits, uint32_t generators, const uint32_t* permutations_host,
+                             const uint64_t* parents, uint64_t count, uint64_t* children, void* stream);
+
+/* Exact lexicographic multiset rank of packed states.  counts_host[c] is the
+ * multiplicity of symbol code c (distinct codes, sum = degree).  Replaces the
+ * device contract bitmap_rank_component, cuda/permutation_bitmap.cuh:23-49.
+ * Invalid states get rank UINT64_MAX and set *error bit 4 (rank range). */
+MGBFS2_API int mgbfs2_rank_packed(uint32_t degree, uint32_t bits, uint32_t distinct, const uint32_t* counts_host,
+                       const uint64_t* words, uint64_t count, uint64_t* ranks, uint32_t* error, void* stream);
+
+/* Test-and-set claim of ranks in a bitmap of `domain` bits; won[i] = 1 for
+ * exactly one occurrence of every rank not set before.  warp = 1 merges bits of
+ * a warp that share a word into one atomicOr.  Replaces bitmap_accept /
+ * bitmap_accept_grouped, cuda/permutation_bitmap.cu:105-205. */
+MGBFS2_API int mgbfs2_bitmap_claim(const uint64_t* ranks, uint64_t count, uint64_t* bitmap, uint64_t domain, uint8_t* won,
+                        uint32_t warp, uint32_t* error, void* stream);
+
+/* Exact-key insertion of packed keys into an open-addressing table of `slots`
+ * (power of two, initialised to all-ones); inserted[i] = 1 for exactly one
+ * occurrence of each key that was absent.  Replaces accept_candidates,
+ * cuda/generic_visited.cu:18-58 (single-word keys). */
+MGBFS2_API int mgbfs2_hash_insert(const uint64_t* keys, uint64_t count, uint64_t* table, uint64_t slots, uint8_t* inserted,
+                       uint32_t* error, void* stream);
+
+/* Tile-local sort-unique: each tile of `tile` keys (<= 4096, power of two) is
+ * radix-sorted in shared memory and its distinct keys are written, sorted, to
+ * out[tile_index * tile ...]; counts[tile_index] = distinct keys of that tile.
+ * Replaces the CUB sort + unique stage of cuda/permutation_bitmap_batch.cu:48-160
+ * and cuda/segmented_hash_batch.cu:53-190 (here per tile, in shared memory). */
+MGBFS2_API int mgbfs2_sort_unique_tiles(const uint64_t* keys, uint64_t count, uint32_t tile, uint32_t key_bits,
+                             uint64_t* out, uint32_t* counts, void* stream);
+
+/* Owner routing inside one GPU: key k goes to shard (k >> shift) (< shards);
+ * buckets is shards x capacity; counts[s] = keys routed to s (exact, may exceed
+ * capacity, which sets error bit 3).  Replaces route / bitmap_route,
+ * cuda/generic_route.cu:7-37 and cuda/permutation_bitmap.cu:27-48. */
+MGBFS2_API int mgbfs2_bucket_keys(const uint64_t* keys, uint64_t count, uint32_t shift, uint32_t shards, uint64_t* buckets,
+                       uint64_t capacity, unsigned long long* counts, uint32_t* error, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGBFS2_H */

@@ -1,0 +1,821 @@
+// Host engine of libmgbfs2: graph validation and packing, the plain planner,
+// the level-synchronous layer loop and the graph-level C ABI.
+//
+// Reference counterparts (TryDotAtwo/MultiGPUBFS):
+//   graph validation      multigpubfs/graph_definition.py:46-69
+//   state-space bound     crates/mgbfs-runtime/src/generic_memory.rs:82-108
+//   Coxeter certificate   multigpubfs/workload_geometry.py:2-19
+//   layer loop            crates/mgbfs-runtime/src/generic_run.rs:25-34,
+//                         crates/mgbfs-runtime/src/generic_native.rs:106-126
+//   three-layer banks     crates/mgbfs-runtime/src/generic_distributed_native.rs:166-179,
+//                         cuda/generic_rolling.cuh:3-47
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/mgbfs2.h"
+#include "engine.h"
+#include "packed_kernels.cuh"
+
+namespace mgbfs2 {
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? MGBFS2_OK : MGBFS2_CUDA_BASE + static_cast<int>(e); }
+
+#define MG_CHECK(expr)                         \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) return cuda_status(_e); \
+  } while (0)
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+void set_message(char* error, size_t capacity, const std::string& text) {
+  if (!error || !capacity) return;
+  std::snprintf(error, capacity, "%s", text.c_str());
+}
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// n! / prod(c!) with saturation at UINT64_MAX.
+uint64_t multinomial(const std::vector<uint32_t>& counts) {
+  unsigned __int128 ways = 1;
+  uint64_t placed = 0;
+  for (uint32_t c : counts) {
+    for (uint32_t k = 1; k <= c; ++k) {
+      ways = ways * (placed + k) / k;
+      if (ways > static_cast<unsigned __int128>(UINT64_MAX)) return UINT64_MAX;
+    }
+    placed += c;
+  }
+  return static_cast<uint64_t>(ways);
+}
+
+uint64_t sat_mul(uint64_t a, uint64_t b) {
+  unsigned __int128 r = static_cast<unsigned __int128>(a) * b;
+  return r > UINT64_MAX ? UINT64_MAX : static_cast<uint64_t>(r);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Graph construction and validation.
+
+int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error, size_t cap) {
+  if (!d || !out) {
+    set_message(error, cap, "GRAPH_ARGUMENT");
+    return MGBFS2_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  auto fail = [&](const char* msg) {
+    set_message(error, cap, msg);
+    return MGBFS2_INVALID_ARGUMENT;
+  };
+  if (d->kind > 1) return fail("GRAPH_ACTION_KIND");
+  if (!d->generators || !d->start || d->elements == 0) return fail("GRAPH_GENERATORS");
+  auto g = new Graph();
+  g->device = dev;
+  g->kind = d->kind;
+  g->elements = d->elements;
+  g->gens = d->generators;
+  g->start.assign(d->start, d->start + d->elements);
+  g->orbit_bound = d->orbit_bound;
+  if (d->kind == 0) {
+    if (!d->permutations) { delete g; return fail("GRAPH_PERMUTATION_GENERATOR"); }
+    g->rows = d->elements;
+    g->cols = 1;
+    g->perms.assign(d->permutations, d->permutations + static_cast<size_t>(d->generators) * d->elements);
+    std::vector<uint8_t> seen(d->elements);
+    for (uint32_t k = 0; k < d->generators; ++k) {
+      std::fill(seen.begin(), seen.end(), 0);
+      for (uint32_t i = 0; i < d->elements; ++i) {
+        const uint32_t v = g->perms[static_cast<size_t>(k) * d->elements + i];
+        if (v >= d->elements || seen[v]) { delete g; return fail("GRAPH_PERMUTATION_GENERATOR"); }
+        seen[v] = 1;
+      }
+    }
+  } else {
+    if (!d->matrices || !d->moduli || d->rows == 0 || d->cols == 0 ||
+        static_cast<uint64_t>(d->rows) * d->cols != d->elements) {
+      delete g;
+      return fail("GRAPH_MATRIX_SHAPE");
+    }
+    g->rows = d->rows;
+    g->cols = d->cols;
+    g->matrices.assign(d->matrices, d->matrices + static_cast<size_t>(d->generators) * d->rows * d->rows);
+    g->moduli.assign(d->moduli, d->moduli + d->generators);
+    for (uint32_t m : g->moduli)
+      if (m != 0 && (m < 2 || m > (1u << 31))) { delete g; return fail("GRAPH_MATRIX_MODULUS"); }
+  }
+  int rc = cuda_status(cudaSetDevice(dev));
+  if (rc) { set_message(error, cap, "CUDA_SET_DEVICE"); delete g; return rc; }
+  rc = cuda_status(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  if (rc) { set_message(error, cap, "CUDA_STREAM"); delete g; return rc; }
+  for (cudaEvent_t* e : {&g->ev_run[0], &g->ev_run[1], &g->ev_kernel[0], &g->ev_kernel[1]}) {
+    rc = cuda_status(cudaEventCreate(e));
+    if (rc) { set_message(error, cap, "CUDA_EVENT"); delete g; return rc; }
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) g->sm_count = prop.multiProcessorCount;
+  g->analyse();
+  *out = g;
+  return MGBFS2_OK;
+}
+
+// Packing, inverse closure, rank domain, state bound and Coxeter certificate.
+void Graph::analyse() {
+  const uint32_t n = elements;
+  inverse_closed = false;
+  if (kind == 0) {
+    // Dense codes: i-th smallest distinct label -> i.
+    labels = start;
+    std::sort(labels.begin(), labels.end());
+    labels.erase(std::unique(labels.begin(), labels.end()), labels.end());
+    distinct = static_cast<uint32_t>(labels.size());
+    codes.resize(n);
+    for (uint32_t i = 0; i < n; ++i)
+      codes[i] = static_cast<uint32_t>(std::lower_bound(labels.begin(), labels.end(), start[i]) - labels.begin());
+    bits = 4;
+    while (bits < 32 && (1ull << bits) < distinct) bits *= 2;
+    packed = static_cast<uint64_t>(n) * bits <= 64;
+    if (packed) {
+      start_word = 0;
+      for (uint32_t i = 0; i < n; ++i) start_word |= static_cast<uint64_t>(codes[i]) << (bits * i);
+      key_mask = (n * bits == 64) ? ~0ull : ((1ull << (n * bits)) - 1);
+    }
+    code_counts.assign(distinct, 0);
+    for (uint32_t c : codes) code_counts[c]++;
+    // Inverse closure (graph_definition.py:84-92).
+    std::map<std::vector<uint32_t>, int> available;
+    for (uint32_t k = 0; k < gens; ++k)
+      available[std::vector<uint32_t>(perms.begin() + static_cast<size_t>(k) * n,
+                                      perms.begin() + static_cast<size_t>(k + 1) * n)] = 1;
+    inverse_closed = true;
+    for (uint32_t k = 0; k < gens && inverse_closed; ++k) {
+      std::vector<uint32_t> inv(n);
+      for (uint32_t i = 0; i < n; ++i) inv[perms[static_cast<size_t>(k) * n + i]] = i;
+      if (!available.count(inv)) inverse_closed = false;
+    }
+    // Rank domain of the bitmap: the multiset permutations of the start.
+    rank_total = multinomial(code_counts);
+    lehmer = packed && bits == 4 && distinct == n && n <= 16;
+    rank_ok = packed && (bits == 4 || bits == 8) && distinct <= 16 && rank_total != UINT64_MAX;
+    // State bound: positions in one cycle component of the generators keep
+    // their labels; the product of per-component multinomials bounds the
+    // orbit (generic_memory.rs:82-108).
+    std::vector<uint32_t> parent(n);
+    for (uint32_t i = 0; i < n; ++i) parent[i] = i;
+    auto root = [&](uint32_t x) {
+      while (parent[x] != x) x = parent[x] = parent[parent[x]];
+      return x;
+    };
+    for (uint32_t k = 0; k < gens; ++k)
+      for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t a = root(i), b = root(perms[static_cast<size_t>(k) * n + i]);
+        parent[a] = b;
+      }
+    std::map<uint32_t, std::map<uint32_t, uint32_t>> comp;
+    for (uint32_t i = 0; i < n; ++i) comp[root(i)][codes[i]]++;
+    state_bound = 1;
+    for (auto& c : comp) {
+      std::vector<uint32_t> counts;
+      for (auto& kv : c.second) counts.push_back(kv.second);
+      state_bound = sat_mul(state_bound, multinomial(counts));
+    }
+    if (orbit_bound) state_bound = std::min(state_bound, orbit_bound);
+    // Coxeter certificate: generators = all adjacent transpositions, distinct
+    // labels -> layer k holds the permutations with k inversions.
+    coxeter.clear();
+    if (distinct == n && gens == n - 1 && n >= 2 && n <= 32) {
+      std::vector<std::vector<uint32_t>> expected;
+      for (uint32_t i = 0; i + 1 < n; ++i) {
+        std::vector<uint32_t> p(n);
+        for (uint32_t j = 0; j < n; ++j) p[j] = j;
+        std::swap(p[i], p[i + 1]);
+        expected.push_back(p);
+      }
+      bool match = true;
+      std::vector<std::vector<uint32_t>> have;
+      for (uint32_t k = 0; k < gens; ++k)
+        have.emplace_back(perms.begin() + static_cast<size_t>(k) * n, perms.begin() + static_cast<size_t>(k + 1) * n);
+      std::sort(have.begin(), have.end());
+      std::sort(expected.begin(), expected.end());
+      match = have == expected;
+      if (match) {
+        std::vector<unsigned __int128> sizes{1};
+        for (uint32_t i = 1; i <= n; ++i) {
+          std::vector<unsigned __int128> out(sizes.size() + i - 1);
+          unsigned __int128 window = 0;
+          for (size_t j = 0; j < out.size(); ++j) {
+            if (j < sizes.size()) window += sizes[j];
+            if (j >= i) window -= sizes[j - i];
+            out[j] = window;
+          }
+          sizes.swap(out);
+        }
+        for (auto s : sizes) coxeter.push_back(s > UINT64_MAX ? UINT64_MAX : static_cast<uint64_t>(s));
+      }
+    }
+  } else {
+    packed = false;
+    state_bound = orbit_bound;
+    // Canonical same-modulus entries bound the orbit (workload_geometry.py:21-36).
+    bool same = !moduli.empty();
+    for (uint32_t m : moduli) same = same && m == moduli[0];
+    if (same && moduli[0]) {
+      bool canonical = true;
+      for (int64_t v : start) canonical = canonical && v >= 0 && v < static_cast<int64_t>(moduli[0]);
+      uint64_t b = 1;
+      for (size_t i = 0; i < start.size(); ++i) b = sat_mul(b, moduli[0]);
+      if (!canonical) b = b == UINT64_MAX ? b : b + 1;
+      state_bound = state_bound ? std::min(state_bound, b) : b;
+    }
+    inverse_closed = matrix_inverse_closed();
+  }
+  build_program();
+}
+
+// Displacement-group programs of the packed generators.
+void Graph::build_program() {
+  term_begin.assign(1, 0);
+  terms.clear();
+  if (!packed) return;
+  const uint32_t n = elements;
+  for (uint32_t k = 0; k < gens; ++k) {
+    std::map<int, uint64_t> groups;  // displacement -> mask of destination symbols
+    for (uint32_t i = 0; i < n; ++i) {
+      const int src = static_cast<int>(perms[static_cast<size_t>(k) * n + i]);
+      const uint64_t sym = (bits == 64) ? ~0ull : ((1ull << bits) - 1);
+      groups[src - static_cast<int>(i)] |= sym << (bits * i);
+    }
+    for (auto& kv : groups) {
+      Term t;
+      t.mask = kv.second;
+      const int shift = kv.first * static_cast<int>(bits);
+      t.rshift = shift > 0 ? static_cast<uint32_t>(shift) : 0u;
+      t.lshift = shift < 0 ? static_cast<uint32_t>(-shift) : 0u;
+      terms.push_back(t);
+    }
+    term_begin.push_back(static_cast<uint32_t>(terms.size()));
+  }
+}
+
+// graph_definition.py:93-108, restated over int64 with wrap-before-modulus.
+static std::vector<int64_t> mat_mul_mod(const std::vector<int64_t>& a, const std::vector<int64_t>& b, uint32_t n,
+                                        uint32_t m, uint32_t mod) {
+  std::vector<int64_t> out(static_cast<size_t>(n) * m);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t j = 0; j < m; ++j) {
+      uint64_t total = 0;
+      for (uint32_t k = 0; k < n; ++k)
+        total += static_cast<uint64_t>(a[i * n + k]) * static_cast<uint64_t>(b[static_cast<size_t>(k) * m + j]);
+      int64_t v = static_cast<int64_t>(total);
+      if (mod) {
+        v %= static_cast<int64_t>(mod);
+        if (v < 0) v += mod;
+      }
+      out[static_cast<size_t>(i) * m + j] = v;
+    }
+  return out;
+}
+
+bool Graph::matrix_inverse_closed() const {
+  const uint32_t n = rows;
+  for (uint32_t m : moduli)
+    if (m != moduli[0]) return false;
+  const uint32_t mod = moduli[0];
+  if (mod && (mod & (mod - 1))) {
+    for (uint32_t k = 0; k < gens; ++k)
+      for (uint32_t i = 0; i < n; ++i) {
+        unsigned __int128 s = 0;
+        for (uint32_t j = 0; j < n; ++j) {
+          const int64_t v = matrices[static_cast<size_t>(k) * n * n + i * n + j];
+          const unsigned __int128 a = v < 0 ? static_cast<unsigned __int128>(-(v + 1)) + 1 : v;
+          s += a * (mod - 1);
+        }
+        if (s > static_cast<unsigned __int128>(INT64_MAX)) return false;
+      }
+  }
+  std::vector<int64_t> eye(static_cast<size_t>(n) * n, 0);
+  for (uint32_t i = 0; i < n; ++i) eye[i * n + i] = 1;
+  auto gen = [&](uint32_t k) {
+    return std::vector<int64_t>(matrices.begin() + static_cast<size_t>(k) * n * n,
+                                matrices.begin() + static_cast<size_t>(k + 1) * n * n);
+  };
+  auto compose = [&](uint32_t a, uint32_t b) {
+    std::vector<int64_t> right = gen(b);
+    if (mod)
+      for (auto& v : right) {
+        v %= static_cast<int64_t>(mod);
+        if (v < 0) v += mod;
+      }
+    return mat_mul_mod(gen(a), right, n, n, mod);
+  };
+  for (uint32_t a = 0; a < gens; ++a) {
+    bool found = false;
+    for (uint32_t b = 0; b < gens && !found; ++b) found = compose(a, b) == eye && compose(b, a) == eye;
+    if (!found) return false;
+  }
+  for (uint32_t k = 0; k < gens; ++k)
+    if (moduli[k])
+      for (int64_t v : start)
+        if (v < 0 || v >= static_cast<int64_t>(moduli[k])) return false;
+  return true;
+}
+
+Graph::~Graph() {
+  release();
+  for (cudaEvent_t e : {ev_run[0], ev_run[1], ev_kernel[0], ev_kernel[1]})
+    if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Graph::release() {
+  cudaSetDevice(device);
+  for (DeviceBuffer* b : {&bitmap, &front, &next, &table, &bank[0], &bank[1], &bank[2], &program, &control_buf,
+                          &scratch})
+    b->free();
+  wide_release();
+  if (host_control) {
+    cudaFreeHost(host_control);
+    host_control = nullptr;
+  }
+}
+
+int DeviceBuffer::ensure(size_t want) {
+  if (want <= bytes) return MGBFS2_OK;
+  free();
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? MGBFS2_OUT_OF_MEMORY : cuda_status(e);
+  }
+  ptr = p;
+  bytes = want;
+  return MGBFS2_OK;
+}
+
+void DeviceBuffer::free() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Plain planner.
+
+int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
+  mgbfs2_plan_request r{};
+  if (req) r = *req;
+  if (r.visited > MGBFS2_VISITED_HASH3 || r.dedup > MGBFS2_DEDUP_BUCKET || r.planner > MGBFS2_PLANNER_LEARNED)
+    return MGBFS2_INVALID_ARGUMENT;
+  MG_CHECK(cudaSetDevice(device));
+  size_t free_bytes = 0, total_bytes = 0;
+  MG_CHECK(cudaMemGetInfo(&free_bytes, &total_bytes));
+  const uint64_t reserve = r.reserve_bytes ? r.reserve_bytes : (2ull << 30);
+  if (free_bytes <= reserve) return MGBFS2_OUT_OF_MEMORY;
+  const uint64_t budget = free_bytes - reserve;
+  mgbfs2_plan_info p{};
+  p.packed = packed;
+  p.bits_per_symbol = packed ? bits : 64;
+  p.key_words = packed ? 1 : wide_key_words();
+  p.state_bound = state_bound;
+  p.inverse_closed = inverse_closed;
+  p.planner = r.planner;
+  p.shards = r.shards ? r.shards : 64;
+  p.block = kBlock;
+  uint32_t visited = r.visited;
+  if (!packed) {
+    if (visited == MGBFS2_VISITED_BITMAP) return MGBFS2_UNSUPPORTED;
+    if (visited == MGBFS2_VISITED_AUTO) visited = inverse_closed ? MGBFS2_VISITED_HASH3 : MGBFS2_VISITED_HASH;
+  }
+  const uint64_t bitmap_bytes = rank_ok ? ((rank_total + 63) / 64) * 8 : UINT64_MAX;
+  if (visited == MGBFS2_VISITED_AUTO) {
+    // The bitmap costs total/8 bytes, an exact hash ~16 B per state: take the
+    // bitmap when it is the smaller exact structure and fits comfortably.
+    const bool dense = state_bound && rank_total / 128 <= state_bound;
+    if (rank_ok && bitmap_bytes <= budget / 2 && (dense || bitmap_bytes <= (64ull << 20)))
+      visited = MGBFS2_VISITED_BITMAP;
+    else
+      visited = inverse_closed ? MGBFS2_VISITED_HASH3 : MGBFS2_VISITED_HASH;
+  }
+  if (visited == MGBFS2_VISITED_BITMAP && !rank_ok) return MGBFS2_UNSUPPORTED;
+  if (visited == MGBFS2_VISITED_HASH3 && !inverse_closed) return MGBFS2_INVALID_ARGUMENT;
+  uint32_t dedup = r.dedup;
+  if (dedup == MGBFS2_DEDUP_AUTO) dedup = visited == MGBFS2_VISITED_BITMAP ? MGBFS2_DEDUP_WARP : MGBFS2_DEDUP_ATOMIC;
+  if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
+  if ((dedup == MGBFS2_DEDUP_SORT || dedup == MGBFS2_DEDUP_BUCKET) && !(visited == MGBFS2_VISITED_BITMAP && lehmer))
+    return MGBFS2_UNSUPPORTED;
+  p.visited = visited;
+  p.dedup = dedup;
+  p.history_layers = visited == MGBFS2_VISITED_HASH3 ? 3 : 1;
+  p.bitmap_bits = visited == MGBFS2_VISITED_BITMAP ? rank_total : 0;
+  // Frontier capacity: the orbit bound (or the caller's cap) within memory.
+  uint64_t fixed = visited == MGBFS2_VISITED_BITMAP ? bitmap_bytes : 0;
+  if (fixed >= budget) return MGBFS2_OUT_OF_MEMORY;
+  uint64_t cap = state_bound ? state_bound : UINT64_MAX;
+  if (!coxeter.empty()) cap = std::min(cap, *std::max_element(coxeter.begin(), coxeter.end()));
+  if (r.capacity) cap = std::min(cap, r.capacity);
+  const uint64_t per_state = packed ? 16 : 16ull * (wide_key_words() + 2);
+  const uint64_t hash_per_state = visited == MGBFS2_VISITED_BITMAP ? 0 : (visited == MGBFS2_VISITED_HASH3 ? 48 : 16);
+  cap = std::min(cap, (budget - fixed) / (per_state + hash_per_state));
+  if (cap == 0) return MGBFS2_OUT_OF_MEMORY;
+  p.capacity = cap;
+  if (visited == MGBFS2_VISITED_HASH) {
+    const uint64_t want = state_bound ? state_bound : cap;
+    p.table_slots = std::max<uint64_t>(1024, next_pow2(2 * std::min(want, cap)));
+  }
+  p.device_bytes = fixed + (visited == MGBFS2_VISITED_HASH ? p.table_slots * 8 : 0);
+  if (!packed) {
+    int rc = wide_plan(&p, budget);
+    if (rc) return rc;
+  }
+  // Fixed allocations of the plan.
+  int rc = MGBFS2_OK;
+  if (p.visited == MGBFS2_VISITED_BITMAP) rc = bitmap.ensure(bitmap_bytes);
+  if (!rc) rc = control_buf.ensure(sizeof(Control));
+  if (!rc && packed) rc = program.ensure(terms.size() * sizeof(Term) + term_begin.size() * sizeof(uint32_t) + 16);
+  if (!rc && !host_control) rc = cuda_status(cudaMallocHost(&host_control, sizeof(Control)));
+  if (rc) return rc;
+  if (packed) {
+    MG_CHECK(cudaMemcpyAsync(program.ptr, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, stream));
+    MG_CHECK(cudaMemcpyAsync(static_cast<char*>(program.ptr) + terms.size() * sizeof(Term), term_begin.data(),
+                             term_begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    MG_CHECK(cudaStreamSynchronize(stream));
+  }
+  plan = p;
+  planned = true;
+  if (out) *out = p;
+  return MGBFS2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Kernel selection.
+
+using ExpandFn = void (*)(ExpandParams);
+
+template <int V, bool W>
+static ExpandFn pick_lehmer(uint32_t n) {
+  switch (n) {
+#define MG_CASE(K) \
+  case K:          \
+    return expand_packed<V, K, W>;
+    MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
+    MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
+#undef MG_CASE
+    default:
+      return nullptr;
+  }
+}
+
+static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
+  switch (visit) {
+    case V_LEHMER:
+      return warp ? pick_lehmer<V_LEHMER, true>(n) : pick_lehmer<V_LEHMER, false>(n);
+    case V_MULTISET:
+      return warp ? expand_packed<V_MULTISET, 0, true> : expand_packed<V_MULTISET, 0, false>;
+    case V_HASH:
+      return expand_packed<V_HASH, 0, false>;
+    default:
+      return expand_packed<V_HASH3, 0, false>;
+  }
+}
+
+int Graph::visit_kind() const {
+  if (plan.visited == MGBFS2_VISITED_BITMAP) return (lehmer && elements >= 2) ? V_LEHMER : V_MULTISET;
+  return plan.visited == MGBFS2_VISITED_HASH ? V_HASH : V_HASH3;
+}
+
+uint32_t Graph::grid_for(const void* fn, size_t smem, uint64_t work_blocks) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const uint64_t full = static_cast<uint64_t>(per_sm) * static_cast<uint64_t>(sm_count);
+  return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(full, work_blocks)));
+}
+
+// ---------------------------------------------------------------------------
+// Layer loop.
+
+uint64_t Graph::next_bound(uint32_t depth, uint64_t count, uint64_t visited) const {
+  // Upper bound on |L_{d+1}|: every parent yields at most g new states, at
+  // most g-1 for d >= 1 on inverse-closed graphs (one edge leads back to
+  // L_{d-1}); never more than the unvisited part of the orbit bound; exact on
+  // certified Coxeter graphs.
+  const uint64_t per = (inverse_closed && depth >= 1 && gens > 1) ? gens - 1 : gens;
+  uint64_t b = sat_mul(count, per);
+  if (state_bound && state_bound >= visited) b = std::min(b, state_bound - visited);
+  if (!coxeter.empty()) b = depth + 1 < coxeter.size() ? std::min(b, coxeter[depth + 1]) : 0;
+  return b;
+}
+
+int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status) {
+  if (!planned) return MGBFS2_STATE;
+  MG_CHECK(cudaSetDevice(device));
+  if (!packed) return wide_run(limits, cb, user, status);
+  mgbfs2_status st{};
+  layer_sizes.assign(1, 1);
+  layer_seconds.clear();
+  small_layer.clear();
+  small_depth = UINT32_MAX;
+  launches = 0;
+  const auto started = Clock::now();
+  const int visit = visit_kind();
+  const bool warp = plan.dedup == MGBFS2_DEDUP_WARP;
+  ExpandFn fn = pick_expand(visit, warp, elements);
+  if (!fn) return MGBFS2_UNSUPPORTED;
+
+  ExpandParams p{};
+  p.terms = static_cast<const Term*>(program.ptr);
+  p.term_begin = reinterpret_cast<const uint32_t*>(static_cast<const char*>(program.ptr) + terms.size() * sizeof(Term));
+  p.gens = gens;
+  p.total_terms = static_cast<uint32_t>(terms.size());
+  p.control = static_cast<Control*>(control_buf.ptr);
+  p.key_mask = key_mask;
+  p.ppt = gens <= 4 ? 4 : 2;
+  const size_t smem = terms.size() * sizeof(Term) + term_begin.size() * sizeof(uint32_t);
+  if (visit == V_MULTISET) {
+    p.ms.n = elements;
+    p.ms.bits = bits;
+    p.ms.distinct = distinct;
+    p.ms.total = rank_total;
+    for (uint32_t c = 0; c < distinct && c < 16; ++c) p.ms.counts[c] = code_counts[c];
+  }
+  int rc = MGBFS2_OK;
+  double kernel_seconds = 0.0;
+  MG_CHECK(cudaEventRecord(ev_run[0], stream));
+  // Initial state: visited structure cleared, start seeded, frontier = {start}.
+  MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
+  if (visit == V_LEHMER || visit == V_MULTISET) {
+    MG_CHECK(cudaMemsetAsync(bitmap.ptr, 0, bitmap.bytes, stream));
+    p.bitmap = static_cast<unsigned long long*>(bitmap.ptr);
+  } else if (visit == V_HASH) {
+    table_slots = plan.table_slots;
+    if ((rc = table.ensure(table_slots * 8))) return rc;
+    MG_CHECK(cudaMemsetAsync(table.ptr, 0xff, table_slots * 8, stream));
+  } else {
+    for (int b = 0; b < 3; ++b) bank_slots[b] = 0;
+    bank_slots[0] = 1024;
+    if ((rc = bank[0].ensure(bank_slots[0] * 8))) return rc;
+    MG_CHECK(cudaMemsetAsync(bank[0].ptr, 0xff, bank_slots[0] * 8, stream));
+  }
+  if ((rc = front.ensure(16))) return rc;
+  MG_CHECK(cudaMemcpyAsync(front.ptr, &start_word, 8, cudaMemcpyHostToDevice, stream));
+  {
+    ExpandParams s = p;
+    if (visit == V_HASH) {
+      s.table = static_cast<unsigned long long*>(table.ptr);
+      s.table_mask = table_slots - 1;
+    } else if (visit == V_HASH3) {
+      s.table = static_cast<unsigned long long*>(bank[0].ptr);
+      s.table_mask = bank_slots[0] - 1;
+    }
+    s.probe_limit = 1u << 20;
+    seed_packed<<<1, 32, 0, stream>>>(s, start_word, visit, elements);
+    ++launches;
+    MG_CHECK(cudaGetLastError());
+  }
+  uint64_t count = 1, visited = 1;
+  uint32_t depth = 0;
+  if (count < 1000) {
+    small_layer.assign(1, start_word);
+    small_depth = 0;
+  }
+  uint64_t peak = plan.device_bytes;
+  st.reason = MGBFS2_REASON_FRONTIER_EXHAUSTED;
+  for (;;) {
+    const double elapsed = std::chrono::duration<double>(Clock::now() - started).count();
+    if (limits && limits->cancel && *limits->cancel) { st.reason = MGBFS2_REASON_CANCELLED; break; }
+    if (limits && limits->max_seconds > 0 && elapsed >= limits->max_seconds) { st.reason = MGBFS2_REASON_DEADLINE; break; }
+    if (limits && limits->max_layers && layer_sizes.size() >= limits->max_layers) {
+      st.reason = MGBFS2_REASON_LAYER_LIMIT;
+      break;
+    }
+    const auto layer_start = Clock::now();
+    const uint64_t bound = next_bound(depth, count, visited);
+    const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(bound, 1), plan.capacity);
+    if ((rc = next.ensure((cap + 2) * 8))) break;
+    p.frontier = static_cast<const unsigned long long*>(front.ptr);
+    p.count = count;
+    p.next = static_cast<unsigned long long*>(next.ptr);
+    p.capacity = cap;
+    p.probe_limit = 1u << 20;
+    if (visit == V_HASH) {
+      // Grow (rehash) so the table stays at most half full after this layer.
+      const uint64_t need = visited + bound;
+      if (need > table_slots / 2) {
+        const uint64_t slots = next_pow2(2 * need);
+        DeviceBuffer grown;
+        if ((rc = grown.ensure(slots * 8))) break;
+        MG_CHECK(cudaMemsetAsync(grown.ptr, 0xff, slots * 8, stream));
+        rehash_table<<<grid_for(reinterpret_cast<const void*>(rehash_table), 0, (table_slots + kBlock - 1) / kBlock),
+                       kBlock, 0, stream>>>(static_cast<const unsigned long long*>(table.ptr), table_slots,
+                                            static_cast<unsigned long long*>(grown.ptr), slots - 1, key_mask,
+                                            &p.control->error);
+        ++launches;
+        MG_CHECK(cudaGetLastError());
+        MG_CHECK(cudaStreamSynchronize(stream));
+        table.free();
+        table = grown;
+        grown.ptr = nullptr;
+        grown.bytes = 0;
+        table_slots = slots;
+      }
+      p.table = static_cast<unsigned long long*>(table.ptr);
+      p.table_mask = table_slots - 1;
+      p.tag = 0;
+    } else if (visit == V_HASH3) {
+      const int ins = (depth + 1) % 3, cur = depth % 3, prev = (depth + 2) % 3;
+      const uint64_t slots = std::max<uint64_t>(1024, next_pow2(2 * std::max<uint64_t>(bound, 1)));
+      if ((rc = bank[ins].ensure(slots * 8))) break;
+      bank_slots[ins] = slots;
+      MG_CHECK(cudaMemsetAsync(bank[ins].ptr, 0xff, slots * 8, stream));
+      p.table = static_cast<unsigned long long*>(bank[ins].ptr);
+      p.table_mask = slots - 1;
+      p.look0 = static_cast<const unsigned long long*>(bank[cur].ptr);
+      p.look0_mask = bank_slots[cur] - 1;
+      p.look1 = depth >= 1 ? static_cast<const unsigned long long*>(bank[prev].ptr) : nullptr;
+      p.look1_mask = depth >= 1 ? bank_slots[prev] - 1 : 0;
+    }
+    MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
+    const uint64_t tiles = (count + kBlock * p.ppt - 1) / (kBlock * p.ppt);
+    const uint32_t grid = grid_for(reinterpret_cast<const void*>(fn), smem, tiles);
+    MG_CHECK(cudaEventRecord(ev_kernel[0], stream));
+    fn<<<grid, kBlock, smem, stream>>>(p);
+    ++launches;
+    MG_CHECK(cudaGetLastError());
+    MG_CHECK(cudaEventRecord(ev_kernel[1], stream));
+    MG_CHECK(cudaMemcpyAsync(host_control, control_buf.ptr, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+    MG_CHECK(cudaStreamSynchronize(stream));
+    {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev_kernel[0], ev_kernel[1]) == cudaSuccess) kernel_seconds += ms * 1e-3;
+    }
+    st.successors += count * gens;
+    const Control c = *host_control;
+    peak = std::max<uint64_t>(peak, bitmap.bytes + front.bytes + next.bytes + table.bytes + bank[0].bytes +
+                                        bank[1].bytes + bank[2].bytes);
+    if (c.error) {
+      st.reason = MGBFS2_REASON_RESOURCE;
+      st.fatal = c.error;
+      break;
+    }
+    if (c.next_count == 0) {
+      st.complete = 1;
+      break;
+    }
+    if (c.next_count > cap) {
+      st.reason = MGBFS2_REASON_RESOURCE;
+      st.fatal = ERR_FRONTIER_OVERFLOW;
+      break;
+    }
+    const double secs = std::chrono::duration<double>(Clock::now() - layer_start).count();
+    layer_sizes.push_back(c.next_count);
+    layer_seconds.push_back(secs);
+    std::swap(front, next);
+    count = c.next_count;
+    visited += count;
+    ++depth;
+    if (count < 1000) {
+      small_layer.resize(count);
+      MG_CHECK(cudaMemcpy(small_layer.data(), front.ptr, count * 8, cudaMemcpyDeviceToHost));
+      small_depth = depth;
+    }
+    if (cb && cb(user, depth, count, secs)) {
+      st.reason = MGBFS2_REASON_CANCELLED;
+      break;
+    }
+  }
+  last_count = count;
+  st.layers = static_cast<uint32_t>(layer_sizes.size());
+  for (uint64_t s : layer_sizes) st.states += s;
+  if (cudaEventRecord(ev_run[1], stream) == cudaSuccess && cudaEventSynchronize(ev_run[1]) == cudaSuccess) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ev_run[0], ev_run[1]) == cudaSuccess) st.device_seconds = ms * 1e-3;
+  }
+  st.kernel_seconds = kernel_seconds;
+  st.bfs_seconds = std::chrono::duration<double>(Clock::now() - started).count();
+  st.kernel_launches = launches;
+  st.peak_device_bytes = peak;
+  if (status) *status = st;
+  return rc;
+}
+
+std::vector<int64_t> Graph::decode(uint64_t w) const {
+  std::vector<int64_t> row(elements);
+  const uint64_t mask = bits == 64 ? ~0ull : ((1ull << bits) - 1);
+  for (uint32_t i = 0; i < elements; ++i) row[i] = labels[(w >> (bits * i)) & mask];
+  return row;
+}
+
+int Graph::sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* rows) {
+  if (!rows) return MGBFS2_INVALID_ARGUMENT;
+  *rows = 0;
+  if (layer_sizes.empty()) return MGBFS2_STATE;
+  if (!packed) return wide_sample(which, out, cap_rows, rows);
+  const uint32_t deepest = static_cast<uint32_t>(layer_sizes.size() - 1);
+  std::vector<uint64_t> words;
+  if (which == 0) {
+    const uint64_t n = std::min<uint64_t>(last_count, cap_rows);
+    words.resize(n);
+    if (n) MG_CHECK(cudaMemcpy(words.data(), front.ptr, n * 8, cudaMemcpyDeviceToHost));
+  } else {
+    if (deepest == 0 || small_depth != deepest - 1 || layer_sizes[deepest - 1] >= 1000) return MGBFS2_OK;
+    words.assign(small_layer.begin(), small_layer.begin() + std::min<size_t>(small_layer.size(), cap_rows));
+  }
+  std::vector<std::vector<int64_t>> decoded;
+  for (uint64_t w : words) decoded.push_back(decode(w));
+  std::sort(decoded.begin(), decoded.end());
+  for (size_t i = 0; i < decoded.size(); ++i)
+    if (out) std::memcpy(out + i * elements, decoded[i].data(), elements * sizeof(int64_t));
+  *rows = decoded.size();
+  return MGBFS2_OK;
+}
+
+}  // namespace mgbfs2
+
+// ---------------------------------------------------------------------------
+// C ABI.
+
+using mgbfs2::Graph;
+
+struct mgbfs2_graph {
+  Graph* impl;
+};
+
+extern "C" {
+
+int mgbfs2_graph_create(const mgbfs2_graph_desc* desc, int device, mgbfs2_graph** out, char* error,
+                        size_t error_capacity) {
+  if (!out) return MGBFS2_INVALID_ARGUMENT;
+  *out = nullptr;
+  Graph* g = nullptr;
+  int rc = Graph::create(desc, device, &g, error, error_capacity);
+  if (rc) return rc;
+  *out = new mgbfs2_graph{g};
+  return MGBFS2_OK;
+}
+
+int mgbfs2_plan(mgbfs2_graph* graph, const mgbfs2_plan_request* request, mgbfs2_plan_info* plan) {
+  if (!graph) return MGBFS2_INVALID_ARGUMENT;
+  return graph->impl->make_plan(request, plan);
+}
+
+int mgbfs2_run(mgbfs2_graph* graph, const mgbfs2_run_limits* limits, mgbfs2_layer_callback callback, void* user,
+               mgbfs2_status* status) {
+  if (!graph) return MGBFS2_INVALID_ARGUMENT;
+  return graph->impl->run(limits, callback, user, status);
+}
+
+int mgbfs2_layer_table(const mgbfs2_graph* graph, uint64_t* sizes, double* seconds, size_t capacity,
+                       size_t* count) {
+  if (!graph || !count) return MGBFS2_INVALID_ARGUMENT;
+  const Graph* g = graph->impl;
+  *count = g->layer_sizes.size();
+  for (size_t i = 0; i < g->layer_sizes.size() && i < capacity; ++i) {
+    if (sizes) sizes[i] = g->layer_sizes[i];
+    if (seconds) seconds[i] = i == 0 ? 0.0 : g->layer_seconds[i - 1];
+  }
+  return MGBFS2_OK;
+}
+
+int mgbfs2_sample(mgbfs2_graph* graph, uint32_t which, int64_t* out, size_t capacity_rows, size_t* rows) {
+  if (!graph || which > 1) return MGBFS2_INVALID_ARGUMENT;
+  return graph->impl->sample(which, out, capacity_rows, rows);
+}
+
+const char* mgbfs2_status_string(int code) {
+  switch (code) {
+    case MGBFS2_OK: return "OK";
+    case MGBFS2_INVALID_ARGUMENT: return "INVALID_ARGUMENT";
+    case MGBFS2_UNSUPPORTED: return "UNSUPPORTED";
+    case MGBFS2_OUT_OF_MEMORY: return "OUT_OF_MEMORY";
+    case MGBFS2_CAPACITY: return "CAPACITY";
+    case MGBFS2_DEVICE_STATUS: return "DEVICE_STATUS";
+    case MGBFS2_STATE: return "STATE";
+    case MGBFS2_NOT_FOUND: return "NOT_FOUND";
+    default:
+      if (code >= MGBFS2_CUDA_BASE) return cudaGetErrorString(static_cast<cudaError_t>(code - MGBFS2_CUDA_BASE));
+      return "UNKNOWN";
+  }
+}
+
+void mgbfs2_destroy(mgbfs2_graph* graph) {
+  if (!graph) return;
+  delete graph->impl;
+  delete graph;
+}
+
+}  // extern "C"

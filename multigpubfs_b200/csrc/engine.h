@@ -1,0 +1,88 @@
+// Host-side engine state of one graph handle (libmgbfs2 internal header).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/mgbfs2.h"
+#include "device.cuh"
+
+namespace mgbfs2 {
+
+int cuda_status(cudaError_t e);
+
+// A plain device allocation that only grows.  No destructor: owners call free().
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t want);
+  void free();
+};
+
+struct WideState;  // int64-key arena path (wide.cu)
+
+struct Graph {
+  // Description.
+  int device = 0;
+  uint32_t kind = 0, elements = 0, rows = 0, cols = 0, gens = 0;
+  std::vector<uint32_t> perms;
+  std::vector<int64_t> matrices;
+  std::vector<uint32_t> moduli;
+  std::vector<int64_t> start;
+  uint64_t orbit_bound = 0;
+
+  // Analysis.
+  bool packed = false, inverse_closed = false, lehmer = false, rank_ok = false;
+  uint32_t bits = 4, distinct = 0;
+  std::vector<int64_t> labels;     // code -> label
+  std::vector<uint32_t> codes;     // start codes
+  std::vector<uint32_t> code_counts;
+  uint64_t start_word = 0, key_mask = ~0ull;
+  uint64_t rank_total = 0, state_bound = 0;
+  std::vector<uint64_t> coxeter;   // certified layer sizes, empty if not Coxeter
+  std::vector<Term> terms;
+  std::vector<uint32_t> term_begin;
+
+  // Plan and device state.
+  bool planned = false;
+  mgbfs2_plan_info plan{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_run[2] = {nullptr, nullptr}, ev_kernel[2] = {nullptr, nullptr};
+  int sm_count = 148;
+  DeviceBuffer bitmap, front, next, table, bank[3], program, control_buf, scratch;
+  uint64_t table_slots = 0, bank_slots[3] = {0, 0, 0};
+  Control* host_control = nullptr;
+  WideState* wide = nullptr;
+
+  // Results.
+  std::vector<uint64_t> layer_sizes;
+  std::vector<double> layer_seconds;
+  std::vector<uint64_t> small_layer;  // the most recent layer with < 1000 states
+  uint32_t small_depth = UINT32_MAX;
+  uint64_t last_count = 0;
+  uint32_t launches = 0;
+
+  static int create(const mgbfs2_graph_desc* d, int device, Graph** out, char* error, size_t cap);
+  ~Graph();
+  void analyse();
+  void build_program();
+  bool matrix_inverse_closed() const;
+  void release();
+  int make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out);
+  int run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status);
+  int sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* rows);
+  int visit_kind() const;
+  uint32_t grid_for(const void* fn, size_t smem, uint64_t work_blocks);
+  uint64_t next_bound(uint32_t depth, uint64_t count, uint64_t visited) const;
+  std::vector<int64_t> decode(uint64_t w) const;
+
+  // Wide (multi-word int64 key) path, wide.cu.
+  uint32_t wide_key_words() const;
+  int wide_plan(mgbfs2_plan_info* p, uint64_t budget);
+  int wide_run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status);
+  int wide_sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* rows);
+  void wide_release();
+};
+
+}  // namespace mgbfs2

@@ -1,0 +1,220 @@
+// Fused layer-expansion kernels of the packed (one-word state) path.
+//
+// One launch expands a whole frontier layer: parent load (128-bit, coalesced)
+// -> generator application in registers -> visited test-and-set -> block
+// compaction of the winners in shared memory -> one global reservation per
+// tile -> coalesced append to the next frontier.  The reference splits the
+// same work over accept_candidates (cuda/generic_visited.cu:18-58) for the
+// hash and bitmap_route + bitmap_accept[_grouped] (cuda/permutation_bitmap.cu:
+// 27-48, 105-205) for the bitmap, with one global atomicAdd per appended row.
+#pragma once
+#include "device.cuh"
+
+namespace mgbfs2 {
+
+enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3 };
+
+constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
+constexpr uint32_t kBlock = 256;
+
+struct ExpandParams {
+  const unsigned long long* frontier;
+  unsigned long long count;
+  unsigned long long* next;
+  unsigned long long capacity;
+  const Term* terms;
+  const uint32_t* term_begin;
+  uint32_t gens, total_terms;
+  Control* control;
+  unsigned long long* bitmap;
+  MultisetDomain ms;
+  unsigned long long* table;  // insert table (all-visited table, or bank of layer d+1)
+  unsigned long long table_mask, key_mask, tag;
+  uint32_t probe_limit, ppt;
+  const unsigned long long* look0;  // three-bank lookups: layer d and layer d-1
+  unsigned long long look0_mask;
+  const unsigned long long* look1;
+  unsigned long long look1_mask;
+};
+
+// Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the
+// warp-aggregated bitmap path uses warp collectives); `valid` masks lanes
+// without a candidate.
+template <int V, int N, bool WARP>
+__device__ __forceinline__ bool claim(const ExpandParams& p, uint64_t c, bool valid) {
+  if constexpr (V == V_LEHMER || V == V_MULTISET) {
+    uint64_t r = 0;
+    bool ok = valid;
+    if (valid) {
+      if constexpr (V == V_LEHMER) {
+        r = lehmer_rank4<N>(c);
+      } else {
+        ok = multiset_rank(c, p.ms, &r);
+        if (!ok) raise_error(&p.control->error, ERR_RANK_RANGE);
+      }
+    }
+    if constexpr (WARP) {
+      // Lanes whose ranks share a bitmap word merge their bits into one
+      // atomicOr; among lanes with the same rank only the lowest may win.
+      const unsigned active = __ballot_sync(kFullMask, ok);
+      bool won = false;
+      if (ok) {
+        const unsigned long long word = r >> 6;
+        const unsigned peers = __match_any_sync(active, word);
+        const unsigned same = __match_any_sync(peers, static_cast<unsigned long long>(r));
+        const unsigned long long bit = 1ull << (r & 63);
+        const unsigned lo = __reduce_or_sync(peers, static_cast<unsigned>(bit));
+        const unsigned hi = __reduce_or_sync(peers, static_cast<unsigned>(bit >> 32));
+        const int leader = __ffs(peers) - 1;
+        const int lane = static_cast<int>(lane_id());
+        unsigned long long old = 0;
+        if (lane == leader) old = atomicOr(&p.bitmap[word], (static_cast<unsigned long long>(hi) << 32) | lo);
+        old = __shfl_sync(peers, old, leader);
+        won = (lane == __ffs(same) - 1) && !(old & bit);
+      }
+      return won;
+    } else {
+      if (!ok) return false;
+      const unsigned long long bit = 1ull << (r & 63);
+      return !(atomicOr(&p.bitmap[r >> 6], bit) & bit);
+    }
+  } else if constexpr (V == V_HASH) {
+    if (!valid) return false;
+    const int rc = hash_insert(p.table, p.table_mask, c, p.key_mask, p.tag, p.probe_limit);
+    if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+    return rc == 1;
+  } else {
+    if (!valid) return false;
+    // Inverse-closed graphs: every neighbour of layer d lies in d-1, d or d+1.
+    if (hash_contains(p.look0, p.look0_mask, c, p.key_mask) || hash_contains(p.look1, p.look1_mask, c, p.key_mask))
+      return false;
+    const int rc = hash_insert(p.table, p.table_mask, c, p.key_mask, 0, p.probe_limit);
+    if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+    return rc == 1;
+  }
+}
+
+// Append the block's shared-memory winners to the next frontier with one
+// global reservation.  Called by all threads of the block.
+__device__ __forceinline__ void flush_block(const ExpandParams& p, unsigned long long* out, uint32_t* out_count,
+                                            unsigned long long* out_base) {
+  __syncthreads();
+  const uint32_t n = *out_count;
+  if (threadIdx.x == 0 && n) *out_base = atomicAdd(&p.control->next_count, static_cast<unsigned long long>(n));
+  __syncthreads();
+  const unsigned long long base = *out_base;
+  bool overflow = false;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const unsigned long long pos = base + i;
+    if (pos < p.capacity) p.next[pos] = out[i];
+    else overflow = true;
+  }
+  if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
+  __syncthreads();
+  if (threadIdx.x == 0) *out_count = 0;
+  __syncthreads();
+}
+
+template <int V, int N, bool WARP>
+__global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
+  extern __shared__ __align__(16) unsigned char program_smem[];
+  __shared__ unsigned long long out[kOutCap];
+  __shared__ uint32_t out_count;
+  __shared__ unsigned long long out_base;
+  Term* terms = reinterpret_cast<Term*>(program_smem);
+  uint32_t* begin = reinterpret_cast<uint32_t*>(program_smem + p.total_terms * sizeof(Term));
+  for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i <= p.gens; i += blockDim.x) begin[i] = p.term_begin[i];
+  if (threadIdx.x == 0) out_count = 0;
+  __syncthreads();
+
+  const uint32_t lane = lane_id();
+  const uint32_t tile = blockDim.x * p.ppt;
+  const unsigned long long tiles = (p.count + tile - 1) / tile;
+  for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const unsigned long long base = t * tile;
+    uint64_t par[4];
+    bool val[4];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      par[2 * j] = par[2 * j + 1] = 0;
+      val[2 * j] = val[2 * j + 1] = false;
+      if (2 * j < static_cast<int>(p.ppt)) {
+        const unsigned long long i0 = base + 2ull * (j * blockDim.x + threadIdx.x);
+        if (i0 + 1 < p.count) {
+          const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p.frontier + i0);
+          par[2 * j] = v.x;
+          par[2 * j + 1] = v.y;
+          val[2 * j] = val[2 * j + 1] = true;
+        } else if (i0 < p.count) {
+          par[2 * j] = p.frontier[i0];
+          val[2 * j] = true;
+        }
+      }
+    }
+    for (uint32_t g = 0; g < p.gens; ++g) {
+      const uint32_t tb = begin[g], te = begin[g + 1];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k >= static_cast<int>(p.ppt)) break;
+        const uint64_t c = val[k] ? apply_terms(par[k], terms, tb, te) : 0;
+        const bool won = claim<V, N, WARP>(p, c, val[k]);
+        const unsigned m = __ballot_sync(kFullMask, won);
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          uint32_t wb = 0;
+          if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
+          wb = __shfl_sync(kFullMask, wb, leader);
+          if (won) out[wb + __popc(m & lanemask_lt())] = c;
+        }
+      }
+      if (g + 1 < p.gens) {
+        __syncthreads();
+        const uint32_t pending = out_count;
+        __syncthreads();
+        if (pending + tile > kOutCap) flush_block(p, out, &out_count, &out_base);
+      }
+    }
+    flush_block(p, out, &out_count, &out_base);
+  }
+}
+
+// Marks the start state visited (and, for the hash paths, inserts it).
+__global__ void seed_packed(ExpandParams p, unsigned long long start, int kind, uint32_t n) {
+  if (threadIdx.x || blockIdx.x) return;
+  uint64_t r = 0;
+  if (kind == V_LEHMER) {
+    r = lehmer_rank4_n(start, n);
+    atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
+  } else if (kind == V_MULTISET) {
+    if (multiset_rank(start, p.ms, &r)) atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
+    else raise_error(&p.control->error, ERR_RANK_RANGE);
+  } else {
+    if (hash_insert(p.table, p.table_mask, start, p.key_mask, p.tag, p.probe_limit) < 0)
+      raise_error(&p.control->error, ERR_TABLE_FULL);
+  }
+}
+
+// Re-inserts every key of an old all-visited table into a larger one.
+__global__ void rehash_table(const unsigned long long* old_table, unsigned long long old_slots,
+                             unsigned long long* table, unsigned long long mask, unsigned long long key_mask,
+                             unsigned int* error) {
+  for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < old_slots;
+       i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long v = old_table[i];
+    if (v == kEmpty) continue;
+    // Keep the tag bits: insert the full word, compare on the key bits.
+    uint64_t slot = mix64(v & key_mask) & mask;
+    bool placed = false;
+    for (unsigned long long probe = 0; probe <= mask; ++probe) {
+      if (atomicCAS(&table[slot], kEmpty, v) == kEmpty) {
+        placed = true;
+        break;
+      }
+      slot = (slot + 1) & mask;
+    }
+    if (!placed) atomicOr(error, ERR_TABLE_FULL);
+  }
+}
+
+}  // namespace mgbfs2

@@ -1,0 +1,165 @@
+"""ctypes binding of libmgbfs2.so (the C ABI declared in include/mgbfs2.h).
+
+There is no CPU fallback: if the shared library is missing or no CUDA device
+is present, every entry point raises ``NativeUnavailable``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+from .build import LIBRARY
+
+_LOCK = threading.Lock()
+_LIB = None
+
+DEVICE_STATUS = 5  # MGBFS2_DEVICE_STATUS
+VISITED = {"auto": 0, "bitmap": 1, "hash": 2, "hash3": 3}
+VISITED_NAMES = {v: k for k, v in VISITED.items()}
+DEDUP = {"auto": 0, "atomic": 1, "warp": 2, "sort": 3, "bucket": 4}
+DEDUP_NAMES = {v: k for k, v in DEDUP.items()}
+PLANNER = {"plain": 0, "learned": 1}
+REASONS = {0: "FRONTIER_EXHAUSTED", 1: "DEADLINE", 2: "CANCELLED", 3: "RESOURCE", 4: "PROFILE_LAYER_LIMIT"}
+ERROR_BITS = {1: "FRONTIER_OVERFLOW", 2: "TABLE_FULL", 4: "RANK_RANGE", 8: "BUCKET_OVERFLOW", 16: "WAIT_LIMIT",
+              32: "ARENA_OVERFLOW", 64: "BAD_STATE"}
+
+
+class NativeUnavailable(RuntimeError):
+    """libmgbfs2 could not be loaded or no CUDA device is usable."""
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, where: str, message: str = ""):
+        self.code = code
+        text = f"{where}: MGBFS2_STATUS_{code} ({status_string(code)})"
+        if message:
+            text += f": {message}"
+        super().__init__(text)
+
+
+class GraphDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("elements", C.c_uint32), ("rows", C.c_uint32), ("cols", C.c_uint32),
+                ("generators", C.c_uint32), ("permutations", C.POINTER(C.c_uint32)),
+                ("matrices", C.POINTER(C.c_int64)), ("moduli", C.POINTER(C.c_uint32)),
+                ("start", C.POINTER(C.c_int64)), ("orbit_bound", C.c_uint64)]
+
+
+class PlanRequest(C.Structure):
+    _fields_ = [("visited", C.c_uint32), ("dedup", C.c_uint32), ("capacity", C.c_uint64),
+                ("reserve_bytes", C.c_uint64), ("shards", C.c_uint32), ("block", C.c_uint32),
+                ("planner", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("visited", C.c_uint32), ("dedup", C.c_uint32), ("packed", C.c_uint32),
+                ("bits_per_symbol", C.c_uint32), ("key_words", C.c_uint32), ("history_layers", C.c_uint32),
+                ("capacity", C.c_uint64), ("table_slots", C.c_uint64), ("bitmap_bits", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("state_bound", C.c_uint64), ("shards", C.c_uint32),
+                ("block", C.c_uint32), ("inverse_closed", C.c_uint32), ("planner", C.c_uint32)]
+
+    def to_dict(self):
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["visited"] = VISITED_NAMES.get(self.visited, self.visited)
+        d["dedup"] = DEDUP_NAMES.get(self.dedup, self.dedup)
+        d["planner"] = {0: "plain", 1: "learned"}.get(self.planner, self.planner)
+        return d
+
+
+class RunLimits(C.Structure):
+    _fields_ = [("max_seconds", C.c_double), ("max_layers", C.c_uint32), ("reserved", C.c_uint32),
+                ("cancel", C.POINTER(C.c_int32))]
+
+
+class RunStatus(C.Structure):
+    _fields_ = [("complete", C.c_uint32), ("reason", C.c_uint32), ("fatal", C.c_uint32), ("layers", C.c_uint32),
+                ("states", C.c_uint64), ("successors", C.c_uint64), ("bfs_seconds", C.c_double),
+                ("redo_layers", C.c_uint32), ("kernel_launches", C.c_uint32), ("peak_device_bytes", C.c_uint64),
+                ("device_seconds", C.c_double), ("kernel_seconds", C.c_double)]
+
+
+LAYER_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint64, C.c_double)
+
+_SIGNATURES = {
+    "mgbfs2_graph_create": (C.c_int, [C.POINTER(GraphDesc), C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "mgbfs2_plan": (C.c_int, [C.c_void_p, C.POINTER(PlanRequest), C.POINTER(PlanInfo)]),
+    "mgbfs2_run": (C.c_int, [C.c_void_p, C.POINTER(RunLimits), LAYER_CALLBACK, C.c_void_p, C.POINTER(RunStatus)]),
+    "mgbfs2_layer_table": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_size_t,
+                                     C.POINTER(C.c_size_t)]),
+    "mgbfs2_sample": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int64), C.c_size_t, C.POINTER(C.c_size_t)]),
+    "mgbfs2_status_string": (C.c_char_p, [C.c_int]),
+    "mgbfs2_destroy": (None, [C.c_void_p]),
+    "mgbfs2_successors_i64": (C.c_int, [C.c_uint32] * 5 + [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mgbfs2_successors_packed": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
+                                           C.c_uint64, C.c_void_p, C.c_void_p]),
+    "mgbfs2_rank_packed": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
+                                     C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mgbfs2_bitmap_claim": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32,
+                                      C.c_void_p, C.c_void_p]),
+    "mgbfs2_hash_insert": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
+    "mgbfs2_sort_unique_tiles": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]),
+    "mgbfs2_bucket_keys": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
+}
+
+
+def exported_symbols():
+    """Names declared by include/mgbfs2.h that the library must export."""
+    return sorted(_SIGNATURES)
+
+
+def load(path: str | Path | None = None):
+    """Load libmgbfs2 (no device check).  Raises NativeUnavailable if absent."""
+    global _LIB
+    with _LOCK:
+        if _LIB is not None and path is None:
+            return _LIB
+        target = Path(path) if path else LIBRARY
+        if not target.exists():
+            raise NativeUnavailable(f"libmgbfs2 not built: {target} (run python -m multigpubfs_b200.build)")
+        try:
+            lib = C.CDLL(str(target))
+        except OSError as exc:
+            raise NativeUnavailable(f"libmgbfs2 failed to load: {exc}") from exc
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        if path is None:
+            _LIB = lib
+        return lib
+
+
+def status_string(code: int) -> str:
+    try:
+        return load().mgbfs2_status_string(code).decode()
+    except NativeUnavailable:
+        return "UNKNOWN"
+
+
+def require_device():
+    """Load the library and require a CUDA device (no CPU fallback)."""
+    lib = load()
+    import torch
+    if not torch.cuda.is_available():
+        raise NativeUnavailable("no CUDA device: the native BFS has no CPU fallback")
+    return lib
+
+
+def check(code: int, where: str):
+    if code:
+        raise NativeError(code, where)
+
+
+def stream_handle(stream=None) -> int | None:
+    """cudaStream_t of a torch stream (None -> torch's current stream)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def ptr(tensor) -> int:
+    return tensor.data_ptr()

@@ -1,0 +1,206 @@
+"""GPU parity: every layer table bit-exact against the reference-pinned oracle.
+
+Runs libmgbfs2 through its C ABI (multigpubfs_b200.engine.NativeGraph) on every
+golden case, on LRX S3..S11 (reference packed search), on S13 LRX (the
+reference's shipped table) and Coxeter S13 (Mahonian certificate), and on
+seeded random generator sets against the C oracle, for each visited-set /
+dedup variant that applies.
+"""
+import math
+
+import pytest
+
+from oracle import graph_oracle as G
+from oracle import packed_oracle as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine():
+    from multigpubfs_b200.engine import NativeGraph
+    return NativeGraph
+
+
+def run(graph_dict, **plan):
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.native import NativeError
+    g = GraphDefinition.from_dict(graph_dict)
+    with _engine()(g) as e:
+        try:
+            info = e.plan(**plan)
+        except NativeError as exc:
+            if exc.code == 2:  # MGBFS2_UNSUPPORTED for this variant
+                return None
+            raise
+        r = e.run()
+        return info, r, e.sample(0, 1000), e.sample(1, 1000)
+
+
+VARIANTS = {
+    "auto": {},
+    "bitmap_atomic": dict(visited="bitmap", dedup="atomic"),
+    "bitmap_warp": dict(visited="bitmap", dedup="warp"),
+    "hash": dict(visited="hash"),
+    "hash3": dict(visited="hash3"),
+}
+
+
+def _applicable(case, variant):
+    g = case["graph"]
+    if variant == "hash3":
+        return case["inverse_closed"]
+    if variant.startswith("bitmap"):
+        return g["action"]["kind"] == "permutation" and len(set(g["start"])) <= 16 and \
+            len(g["start"]) * P.bits_for(len(set(g["start"]))) <= 64 and math.factorial(len(g["start"])) < 1 << 34
+    return True
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_golden_cases(exact_cases, variant):
+    ran = 0
+    for case in exact_cases:
+        if not _applicable(case, variant):
+            continue
+        out = run(case["graph"], **VARIANTS[variant])
+        if out is None:
+            assert variant != "auto", case["name"]
+            continue
+        info, r, last, prev = out
+        assert r.complete, (case["name"], r)
+        assert r.layer_sizes == case["layer_sizes"], (case["name"], info)
+        sizes = case["layer_sizes"]
+        if case["last_layer"] is not None:
+            if sizes[-1] <= 1000:
+                assert last == case["last_layer"], case["name"]
+            else:
+                assert len(last) == 1000 and all(x in case["last_layer"] for x in last)
+        if len(sizes) > 1 and sizes[-2] < 1000 and case["previous_layer"] is not None:
+            assert prev == case["previous_layer"], case["name"]
+        else:
+            assert prev == []
+        assert r.successors == sum(sizes) * len(case["graph"]["action"]["generators"])
+        ran += 1
+    assert ran >= 8
+
+
+@pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3"])
+def test_lrx_small(lrx_layers, variant):
+    for n in range(3, 12):
+        out = run(G.permutation_graph(G.lrx_generators(n), list(range(n))), **VARIANTS[variant])
+        assert out is not None
+        assert out[1].layer_sizes == lrx_layers[n], (n, variant)
+
+
+@pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic"])
+def test_lrx13_full_table(lrx13, variant):
+    out = run(G.permutation_graph(G.lrx_generators(13), list(range(13))), **VARIANTS[variant])
+    info, r, last, prev = out
+    assert info["visited"] == "bitmap"
+    assert r.layer_sizes == lrx13
+    # The deepest layer of S13 LRX is a single state; the one before holds 3.
+    assert len(last) == 1 and len(prev) == 3
+
+
+def test_lrx12_three_bank_hash():
+    sizes_ref, _, _ = P.packed_bfs(G.lrx_generators(10), list(range(10)))
+    out = run(G.permutation_graph(G.lrx_generators(10), list(range(10))), visited="hash3")
+    assert out[0]["history_layers"] == 3
+    assert out[1].layer_sizes == sizes_ref
+
+
+@pytest.mark.parametrize("n,variant", [(10, "hash3"), (11, "bitmap_warp"), (13, "bitmap_warp")])
+def test_coxeter(n, variant):
+    out = run(G.permutation_graph(G.coxeter_generators(n), list(range(n))), **VARIANTS[variant])
+    assert out[1].layer_sizes == G.coxeter_layers(n)
+
+
+@pytest.mark.parametrize("closed", [False, True])
+def test_random_sweep_instances(closed):
+    for i in range(12):
+        g = G.sweep_instance(i, closed)
+        n = len(g["start"])
+        ref, last_ref, _ = P.packed_bfs(g["action"]["generators"], g["start"], sample=1 << 22)
+        for variant in ("auto", "hash", "bitmap_warp") + (("hash3",) if closed else ()):
+            out = run(g, **VARIANTS[variant])
+            assert out[1].layer_sizes == ref, (i, variant, n)
+            if ref[-1] <= 1000:
+                assert out[2] == last_ref, (i, variant)
+
+
+def test_layer_limit_deadline_and_cancel():
+    import ctypes
+    from multigpubfs_b200 import GraphDefinition
+    g = GraphDefinition.permutation(G.lrx_generators(9), list(range(9)))
+    with _engine()(g) as e:
+        e.plan()
+        r = e.run(max_layers=5)
+        assert not r.complete and r.reason == "PROFILE_LAYER_LIMIT" and len(r.layer_sizes) == 5
+        flag = ctypes.c_int32(1)
+        r = e.run(cancel_flag=flag)
+        assert not r.complete and r.reason == "CANCELLED" and r.layer_sizes == [1]
+        r = e.run(on_layer=lambda depth, size, secs: depth >= 3)
+        assert r.reason == "CANCELLED" and len(r.layer_sizes) == 4
+        r = e.run()
+        assert r.complete and sum(r.layer_sizes) == math.factorial(9)
+
+
+def test_capacity_overflow_is_resource_not_wrong_answer():
+    from multigpubfs_b200 import GraphDefinition
+    g = GraphDefinition.permutation(G.lrx_generators(8), list(range(8)))
+    with _engine()(g) as e:
+        e.plan(visited="bitmap", capacity=100)
+        r = e.run()
+        assert not r.complete and r.reason == "RESOURCE" and "FRONTIER_OVERFLOW" in r.fatal_names
+        # every completed layer is still exact
+        ref = G.layer_sizes(G.permutation_graph(G.lrx_generators(8), list(range(8))))
+        assert r.layer_sizes == ref[:len(r.layer_sizes)]
+
+
+def test_run_graph_end_to_end(tmp_path, lrx_layers):
+    import hashlib
+    import json
+    from multigpubfs_b200 import GraphDefinition, run_graph
+    g = GraphDefinition.permutation(G.lrx_generators(8), list(range(8)))
+    report = run_graph(g, tmp_path / "out")
+    assert report["status"] == "COMPLETE" and report["reason"] == "FRONTIER_EXHAUSTED"
+    assert report["layer_sizes"] == lrx_layers[8]
+    assert report["graph_digest"] == g.digest()
+    raw = (tmp_path / "out" / "states.json").read_bytes()
+    assert hashlib.sha256(raw).hexdigest() == report["states_sha256"]
+    states = json.loads(raw)
+    assert states["schema"] == 2 and states["state_encoding"] == "signed_int64_vectors"
+    exact = G.exact_layers(G.permutation_graph(G.lrx_generators(8), list(range(8))), 1 << 20)
+    assert states["current"] == exact[-1]
+    assert states["previous_small"] == exact[-2]
+    assert len(report["layer_seconds"]) == len(report["layer_sizes"]) - 1
+
+
+def test_bfs_through_cayleypy_boundary(tmp_path, monkeypatch):
+    import sys
+    import types
+    from types import SimpleNamespace
+    import multigpubfs_b200 as mg
+
+    class CayleyGraph:
+        def __init__(self, definition):
+            self.definition = definition
+
+        def bfs(self, **kwargs):
+            raise AssertionError("original bfs must not run")
+
+    module = types.ModuleType("cayleypy")
+    module.CayleyGraph = CayleyGraph
+    monkeypatch.setitem(sys.modules, "cayleypy", module)
+    gens = G.lrx_generators(5)
+    graph = CayleyGraph(SimpleNamespace(generators_type=SimpleNamespace(name="PERMUTATION"),
+                                        generators_permutations=gens, central_state=list(range(5)), name="lrx-5",
+                                        generator_names=["L", "R", "X"]))
+    mg.enable_native(mg.NativeOptions(output_root=tmp_path))
+    try:
+        result = graph.bfs()
+    finally:
+        mg.disable_native()
+    exact = G.exact_layers(G.permutation_graph(gens, list(range(5))), 1000)
+    assert result.layer_sizes == [len(x) for x in exact]
+    assert result.diameter() == len(exact) - 1
+    assert result.last_layer().tolist() == exact[-1]
