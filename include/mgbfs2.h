@@ -70,7 +70,8 @@ typedef struct {
   uint32_t shards;         /* bucket shards for MGBFS2_DEDUP_BUCKET, 0 = 64 */
   uint32_t block;          /* threads per block, 0 = tuned */
   uint32_t planner;        /* MGBFS2_PLANNER_* */
-  uint32_t reserved;
+  uint32_t bucket_margin;  /* extra entries per shard bucket, 0 = 4096; UINT32_MAX = none */
+  uint64_t bucket_min_work; /* successors per layer from which layers are bucketed, 0 = 2^22 */
 } mgbfs2_plan_request;
 
 typedef struct {

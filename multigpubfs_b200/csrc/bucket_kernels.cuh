@@ -1,0 +1,282 @@
+// Owner routing inside one GPU: the two-kernel bucketed layer expansion of
+// the Lehmer-bitmap path.
+//
+//   route  : parent -> successors -> Lehmer rank r -> shard s = r >> shift,
+//            offset o = r & mask (uint32).  Every thread stages its (at most
+//            kMaxEntries) entries in its own shared-memory slots and counts
+//            them in its warp's private shard histogram; one block-wide scan
+//            turns (shard, warp, lane-rank) into a position of the block's
+//            shard-sorted run, one global atomicAdd per shard reserves the
+//            bucket range, and the runs are written out coalesced.  No
+//            visited-set access.
+//   accept : work items = fixed-size chunks of the shard buckets in
+//            shard-major order, so the blocks resident at any moment all hit
+//            the same ~2^shift-bit bitmap slice, which stays in L2.  Each
+//            offset is one test-and-set (eight in flight per thread); winners
+//            are compacted first and then unranked densely into the next
+//            frontier with one reservation per work item.
+//
+// The visited test thus costs 4 B written + 4 B read of streaming bucket
+// traffic per successor plus L2-resident atomics, instead of a random DRAM
+// sector read-modify-write (the reference routes by owner and claims with
+// random atomics: cuda/permutation_bitmap.cu:27-48 and :105-205).
+//
+// Exactness: a shard bucket that overflows only sets ERR_BUCKET_OVERFLOW while
+// its count keeps the exact total; accept then returns before touching the
+// bitmap and the host redoes the layer with exact per-shard capacities.
+#pragma once
+#include "packed_kernels.cuh"
+
+namespace mgbfs2 {
+
+constexpr uint32_t kMaxShards = 256;
+constexpr uint32_t kMaxEntries = 12;                 // staged successors per thread per flush
+constexpr uint32_t kWarpsPerBlock = kBlock / 32;
+constexpr uint32_t kStageCap = kBlock * kMaxEntries;  // 3072
+constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per accept work item
+
+struct RouteParams {
+  const unsigned long long* frontier;
+  unsigned long long count;
+  const Term* terms;
+  const uint32_t* term_begin;
+  uint32_t gens, total_terms, ppt, shift;
+  uint32_t shards, group;                  // group: generators per flush (group * ppt <= kMaxEntries)
+  uint32_t* buckets;                       // all shards, shard s at [begin[s], begin[s] + cap[s])
+  const unsigned long long* shard_begin;   // per shard
+  const unsigned long long* shard_cap;     // per shard
+  unsigned long long* shard_count;         // per shard, exact
+  Control* control;
+};
+
+struct AcceptParams {
+  const uint32_t* buckets;
+  const unsigned long long* shard_begin;
+  const unsigned long long* shard_count;
+  uint32_t shards, shift;
+  unsigned long long* bitmap;
+  unsigned long long* next;
+  unsigned long long capacity;
+  Control* control;
+};
+
+// One staged entry: offset | shard << 32 | rank-within-warp-and-shard << 40;
+// kNoEntry marks an empty slot.
+constexpr unsigned long long kNoEntry = ~0ull;
+
+struct RouteSmem {
+  // Staging, slot [e][thread]; reused as the block's shard-sorted run.
+  unsigned long long stage[kStageCap];
+  uint32_t hist[kWarpsPerBlock][kMaxShards];  // per-warp counts, then per-warp exclusive offsets
+  uint32_t total[kMaxShards];
+  uint32_t start[kMaxShards + 1];             // start of shard s in the sorted run
+  unsigned long long gbase[kMaxShards];       // reserved bucket position of the run
+};
+
+template <int N>
+__global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
+  extern __shared__ __align__(16) unsigned char program_smem[];
+  __shared__ RouteSmem sm;
+  Term* terms = reinterpret_cast<Term*>(program_smem);
+  uint32_t* tbegin = reinterpret_cast<uint32_t*>(program_smem + p.total_terms * sizeof(Term));
+  for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i <= p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
+  for (uint32_t i = threadIdx.x; i < kWarpsPerBlock * kMaxShards; i += blockDim.x) (&sm.hist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint64_t off_mask = (1ull << p.shift) - 1;
+  const uint32_t tile = kBlock * p.ppt;
+  const unsigned long long tiles = (p.count + tile - 1) / tile;
+  for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const unsigned long long base = t * tile;
+    uint64_t par[4] = {0, 0, 0, 0};
+    bool val[4] = {false, false, false, false};
+    if (p.ppt == 1) {
+      const unsigned long long i0 = base + tid;
+      if (i0 < p.count) {
+        par[0] = p.frontier[i0];
+        val[0] = true;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (2 * j >= static_cast<int>(p.ppt)) break;
+        const unsigned long long i0 = base + 2ull * (j * kBlock + tid);
+        if (i0 + 1 < p.count) {
+          const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p.frontier + i0);
+          par[2 * j] = v.x;
+          par[2 * j + 1] = v.y;
+          val[2 * j] = val[2 * j + 1] = true;
+        } else if (i0 < p.count) {
+          par[2 * j] = p.frontier[i0];
+          val[2 * j] = true;
+        }
+      }
+    }
+    for (uint32_t g0 = 0; g0 < p.gens; g0 += p.group) {
+      const uint32_t g1 = min(p.gens, g0 + p.group);
+      const uint32_t entries = (g1 - g0) * p.ppt;
+      // Produce: rank every successor, count it in the warp's histogram.
+      for (uint32_t g = g0; g < g1; ++g) {
+        const uint32_t tb = tbegin[g], te = tbegin[g + 1];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (k >= static_cast<int>(p.ppt)) break;
+          const uint32_t slot = ((g - g0) * p.ppt + k) * kBlock + tid;
+          if (val[k]) {
+            const uint64_t r = lehmer_rank4<N>(apply_terms(par[k], terms, tb, te));
+            const uint32_t s = static_cast<uint32_t>(r >> p.shift);
+            const unsigned long long local = atomicAdd(&sm.hist[warp][s], 1u);
+            sm.stage[slot] = (r & off_mask) | (static_cast<unsigned long long>(s) << 32) | (local << 40);
+          } else {
+            sm.stage[slot] = kNoEntry;
+          }
+        }
+      }
+      __syncthreads();
+      // Per-shard column scan over warps, then an exclusive scan over shards.
+      for (uint32_t s = tid; s < p.shards; s += kBlock) {
+        uint32_t run = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < kWarpsPerBlock; ++w) {
+          const uint32_t c = sm.hist[w][s];
+          sm.hist[w][s] = run;
+          run += c;
+        }
+        sm.total[s] = run;
+      }
+      __syncthreads();
+      if (tid < 32) {
+        uint32_t carry = 0;
+        for (uint32_t b = 0; b < p.shards; b += 32) {
+          const uint32_t s = b + tid;
+          const uint32_t v = s < p.shards ? sm.total[s] : 0u;
+          uint32_t incl = v;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t up = __shfl_up_sync(kFullMask, incl, o);
+            if (tid >= static_cast<uint32_t>(o)) incl += up;
+          }
+          if (s < p.shards) sm.start[s] = carry + incl - v;
+          carry += __shfl_sync(kFullMask, incl, 31);
+        }
+        if (tid == 0) sm.start[p.shards] = carry;
+      }
+      for (uint32_t s = tid; s < p.shards; s += kBlock)
+        sm.gbase[s] = sm.total[s] ? atomicAdd(&p.shard_count[s], static_cast<unsigned long long>(sm.total[s])) : 0ull;
+      __syncthreads();
+      // Move own entries to registers, then scatter them into the sorted run
+      // (the run keeps offset | shard << 32).
+      unsigned long long ent[kMaxEntries];
+      uint32_t epos[kMaxEntries];
+#pragma unroll
+      for (uint32_t e = 0; e < kMaxEntries; ++e) {
+        ent[e] = kNoEntry;
+        if (e < entries) {
+          ent[e] = sm.stage[e * kBlock + tid];
+          if (ent[e] != kNoEntry) {
+            const uint32_t s = static_cast<uint32_t>(ent[e] >> 32) & 0xffu;
+            epos[e] = sm.start[s] + sm.hist[warp][s] + static_cast<uint32_t>(ent[e] >> 40);
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (uint32_t e = 0; e < kMaxEntries; ++e)
+        if (ent[e] != kNoEntry) sm.stage[epos[e]] = ent[e] & 0xffffffffffull;
+      __syncthreads();
+      const uint32_t n = sm.start[p.shards];
+      bool overflow = false;
+      for (uint32_t i = tid; i < n; i += kBlock) {
+        const unsigned long long v = sm.stage[i];
+        const uint32_t s = static_cast<uint32_t>(v >> 32);
+        const unsigned long long pos = sm.gbase[s] + (i - sm.start[s]);
+        if (pos < __ldg(&p.shard_cap[s])) p.buckets[__ldg(&p.shard_begin[s]) + pos] = static_cast<uint32_t>(v);
+        else overflow = true;
+      }
+      if (overflow) raise_error(&p.control->error, ERR_BUCKET_OVERFLOW);
+      __syncthreads();
+      for (uint32_t i = tid; i < kWarpsPerBlock * kMaxShards; i += kBlock) (&sm.hist[0][0])[i] = 0;
+      __syncthreads();
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
+  __shared__ uint32_t win[kAcceptChunk];
+  __shared__ unsigned long long item_prefix[kMaxShards + 1];
+  __shared__ uint32_t win_count;
+  __shared__ unsigned long long win_base;
+  // A routed layer whose buckets overflowed is redone by the host: leave the
+  // bitmap untouched.
+  if (*reinterpret_cast<volatile unsigned int*>(&p.control->error) & ERR_BUCKET_OVERFLOW) return;
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint32_t s = 0; s < p.shards; ++s) {
+      item_prefix[s] = run;
+      run += (p.shard_count[s] + kAcceptChunk - 1) / kAcceptChunk;
+    }
+    item_prefix[p.shards] = run;
+    win_count = 0;
+  }
+  __syncthreads();
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const unsigned long long items = item_prefix[p.shards];
+  for (unsigned long long item = blockIdx.x; item < items; item += gridDim.x) {
+    uint32_t lo = 0, hi = p.shards;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (item_prefix[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const uint32_t s = lo;
+    const unsigned long long first = (item - item_prefix[s]) * kAcceptChunk;
+    const uint32_t n = static_cast<uint32_t>(min(static_cast<unsigned long long>(kAcceptChunk), p.shard_count[s] - first));
+    const uint32_t* src = p.buckets + p.shard_begin[s] + first;
+    const uint64_t shard_base = static_cast<uint64_t>(s) << p.shift;
+    for (uint32_t round = 0; round < n; round += 8 * kBlock) {
+      uint32_t o[8];
+      unsigned long long old[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = round + k * kBlock + tid;
+        o[k] = i < n ? src[i] : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = round + k * kBlock + tid;
+        const uint64_t r = shard_base | o[k];
+        old[k] = i < n ? atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63)) : ~0ull;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const bool won = !(old[k] & (1ull << (o[k] & 63)));
+        const unsigned m = __ballot_sync(kFullMask, won);
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          uint32_t wb = 0;
+          if (static_cast<int>(lane) == leader) wb = atomicAdd(&win_count, static_cast<uint32_t>(__popc(m)));
+          wb = __shfl_sync(kFullMask, wb, leader);
+          if (won) win[wb + __popc(m & lanemask_lt())] = o[k];
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t nw = win_count;
+    if (tid == 0 && nw) win_base = atomicAdd(&p.control->next_count, static_cast<unsigned long long>(nw));
+    __syncthreads();
+    bool overflow = false;
+    for (uint32_t i = tid; i < nw; i += kBlock) {
+      const unsigned long long pos = win_base + i;
+      if (pos < p.capacity) p.next[pos] = lehmer_unrank4<N>(shard_base | win[i]);
+      else overflow = true;
+    }
+    if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
+    __syncthreads();
+    if (tid == 0) win_count = 0;
+    __syncthreads();
+  }
+}
+
+}  // namespace mgbfs2

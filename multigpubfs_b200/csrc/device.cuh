@@ -86,6 +86,41 @@ __device__ __forceinline__ uint64_t lehmer_rank4(uint64_t w) {
   return lo;
 }
 
+// Inverse of lehmer_rank4<N>: factorial-base digits (mixed radix, least
+// significant first, all divisors compile-time constants), then the c_i-th
+// unused symbol of a sorted nibble list for every position.
+template <int N>
+__device__ __forceinline__ uint64_t lehmer_unrank4(uint64_t r) {
+  constexpr int kSplit = N > 12 ? N - 12 : 0;
+  uint32_t digit[N];
+  uint32_t hi = kSplit ? static_cast<uint32_t>(r / 479001600ull) : 0u;
+  uint32_t lo = kSplit ? static_cast<uint32_t>(r - static_cast<uint64_t>(hi) * 479001600ull) : static_cast<uint32_t>(r);
+#pragma unroll
+  for (int i = N - 1; i >= kSplit; --i) {
+    digit[i] = lo % static_cast<uint32_t>(N - i);
+    lo /= static_cast<uint32_t>(N - i);
+  }
+#pragma unroll
+  for (int i = kSplit - 1; i >= 0; --i) {
+    digit[i] = hi % static_cast<uint32_t>(N - i);
+    hi /= static_cast<uint32_t>(N - i);
+  }
+  uint64_t avail = 0xfedcba9876543210ull;  // symbols still unused, ascending
+  uint64_t out = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    // symbol = nibble c of the list; delete it: the nibbles above c move down
+    // one place, the c nibbles below stay (bit-field insert of the low 4c bits).
+    const uint32_t sh = 4 * digit[i];
+    uint64_t sym, rest;
+    asm("bfe.u64 %0, %1, %2, 4;" : "=l"(sym) : "l"(avail), "r"(sh));
+    asm("bfi.b64 %0, %1, %2, 0, %3;" : "=l"(rest) : "l"(avail), "l"(avail >> 4), "r"(sh));
+    out |= sym << (4 * i);
+    avail = rest;
+  }
+  return out;
+}
+
 // Runtime-N variant for tests and rarely used sizes.
 __device__ __forceinline__ uint64_t lehmer_rank4_n(uint64_t w, uint32_t n) {
   uint64_t rank = 0;

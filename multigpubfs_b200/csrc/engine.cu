@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/mgbfs2.h"
+#include "bucket_kernels.cuh"
 #include "engine.h"
 #include "packed_kernels.cuh"
 
@@ -120,6 +121,10 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
   if (rc) { set_message(error, cap, "CUDA_SET_DEVICE"); delete g; return rc; }
   rc = cuda_status(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   if (rc) { set_message(error, cap, "CUDA_STREAM"); delete g; return rc; }
+  for (DeviceBuffer* b : {&g->bitmap, &g->front, &g->next, &g->table, &g->bank[0], &g->bank[1], &g->bank[2],
+                          &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta})
+    b->stream = g->stream;
+  retain_pool_memory(dev);
   for (cudaEvent_t* e : {&g->ev_run[0], &g->ev_run[1], &g->ev_kernel[0], &g->ev_kernel[1]}) {
     rc = cuda_status(cudaEventCreate(e));
     if (rc) { set_message(error, cap, "CUDA_EVENT"); delete g; return rc; }
@@ -349,26 +354,56 @@ void Graph::release() {
     cudaFreeHost(host_control);
     host_control = nullptr;
   }
+  buckets.free();
+  shard_meta.free();
+  if (host_meta) {
+    cudaFreeHost(host_meta);
+    host_meta = nullptr;
+  }
 }
 
+// Stream-ordered allocations from the device's default memory pool, which
+// keeps freed memory reserved (release threshold = max) so that regrowing a
+// buffer, or a new graph handle in the same process, reuses it without device
+// synchronisation.  Growth is geometric (x1.5) so a BFS regrows O(log) times.
 int DeviceBuffer::ensure(size_t want) {
   if (want <= bytes) return MGBFS2_OK;
+  const size_t grown = std::max(want, bytes + bytes / 2);
   free();
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, want);
+  cudaError_t e = cudaMallocAsync(&p, grown, stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? MGBFS2_OUT_OF_MEMORY : cuda_status(e);
   }
   ptr = p;
-  bytes = want;
+  bytes = grown;
   return MGBFS2_OK;
 }
 
 void DeviceBuffer::free() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) cudaFreeAsync(ptr, stream);
   ptr = nullptr;
   bytes = 0;
+}
+
+int retain_pool_memory(int device) {
+  cudaMemPool_t pool;
+  cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, device);
+  if (e != cudaSuccess) return cuda_status(e);
+  uint64_t threshold = UINT64_MAX;
+  return cuda_status(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+}
+
+// Bytes the pool holds reserved but unused: allocatable without new mappings.
+uint64_t pool_idle_bytes(int device) {
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return 0;
+  uint64_t reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    return 0;
+  return reserved > used ? reserved - used : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -382,6 +417,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   MG_CHECK(cudaSetDevice(device));
   size_t free_bytes = 0, total_bytes = 0;
   MG_CHECK(cudaMemGetInfo(&free_bytes, &total_bytes));
+  free_bytes += pool_idle_bytes(device);
   const uint64_t reserve = r.reserve_bytes ? r.reserve_bytes : (2ull << 30);
   if (free_bytes <= reserve) return MGBFS2_OUT_OF_MEMORY;
   const uint64_t budget = free_bytes - reserve;
@@ -416,6 +452,22 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
   if ((dedup == MGBFS2_DEDUP_SORT || dedup == MGBFS2_DEDUP_BUCKET) && !(visited == MGBFS2_VISITED_BITMAP && lehmer))
     return MGBFS2_UNSUPPORTED;
+  if (dedup == MGBFS2_DEDUP_SORT) return MGBFS2_UNSUPPORTED;
+  if (dedup == MGBFS2_DEDUP_BUCKET) {
+    // Power-of-two shard width so a rank splits into (shard, uint32 offset).
+    // Default: 4 MiB bitmap slices (2^25 bits), so the slices the resident
+    // accept blocks work on stay in L2; at most kMaxShards shards.
+    const uint64_t want = std::min<uint64_t>(
+        r.shards ? r.shards : std::max<uint64_t>(1, (rank_total + (1ull << 25) - 1) >> 25), kMaxShards);
+    uint32_t shift = 6;
+    while (((rank_total + (1ull << shift) - 1) >> shift) > want) ++shift;
+    if (shift > 32) return MGBFS2_UNSUPPORTED;
+    bucket_shift = shift;
+    bucket_shards = static_cast<uint32_t>((rank_total + (1ull << shift) - 1) >> shift);
+    p.shards = bucket_shards;
+    bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
+    bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
+  }
   p.visited = visited;
   p.dedup = dedup;
   p.history_layers = visited == MGBFS2_VISITED_HASH3 ? 3 : 1;
@@ -491,6 +543,101 @@ static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
   }
 }
 
+using RouteFn = void (*)(RouteParams);
+using AcceptFn = void (*)(AcceptParams);
+
+static void pick_bucket(uint32_t n, RouteFn* route, AcceptFn* accept) {
+  switch (n) {
+#define MG_CASE(K)               \
+  case K:                        \
+    *route = route_lehmer<K>;    \
+    *accept = accept_lehmer<K>;  \
+    return;
+    MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
+    MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
+#undef MG_CASE
+    default:
+      *route = nullptr;
+      *accept = nullptr;
+  }
+}
+
+// Per-shard bucket capacities for `work` routed successors: the previous
+// routed layer's shard distribution plus 20% and a fixed margin (uniform x2
+// before any history), or exactly the counts of the failed attempt when
+// `exact` (the redo after an overflow, which cannot overflow again).
+int Graph::bucket_setup(uint64_t work, bool exact) {
+  const uint32_t S = bucket_shards;
+  int rc = MGBFS2_OK;
+  if (!host_meta && (rc = cuda_status(cudaMallocHost(&host_meta, 3 * kMaxShards * sizeof(unsigned long long)))))
+    return rc;
+  if ((rc = shard_meta.ensure(3 * kMaxShards * sizeof(unsigned long long)))) return rc;
+  unsigned long long* begin = host_meta;
+  unsigned long long* cap = host_meta + kMaxShards;
+  const unsigned long long* counts = host_meta + 2 * kMaxShards;
+  uint64_t total = 0;
+  for (uint32_t s = 0; s < S; ++s) {
+    uint64_t c;
+    if (exact) {
+      c = counts[s];
+    } else if (shard_history_total) {
+      const double frac = static_cast<double>(shard_history[s]) / static_cast<double>(shard_history_total);
+      c = static_cast<uint64_t>(frac * static_cast<double>(work) * 1.2) + bucket_margin;
+    } else {
+      c = 2 * (work / S) + bucket_margin;
+    }
+    begin[s] = total;
+    cap[s] = c;
+    total += c;
+  }
+  if ((rc = buckets.ensure(total * sizeof(uint32_t)))) return rc;
+  MG_CHECK(cudaMemcpyAsync(shard_meta.ptr, host_meta, 2 * kMaxShards * sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice, stream));
+  MG_CHECK(cudaMemsetAsync(static_cast<unsigned long long*>(shard_meta.ptr) + 2 * kMaxShards, 0,
+                           kMaxShards * sizeof(unsigned long long), stream));
+  return MGBFS2_OK;
+}
+
+int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const ExpandParams& p, size_t smem) {
+  unsigned long long* meta = static_cast<unsigned long long*>(shard_meta.ptr);
+  RouteParams rp{};
+  rp.frontier = p.frontier;
+  rp.count = p.count;
+  rp.terms = p.terms;
+  rp.term_begin = p.term_begin;
+  rp.gens = p.gens;
+  rp.total_terms = p.total_terms;
+  // Parents per thread and generators per flush: at most kMaxEntries staged
+  // successors per thread.
+  rp.ppt = p.gens <= 3 ? 4 : (p.gens <= 6 ? 2 : 1);
+  rp.group = kMaxEntries / rp.ppt;
+  rp.shift = bucket_shift;
+  rp.shards = bucket_shards;
+  rp.buckets = static_cast<uint32_t*>(buckets.ptr);
+  rp.shard_begin = meta;
+  rp.shard_cap = meta + kMaxShards;
+  rp.shard_count = meta + 2 * kMaxShards;
+  rp.control = p.control;
+  const uint64_t tiles = (p.count + kBlock * rp.ppt - 1) / (kBlock * rp.ppt);
+  reinterpret_cast<RouteFn>(const_cast<void*>(route_fn))<<<grid_for(route_fn, smem, tiles), kBlock, smem, stream>>>(rp);
+  ++launches;
+  MG_CHECK(cudaGetLastError());
+  AcceptParams ap{};
+  ap.buckets = static_cast<const uint32_t*>(buckets.ptr);
+  ap.shard_begin = meta;
+  ap.shard_count = meta + 2 * kMaxShards;
+  ap.shards = bucket_shards;
+  ap.shift = bucket_shift;
+  ap.bitmap = p.bitmap;
+  ap.next = p.next;
+  ap.capacity = p.capacity;
+  ap.control = p.control;
+  reinterpret_cast<AcceptFn>(const_cast<void*>(accept_fn))<<<grid_for(accept_fn, 0, UINT32_MAX), kBlock, 0, stream>>>(ap);
+  ++launches;
+  MG_CHECK(cudaGetLastError());
+  return MGBFS2_OK;
+}
+
 int Graph::visit_kind() const {
   if (plan.visited == MGBFS2_VISITED_BITMAP) return (lehmer && elements >= 2) ? V_LEHMER : V_MULTISET;
   return plan.visited == MGBFS2_VISITED_HASH ? V_HASH : V_HASH3;
@@ -528,14 +675,26 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   mgbfs2_status st{};
   layer_sizes.assign(1, 1);
   layer_seconds.clear();
-  small_layer.clear();
-  small_depth = UINT32_MAX;
+  for (int i = 0; i < 2; ++i) {
+    small_layer[i].clear();
+    small_depth[i] = UINT32_MAX;
+  }
   launches = 0;
   const auto started = Clock::now();
   const int visit = visit_kind();
   const bool warp = plan.dedup == MGBFS2_DEDUP_WARP;
   ExpandFn fn = pick_expand(visit, warp, elements);
   if (!fn) return MGBFS2_UNSUPPORTED;
+  // Bucketed layers for large frontiers; small layers use the fused kernel.
+  const bool bucketed = plan.dedup == MGBFS2_DEDUP_BUCKET && visit == V_LEHMER;
+  RouteFn route_fn = nullptr;
+  AcceptFn accept_fn = nullptr;
+  if (bucketed) {
+    pick_bucket(elements, &route_fn, &accept_fn);
+    if (!route_fn) return MGBFS2_UNSUPPORTED;
+  }
+  shard_history.assign(bucket_shards, 0);
+  shard_history_total = 0;
 
   ExpandParams p{};
   p.terms = static_cast<const Term*>(program.ptr);
@@ -590,8 +749,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   uint64_t count = 1, visited = 1;
   uint32_t depth = 0;
   if (count < 1000) {
-    small_layer.assign(1, start_word);
-    small_depth = 0;
+    keep_small(0, std::vector<uint64_t>(1, start_word));
   }
   uint64_t peak = plan.device_bytes;
   st.reason = MGBFS2_REASON_FRONTIER_EXHAUSTED;
@@ -618,6 +776,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       if (need > table_slots / 2) {
         const uint64_t slots = next_pow2(2 * need);
         DeviceBuffer grown;
+        grown.stream = stream;
         if ((rc = grown.ensure(slots * 8))) break;
         MG_CHECK(cudaMemsetAsync(grown.ptr, 0xff, slots * 8, stream));
         rehash_table<<<grid_for(reinterpret_cast<const void*>(rehash_table), 0, (table_slots + kBlock - 1) / kBlock),
@@ -649,19 +808,40 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       p.look1 = depth >= 1 ? static_cast<const unsigned long long*>(bank[prev].ptr) : nullptr;
       p.look1_mask = depth >= 1 ? bank_slots[prev] - 1 : 0;
     }
-    MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
-    const uint64_t tiles = (count + kBlock * p.ppt - 1) / (kBlock * p.ppt);
-    const uint32_t grid = grid_for(reinterpret_cast<const void*>(fn), smem, tiles);
-    MG_CHECK(cudaEventRecord(ev_kernel[0], stream));
-    fn<<<grid, kBlock, smem, stream>>>(p);
-    ++launches;
-    MG_CHECK(cudaGetLastError());
-    MG_CHECK(cudaEventRecord(ev_kernel[1], stream));
-    MG_CHECK(cudaMemcpyAsync(host_control, control_buf.ptr, sizeof(Control), cudaMemcpyDeviceToHost, stream));
-    MG_CHECK(cudaStreamSynchronize(stream));
-    {
+    const uint64_t work = count * gens;
+    const bool routed = bucketed && work >= bucket_min_work;
+    // One attempt; a routed layer whose shard buckets overflowed left the
+    // bitmap untouched and is redone once with the exact shard counts.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
+      if (routed && (rc = bucket_setup(work, attempt == 1))) break;
+      MG_CHECK(cudaEventRecord(ev_kernel[0], stream));
+      if (routed) {
+        if ((rc = bucket_launch(reinterpret_cast<const void*>(route_fn), reinterpret_cast<const void*>(accept_fn), p,
+                                smem)))
+          break;
+      } else {
+        const uint64_t tiles = (count + kBlock * p.ppt - 1) / (kBlock * p.ppt);
+        const uint32_t grid = grid_for(reinterpret_cast<const void*>(fn), smem, tiles);
+        fn<<<grid, kBlock, smem, stream>>>(p);
+        ++launches;
+        MG_CHECK(cudaGetLastError());
+      }
+      MG_CHECK(cudaEventRecord(ev_kernel[1], stream));
+      MG_CHECK(cudaMemcpyAsync(host_control, control_buf.ptr, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+      if (routed)
+        MG_CHECK(cudaMemcpyAsync(host_meta + 2 * kMaxShards, static_cast<unsigned long long*>(shard_meta.ptr) + 2 * kMaxShards,
+                                 bucket_shards * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+      MG_CHECK(cudaStreamSynchronize(stream));
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ev_kernel[0], ev_kernel[1]) == cudaSuccess) kernel_seconds += ms * 1e-3;
+      if (!(routed && host_control->error == ERR_BUCKET_OVERFLOW)) break;
+      ++st.redo_layers;
+    }
+    if (rc) break;
+    if (routed && !host_control->error) {
+      shard_history.assign(host_meta + 2 * kMaxShards, host_meta + 2 * kMaxShards + bucket_shards);
+      shard_history_total = work;
     }
     st.successors += count * gens;
     const Control c = *host_control;
@@ -689,9 +869,10 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     visited += count;
     ++depth;
     if (count < 1000) {
-      small_layer.resize(count);
-      MG_CHECK(cudaMemcpy(small_layer.data(), front.ptr, count * 8, cudaMemcpyDeviceToHost));
-      small_depth = depth;
+      std::vector<uint64_t> words(count);
+      MG_CHECK(cudaMemcpyAsync(words.data(), front.ptr, count * 8, cudaMemcpyDeviceToHost, stream));
+      MG_CHECK(cudaStreamSynchronize(stream));
+      keep_small(depth, std::move(words));
     }
     if (cb && cb(user, depth, count, secs)) {
       st.reason = MGBFS2_REASON_CANCELLED;
@@ -713,6 +894,15 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   return rc;
 }
 
+// Small layers are copied to the host as they complete so that the
+// "previous_small" sample survives the frontier buffers being reused.
+void Graph::keep_small(uint32_t depth, std::vector<uint64_t>&& words) {
+  small_layer[1] = std::move(small_layer[0]);
+  small_depth[1] = small_depth[0];
+  small_layer[0] = std::move(words);
+  small_depth[0] = depth;
+}
+
 std::vector<int64_t> Graph::decode(uint64_t w) const {
   std::vector<int64_t> row(elements);
   const uint64_t mask = bits == 64 ? ~0ull : ((1ull << bits) - 1);
@@ -730,10 +920,15 @@ int Graph::sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* rows) {
   if (which == 0) {
     const uint64_t n = std::min<uint64_t>(last_count, cap_rows);
     words.resize(n);
-    if (n) MG_CHECK(cudaMemcpy(words.data(), front.ptr, n * 8, cudaMemcpyDeviceToHost));
+    if (n) {
+      MG_CHECK(cudaMemcpyAsync(words.data(), front.ptr, n * 8, cudaMemcpyDeviceToHost, stream));
+      MG_CHECK(cudaStreamSynchronize(stream));
+    }
   } else {
-    if (deepest == 0 || small_depth != deepest - 1 || layer_sizes[deepest - 1] >= 1000) return MGBFS2_OK;
-    words.assign(small_layer.begin(), small_layer.begin() + std::min<size_t>(small_layer.size(), cap_rows));
+    if (deepest == 0 || layer_sizes[deepest - 1] >= 1000) return MGBFS2_OK;
+    const int k = small_depth[0] == deepest - 1 ? 0 : (small_depth[1] == deepest - 1 ? 1 : -1);
+    if (k < 0) return MGBFS2_OK;
+    words.assign(small_layer[k].begin(), small_layer[k].begin() + std::min<size_t>(small_layer[k].size(), cap_rows));
   }
   std::vector<std::vector<int64_t>> decoded;
   for (uint64_t w : words) decoded.push_back(decode(w));

@@ -12,15 +12,21 @@ namespace mgbfs2 {
 
 int cuda_status(cudaError_t e);
 
-// A plain device allocation that only grows.  No destructor: owners call free().
+// A device allocation that only grows, ordered on its owner's stream.  No
+// destructor: owners call free().
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
+  cudaStream_t stream = nullptr;
   int ensure(size_t want);
   void free();
 };
 
-struct WideState;  // int64-key arena path (wide.cu)
+int retain_pool_memory(int device);
+uint64_t pool_idle_bytes(int device);
+
+struct WideState;     // int64-key arena path (wide.cu)
+struct ExpandParams;  // packed_kernels.cuh
 
 struct Graph {
   // Description.
@@ -55,11 +61,23 @@ struct Graph {
   Control* host_control = nullptr;
   WideState* wide = nullptr;
 
+  // Bucketed (owner-routed) bitmap layers: shard s holds ranks
+  // [s << bucket_shift, (s + 1) << bucket_shift).
+  uint32_t bucket_shift = 0, bucket_shards = 0;
+  uint64_t bucket_margin = 4096, bucket_min_work = 1ull << 22;
+  DeviceBuffer buckets, shard_meta;            // uint32 offsets; begin/cap/count per shard
+  unsigned long long* host_meta = nullptr;     // pinned: begin, cap, count (3 x kMaxShards)
+  std::vector<uint64_t> shard_history;         // last routed layer's per-shard counts
+  uint64_t shard_history_total = 0;
+  int bucket_setup(uint64_t work, bool exact);
+  int bucket_launch(const void* route, const void* accept, const ExpandParams& p, size_t smem);
+
   // Results.
   std::vector<uint64_t> layer_sizes;
   std::vector<double> layer_seconds;
-  std::vector<uint64_t> small_layer;  // the most recent layer with < 1000 states
-  uint32_t small_depth = UINT32_MAX;
+  std::vector<uint64_t> small_layer[2];  // the two most recent layers with < 1000 states
+  uint32_t small_depth[2] = {UINT32_MAX, UINT32_MAX};
+  void keep_small(uint32_t depth, std::vector<uint64_t>&& words);
   uint64_t last_count = 0;
   uint32_t launches = 0;
 

@@ -180,7 +180,11 @@ int Graph::wide_plan(mgbfs2_plan_info* p, uint64_t budget) {
   p->visited = MGBFS2_VISITED_HASH;
   p->history_layers = 1;
   p->dedup = MGBFS2_DEDUP_ATOMIC;
-  if (!wide) wide = new WideState();
+  if (!wide) {
+    wide = new WideState();
+    for (DeviceBuffer* b : {&wide->arena, &wide->table, &wide->perms, &wide->mats, &wide->mods, &wide->counters})
+      b->stream = stream;
+  }
   WideState& w = *wide;
   w.K = wide_key_words();
   w.bits = 64;
@@ -212,15 +216,17 @@ int Graph::wide_plan(mgbfs2_plan_info* p, uint64_t budget) {
   int rc = MGBFS2_OK;
   if (kind == 0) {
     if ((rc = w.perms.ensure(perms.size() * 4 + 4))) return rc;
-    if (cudaMemcpy(w.perms.ptr, perms.data(), perms.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(w.perms.ptr, perms.data(), perms.size() * 4, cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return MGBFS2_CUDA_BASE;
   } else {
     if ((rc = w.mats.ensure(matrices.size() * 8 + 8)) || (rc = w.mods.ensure(moduli.size() * 4 + 4))) return rc;
-    if (cudaMemcpy(w.mats.ptr, matrices.data(), matrices.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(w.mods.ptr, moduli.data(), moduli.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(w.mats.ptr, matrices.data(), matrices.size() * 8, cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(w.mods.ptr, moduli.data(), moduli.size() * 4, cudaMemcpyHostToDevice, stream) != cudaSuccess)
       return MGBFS2_CUDA_BASE;
   }
-  return w.counters.ensure(16);
+  if ((rc = w.counters.ensure(16))) return rc;
+  return cuda_status(cudaStreamSynchronize(stream));
 }
 
 int Graph::wide_run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status) {
@@ -269,6 +275,7 @@ int Graph::wide_run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, v
     if (visited + bound > w.arena_rows) {
       const uint64_t rows = std::max<uint64_t>(visited + bound, 2 * w.arena_rows);
       DeviceBuffer grown;
+      grown.stream = stream;
       if ((rc = grown.ensure(rows * w.K * 8))) break;
       if (cudaMemcpyAsync(grown.ptr, w.arena.ptr, visited * w.K * 8, cudaMemcpyDeviceToDevice, stream) != cudaSuccess) {
         grown.free();
@@ -370,8 +377,9 @@ int Graph::wide_sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* ro
   }
   const uint64_t n = std::min<uint64_t>(count, cap_rows);
   std::vector<uint64_t> raw(n * w.K);
-  if (n && cudaMemcpy(raw.data(), static_cast<uint64_t*>(w.arena.ptr) + begin * w.K, n * w.K * 8,
-                      cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (n && (cudaMemcpyAsync(raw.data(), static_cast<uint64_t*>(w.arena.ptr) + begin * w.K, n * w.K * 8,
+                            cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess))
     return MGBFS2_CUDA_BASE;
   std::vector<std::vector<int64_t>> decoded(n, std::vector<int64_t>(elements));
   for (uint64_t r = 0; r < n; ++r) {

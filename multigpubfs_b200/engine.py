@@ -90,8 +90,10 @@ class NativeGraph:
         self.close()
 
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
-             planner="plain") -> dict:
+             planner="plain", bucket_margin=None, bucket_min_work=None) -> dict:
         req = native.PlanRequest()
+        req.bucket_margin = 0 if bucket_margin is None else (0xFFFFFFFF if bucket_margin == 0 else bucket_margin)
+        req.bucket_min_work = bucket_min_work or 0
         req.visited = native.VISITED[visited]
         req.dedup = native.DEDUP[dedup]
         req.capacity = capacity or 0

@@ -48,7 +48,7 @@ class GraphDesc(C.Structure):
 class PlanRequest(C.Structure):
     _fields_ = [("visited", C.c_uint32), ("dedup", C.c_uint32), ("capacity", C.c_uint64),
                 ("reserve_bytes", C.c_uint64), ("shards", C.c_uint32), ("block", C.c_uint32),
-                ("planner", C.c_uint32), ("reserved", C.c_uint32)]
+                ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64)]
 
 
 class PlanInfo(C.Structure):

@@ -143,7 +143,8 @@ def test_sort_unique_tiles(key_bits):
     rng = np.random.default_rng(key_bits)
     count = 4096 * 5 + 123
     raw = rng.integers(0, 1 << min(key_bits, 62), size=count, dtype=np.int64)
-    raw[::7] = raw[::11][: len(raw[::7])]  # plenty of duplicates
+    idx = rng.integers(1, count, size=count // 3)
+    raw[idx] = raw[idx - 1]  # plenty of duplicates inside each tile
     keys = torch.tensor(raw, device="cuda")
     out, counts = sort_unique_tiles(keys, key_bits)
     out = out.cpu().numpy()

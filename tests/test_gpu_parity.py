@@ -42,6 +42,10 @@ VARIANTS = {
     "bitmap_warp": dict(visited="bitmap", dedup="warp"),
     "hash": dict(visited="hash"),
     "hash3": dict(visited="hash3"),
+    # every layer routed through the shard buckets
+    "bitmap_bucket": dict(visited="bitmap", dedup="bucket", bucket_min_work=1),
+    # no bucket slack: first attempts overflow and are redone with exact counts
+    "bitmap_bucket_tight": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, bucket_margin=0),
 }
 
 
@@ -83,22 +87,37 @@ def test_golden_cases(exact_cases, variant):
     assert ran >= 8
 
 
-@pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3"])
+@pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3", "bitmap_bucket",
+                                     "bitmap_bucket_tight"])
 def test_lrx_small(lrx_layers, variant):
+    redo = 0
     for n in range(3, 12):
         out = run(G.permutation_graph(G.lrx_generators(n), list(range(n))), **VARIANTS[variant])
         assert out is not None
         assert out[1].layer_sizes == lrx_layers[n], (n, variant)
+        redo += out[1].redo_layers
+    if variant == "bitmap_bucket_tight":
+        assert redo > 0  # the exact redo path ran and changed nothing
 
 
-@pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic"])
+@pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic", "bitmap_bucket_default"])
 def test_lrx13_full_table(lrx13, variant):
-    out = run(G.permutation_graph(G.lrx_generators(13), list(range(13))), **VARIANTS[variant])
+    plan = VARIANTS.get(variant, dict(visited="bitmap", dedup="bucket"))
+    out = run(G.permutation_graph(G.lrx_generators(13), list(range(13))), **plan)
     info, r, last, prev = out
     assert info["visited"] == "bitmap"
     assert r.layer_sizes == lrx13
     # The deepest layer of S13 LRX is a single state; the one before holds 3.
-    assert len(last) == 1 and len(prev) == 3
+    assert len(last) == 1 and len(prev) == 3 and len(set(map(tuple, prev))) == 3
+    assert sorted(last[0]) == list(range(13))
+
+
+@pytest.mark.parametrize("n", [12, 13])
+def test_coxeter_bucketed(n):
+    out = run(G.permutation_graph(G.coxeter_generators(n), list(range(n))), visited="bitmap", dedup="bucket")
+    assert out[1].layer_sizes == G.coxeter_layers(n)
+    # The deepest Coxeter layer is the single longest element (the reversal).
+    assert out[2] == [list(range(n))[::-1]]
 
 
 def test_lrx12_three_bank_hash():
