@@ -1,22 +1,28 @@
 // Owner routing inside one GPU: the two-kernel bucketed layer expansion of
 // the Lehmer-bitmap path.
 //
-//   route  : parent -> successors -> Lehmer rank r -> shard s = r >> shift,
-//            offset o = r & mask (uint32).  Every thread stages its (at most
-//            kMaxEntries) entries in its own shared-memory slots and counts
-//            them in its warp's private shard histogram; one block-wide scan
-//            turns (shard, warp, lane-rank) into a position of the block's
-//            shard-sorted run, one global atomicAdd per shard reserves the
-//            bucket range, and the runs are written out coalesced.  No
-//            visited-set access.
-//   accept : work items = fixed-size chunks of the shard buckets in
-//            shard-major order, so the blocks resident at any moment all hit
-//            the same ~2^shift-bit bitmap slice, which stays in L2.  Each
-//            offset is one test-and-set (eight in flight per thread); winners
-//            are compacted first and then unranked densely into the next
-//            frontier with one reservation per work item.
+// Shards are rank ranges fixed by the first `prefix` positions of the state:
+// all permutations that start with the same k symbols occupy one contiguous
+// block of (N-k)! Lehmer ranks, so
+//     shard(state) = Horner of the first k Lehmer digits   (k cheap steps)
+// and shard s owns bitmap bits [s * (N-k)!, (s + 1) * (N-k)!).  k is chosen so
+// a shard's slice is a few MiB.
 //
-// The visited test thus costs 4 B written + 4 B read of streaming bucket
+//   route  : parent -> successors (packed words) -> shard.  Every thread stages
+//            its (at most kMaxEntries) successors in its own shared-memory
+//            slots and counts them in its warp's shard histogram; one block
+//            scan turns (shard, warp, rank-in-warp) into a position of the
+//            block's shard-sorted run; one global atomicAdd per shard reserves
+//            the bucket range; runs are written out coalesced.  No rank, no
+//            visited-set access.
+//   accept : work items = fixed-size chunks of the shard buckets, claimed in
+//            shard-major order from a device-wide counter, so all resident
+//            blocks work on the same one or two slices, which stay in L2.  Each
+//            state is ranked and test-and-set (eight in flight per thread);
+//            the winners -- already packed states -- are block-compacted and
+//            appended to the next frontier with one reservation per item.
+//
+// The visited test thus costs 8 B written + 8 B read of streaming bucket
 // traffic per successor plus L2-resident atomics, instead of a random DRAM
 // sector read-modify-write (the reference routes by owner and claims with
 // random atomics: cuda/permutation_bitmap.cu:27-48 and :105-205).
@@ -34,15 +40,16 @@ constexpr uint32_t kMaxEntries = 12;                 // staged successors per th
 constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kStageCap = kBlock * kMaxEntries;  // 3072
 constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per accept work item
+constexpr uint32_t kNoEntry = 0xffffffffu;
 
 struct RouteParams {
   const unsigned long long* frontier;
   unsigned long long count;
   const Term* terms;
   const uint32_t* term_begin;
-  uint32_t gens, total_terms, ppt, shift;
-  uint32_t shards, group;                  // group: generators per flush (group * ppt <= kMaxEntries)
-  uint32_t* buckets;                       // all shards, shard s at [begin[s], begin[s] + cap[s])
+  uint32_t gens, total_terms, ppt, group;  // group: generators per flush (group * ppt <= kMaxEntries)
+  uint32_t shards, prefix;                 // shard = Horner of the first `prefix` Lehmer digits
+  unsigned long long* buckets;             // all shards, shard s at [begin[s], begin[s] + cap[s])
   const unsigned long long* shard_begin;   // per shard
   const unsigned long long* shard_cap;     // per shard
   unsigned long long* shard_count;         // per shard, exact
@@ -50,41 +57,52 @@ struct RouteParams {
 };
 
 struct AcceptParams {
-  const uint32_t* buckets;
+  const unsigned long long* buckets;
   const unsigned long long* shard_begin;
   const unsigned long long* shard_count;
-  uint32_t shards, shift;
+  uint32_t shards, pad;
   unsigned long long* bitmap;
   unsigned long long* next;
   unsigned long long capacity;
+  unsigned long long* work;                // device work-item counter, zero at launch
   Control* control;
 };
 
-// One staged entry: offset | shard << 32 | rank-within-warp-and-shard << 40;
-// kNoEntry marks an empty slot.
-constexpr unsigned long long kNoEntry = ~0ull;
-
+// Dynamic shared memory of route_lehmer (after the generator program).
 struct RouteSmem {
-  // Staging, slot [e][thread]; reused as the block's shard-sorted run.
-  unsigned long long stage[kStageCap];
+  unsigned long long state[kStageCap];        // staged successors, slot [e][thread]; then the sorted run
+  uint32_t tag[kStageCap];                    // shard | rank-in-warp-and-shard << 8; then the run's shard
   uint32_t hist[kWarpsPerBlock][kMaxShards];  // per-warp counts, then per-warp exclusive offsets
   uint32_t total[kMaxShards];
   uint32_t start[kMaxShards + 1];             // start of shard s in the sorted run
   unsigned long long gbase[kMaxShards];       // reserved bucket position of the run
 };
 
-template <int N>
+// Shard of a packed permutation of N distinct 4-bit codes: the first K Lehmer
+// digits in mixed radix N, N-1, ..., N-K+1.
+template <int N, int K>
+__device__ __forceinline__ uint32_t prefix_shard(uint64_t w) {
+  uint32_t used = 0, shard = 0;
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const uint32_t s = static_cast<uint32_t>(w >> (4 * i)) & 15u;
+    shard = shard * static_cast<uint32_t>(N - i) + (s - __popc(used & ((1u << s) - 1u)));
+    used |= 1u << s;
+  }
+  return shard;
+}
+
+template <int N, int K>
 __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
-  extern __shared__ __align__(16) unsigned char program_smem[];
-  __shared__ RouteSmem sm;
-  Term* terms = reinterpret_cast<Term*>(program_smem);
-  uint32_t* tbegin = reinterpret_cast<uint32_t*>(program_smem + p.total_terms * sizeof(Term));
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  RouteSmem& sm = *reinterpret_cast<RouteSmem*>(dyn_smem);
+  Term* terms = reinterpret_cast<Term*>(dyn_smem + sizeof(RouteSmem));
+  uint32_t* tbegin = reinterpret_cast<uint32_t*>(dyn_smem + sizeof(RouteSmem) + p.total_terms * sizeof(Term));
   for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
   for (uint32_t i = threadIdx.x; i <= p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
   for (uint32_t i = threadIdx.x; i < kWarpsPerBlock * kMaxShards; i += blockDim.x) (&sm.hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  const uint64_t off_mask = (1ull << p.shift) - 1;
   const uint32_t tile = kBlock * p.ppt;
   const unsigned long long tiles = (p.count + tile - 1) / tile;
   for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
@@ -116,7 +134,7 @@ __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
     for (uint32_t g0 = 0; g0 < p.gens; g0 += p.group) {
       const uint32_t g1 = min(p.gens, g0 + p.group);
       const uint32_t entries = (g1 - g0) * p.ppt;
-      // Produce: rank every successor, count it in the warp's histogram.
+      // Produce: successor, its shard, its rank within (warp, shard).
       for (uint32_t g = g0; g < g1; ++g) {
         const uint32_t tb = tbegin[g], te = tbegin[g + 1];
 #pragma unroll
@@ -124,12 +142,12 @@ __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
           if (k >= static_cast<int>(p.ppt)) break;
           const uint32_t slot = ((g - g0) * p.ppt + k) * kBlock + tid;
           if (val[k]) {
-            const uint64_t r = lehmer_rank4<N>(apply_terms(par[k], terms, tb, te));
-            const uint32_t s = static_cast<uint32_t>(r >> p.shift);
-            const unsigned long long local = atomicAdd(&sm.hist[warp][s], 1u);
-            sm.stage[slot] = (r & off_mask) | (static_cast<unsigned long long>(s) << 32) | (local << 40);
+            const uint64_t c = apply_terms(par[k], terms, tb, te);
+            const uint32_t s = prefix_shard<N, K>(c);
+            sm.state[slot] = c;
+            sm.tag[slot] = s | (atomicAdd(&sm.hist[warp][s], 1u) << 8);
           } else {
-            sm.stage[slot] = kNoEntry;
+            sm.tag[slot] = kNoEntry;
           }
         }
       }
@@ -165,33 +183,37 @@ __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
       for (uint32_t s = tid; s < p.shards; s += kBlock)
         sm.gbase[s] = sm.total[s] ? atomicAdd(&p.shard_count[s], static_cast<unsigned long long>(sm.total[s])) : 0ull;
       __syncthreads();
-      // Move own entries to registers, then scatter them into the sorted run
-      // (the run keeps offset | shard << 32).
-      unsigned long long ent[kMaxEntries];
-      uint32_t epos[kMaxEntries];
+      // Own entries to registers, then scatter them into the sorted run.
+      unsigned long long st[kMaxEntries];
+      uint32_t tg[kMaxEntries], pos[kMaxEntries];
 #pragma unroll
       for (uint32_t e = 0; e < kMaxEntries; ++e) {
-        ent[e] = kNoEntry;
+        tg[e] = kNoEntry;
         if (e < entries) {
-          ent[e] = sm.stage[e * kBlock + tid];
-          if (ent[e] != kNoEntry) {
-            const uint32_t s = static_cast<uint32_t>(ent[e] >> 32) & 0xffu;
-            epos[e] = sm.start[s] + sm.hist[warp][s] + static_cast<uint32_t>(ent[e] >> 40);
+          const uint32_t slot = e * kBlock + tid;
+          tg[e] = sm.tag[slot];
+          st[e] = sm.state[slot];
+          if (tg[e] != kNoEntry) {
+            const uint32_t s = tg[e] & 0xffu;
+            pos[e] = sm.start[s] + sm.hist[warp][s] + (tg[e] >> 8);
           }
         }
       }
       __syncthreads();
 #pragma unroll
-      for (uint32_t e = 0; e < kMaxEntries; ++e)
-        if (ent[e] != kNoEntry) sm.stage[epos[e]] = ent[e] & 0xffffffffffull;
+      for (uint32_t e = 0; e < kMaxEntries; ++e) {
+        if (tg[e] != kNoEntry) {
+          sm.state[pos[e]] = st[e];
+          sm.tag[pos[e]] = tg[e] & 0xffu;
+        }
+      }
       __syncthreads();
       const uint32_t n = sm.start[p.shards];
       bool overflow = false;
       for (uint32_t i = tid; i < n; i += kBlock) {
-        const unsigned long long v = sm.stage[i];
-        const uint32_t s = static_cast<uint32_t>(v >> 32);
-        const unsigned long long pos = sm.gbase[s] + (i - sm.start[s]);
-        if (pos < __ldg(&p.shard_cap[s])) p.buckets[__ldg(&p.shard_begin[s]) + pos] = static_cast<uint32_t>(v);
+        const uint32_t s = sm.tag[i];
+        const unsigned long long at = sm.gbase[s] + (i - sm.start[s]);
+        if (at < __ldg(&p.shard_cap[s])) p.buckets[__ldg(&p.shard_begin[s]) + at] = sm.state[i];
         else overflow = true;
       }
       if (overflow) raise_error(&p.control->error, ERR_BUCKET_OVERFLOW);
@@ -204,8 +226,9 @@ __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
 
 template <int N>
 __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
-  __shared__ uint32_t win[kAcceptChunk];
+  __shared__ unsigned long long win[kAcceptChunk];
   __shared__ unsigned long long item_prefix[kMaxShards + 1];
+  __shared__ unsigned long long item_s;
   __shared__ uint32_t win_count;
   __shared__ unsigned long long win_base;
   // A routed layer whose buckets overflowed is redone by the host: leave the
@@ -223,7 +246,12 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
   __syncthreads();
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const unsigned long long items = item_prefix[p.shards];
-  for (unsigned long long item = blockIdx.x; item < items; item += gridDim.x) {
+  for (;;) {
+    // Items are claimed in shard-major order by all blocks together.
+    if (tid == 0) item_s = atomicAdd(p.work, 1ull);
+    __syncthreads();
+    const unsigned long long item = item_s;
+    if (item >= items) break;
     uint32_t lo = 0, hi = p.shards;
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
@@ -233,32 +261,31 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
     const uint32_t s = lo;
     const unsigned long long first = (item - item_prefix[s]) * kAcceptChunk;
     const uint32_t n = static_cast<uint32_t>(min(static_cast<unsigned long long>(kAcceptChunk), p.shard_count[s] - first));
-    const uint32_t* src = p.buckets + p.shard_begin[s] + first;
-    const uint64_t shard_base = static_cast<uint64_t>(s) << p.shift;
+    const unsigned long long* src = p.buckets + p.shard_begin[s] + first;
     for (uint32_t round = 0; round < n; round += 8 * kBlock) {
-      uint32_t o[8];
-      unsigned long long old[8];
+      unsigned long long w[8], old[8];
+      uint64_t r[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = round + k * kBlock + tid;
-        o[k] = i < n ? src[i] : 0u;
+        w[k] = i < n ? src[i] : 0ull;
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = round + k * kBlock + tid;
-        const uint64_t r = shard_base | o[k];
-        old[k] = i < n ? atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63)) : ~0ull;
+        r[k] = lehmer_rank4<N>(w[k]);
+        old[k] = i < n ? atomicOr(&p.bitmap[r[k] >> 6], 1ull << (r[k] & 63)) : ~0ull;
       }
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        const bool won = !(old[k] & (1ull << (o[k] & 63)));
+        const bool won = !(old[k] & (1ull << (r[k] & 63)));
         const unsigned m = __ballot_sync(kFullMask, won);
         if (m) {
           const int leader = __ffs(m) - 1;
           uint32_t wb = 0;
           if (static_cast<int>(lane) == leader) wb = atomicAdd(&win_count, static_cast<uint32_t>(__popc(m)));
           wb = __shfl_sync(kFullMask, wb, leader);
-          if (won) win[wb + __popc(m & lanemask_lt())] = o[k];
+          if (won) win[wb + __popc(m & lanemask_lt())] = w[k];
         }
       }
     }
@@ -268,14 +295,13 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
     __syncthreads();
     bool overflow = false;
     for (uint32_t i = tid; i < nw; i += kBlock) {
-      const unsigned long long pos = win_base + i;
-      if (pos < p.capacity) p.next[pos] = lehmer_unrank4<N>(shard_base | win[i]);
+      const unsigned long long at = win_base + i;
+      if (at < p.capacity) p.next[at] = win[i];
       else overflow = true;
     }
     if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
     __syncthreads();
     if (tid == 0) win_count = 0;
-    __syncthreads();
   }
 }
 

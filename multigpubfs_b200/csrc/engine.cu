@@ -454,16 +454,19 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     return MGBFS2_UNSUPPORTED;
   if (dedup == MGBFS2_DEDUP_SORT) return MGBFS2_UNSUPPORTED;
   if (dedup == MGBFS2_DEDUP_BUCKET) {
-    // Power-of-two shard width so a rank splits into (shard, uint32 offset).
-    // Default: 4 MiB bitmap slices (2^25 bits), so the slices the resident
-    // accept blocks work on stay in L2; at most kMaxShards shards.
-    const uint64_t want = std::min<uint64_t>(
-        r.shards ? r.shards : std::max<uint64_t>(1, (rank_total + (1ull << 25) - 1) >> 25), kMaxShards);
-    uint32_t shift = 6;
-    while (((rank_total + (1ull << shift) - 1) >> shift) > want) ++shift;
-    if (shift > 32) return MGBFS2_UNSUPPORTED;
-    bucket_shift = shift;
-    bucket_shards = static_cast<uint32_t>((rank_total + (1ull << shift) - 1) >> shift);
+    // Shards = states sharing their first K symbols: N!/(N-K)! shards whose
+    // bitmap slices hold (N-K)! bits.  Default: the smallest K (1 or 2) whose
+    // slice is at most 8 MiB, so the slices the resident accept blocks work
+    // on stay in L2; a requested shard count picks K = 2 when N < shards.
+    const uint32_t n = elements;
+    uint64_t fact[17] = {1};
+    for (uint32_t i = 1; i <= 16; ++i) fact[i] = fact[i - 1] * i;
+    uint32_t K = 1;
+    if (r.shards) K = (n < r.shards && n * (n - 1) <= kMaxShards) ? 2 : 1;
+    else if (fact[n - 1] / 8 > (8ull << 20) && n * (n - 1) <= kMaxShards) K = 2;
+    if (n < 2 || fact[n] / fact[n - K] > kMaxShards) return MGBFS2_UNSUPPORTED;
+    bucket_prefix = K;
+    bucket_shards = static_cast<uint32_t>(fact[n] / fact[n - K]);
     p.shards = bucket_shards;
     bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
     bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
@@ -546,12 +549,12 @@ static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
 using RouteFn = void (*)(RouteParams);
 using AcceptFn = void (*)(AcceptParams);
 
-static void pick_bucket(uint32_t n, RouteFn* route, AcceptFn* accept) {
+static void pick_bucket(uint32_t n, uint32_t prefix, RouteFn* route, AcceptFn* accept) {
   switch (n) {
-#define MG_CASE(K)               \
-  case K:                        \
-    *route = route_lehmer<K>;    \
-    *accept = accept_lehmer<K>;  \
+#define MG_CASE(K)                                                       \
+  case K:                                                                \
+    *route = prefix == 1 ? route_lehmer<K, 1> : route_lehmer<K, 2>;      \
+    *accept = accept_lehmer<K>;                                          \
     return;
     MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
     MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
@@ -569,9 +572,9 @@ static void pick_bucket(uint32_t n, RouteFn* route, AcceptFn* accept) {
 int Graph::bucket_setup(uint64_t work, bool exact) {
   const uint32_t S = bucket_shards;
   int rc = MGBFS2_OK;
-  if (!host_meta && (rc = cuda_status(cudaMallocHost(&host_meta, 3 * kMaxShards * sizeof(unsigned long long)))))
-    return rc;
-  if ((rc = shard_meta.ensure(3 * kMaxShards * sizeof(unsigned long long)))) return rc;
+  const size_t meta_bytes = (3 * kMaxShards + 1) * sizeof(unsigned long long);
+  if (!host_meta && (rc = cuda_status(cudaMallocHost(&host_meta, meta_bytes)))) return rc;
+  if ((rc = shard_meta.ensure(meta_bytes))) return rc;
   unsigned long long* begin = host_meta;
   unsigned long long* cap = host_meta + kMaxShards;
   const unsigned long long* counts = host_meta + 2 * kMaxShards;
@@ -590,11 +593,12 @@ int Graph::bucket_setup(uint64_t work, bool exact) {
     cap[s] = c;
     total += c;
   }
-  if ((rc = buckets.ensure(total * sizeof(uint32_t)))) return rc;
+  if ((rc = buckets.ensure(total * sizeof(unsigned long long)))) return rc;
   MG_CHECK(cudaMemcpyAsync(shard_meta.ptr, host_meta, 2 * kMaxShards * sizeof(unsigned long long),
                            cudaMemcpyHostToDevice, stream));
+  // Zero the shard counts and the accept work counter.
   MG_CHECK(cudaMemsetAsync(static_cast<unsigned long long*>(shard_meta.ptr) + 2 * kMaxShards, 0,
-                           kMaxShards * sizeof(unsigned long long), stream));
+                           (kMaxShards + 1) * sizeof(unsigned long long), stream));
   return MGBFS2_OK;
 }
 
@@ -611,23 +615,26 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   // successors per thread.
   rp.ppt = p.gens <= 3 ? 4 : (p.gens <= 6 ? 2 : 1);
   rp.group = kMaxEntries / rp.ppt;
-  rp.shift = bucket_shift;
+  rp.prefix = bucket_prefix;
   rp.shards = bucket_shards;
-  rp.buckets = static_cast<uint32_t*>(buckets.ptr);
+  rp.buckets = static_cast<unsigned long long*>(buckets.ptr);
   rp.shard_begin = meta;
   rp.shard_cap = meta + kMaxShards;
   rp.shard_count = meta + 2 * kMaxShards;
   rp.control = p.control;
   const uint64_t tiles = (p.count + kBlock * rp.ppt - 1) / (kBlock * rp.ppt);
-  reinterpret_cast<RouteFn>(const_cast<void*>(route_fn))<<<grid_for(route_fn, smem, tiles), kBlock, smem, stream>>>(rp);
+  const size_t route_smem = sizeof(RouteSmem) + smem;
+  MG_CHECK(cudaFuncSetAttribute(route_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(route_smem)));
+  reinterpret_cast<RouteFn>(const_cast<void*>(route_fn))<<<grid_for(route_fn, route_smem, tiles), kBlock, route_smem,
+                                                           stream>>>(rp);
   ++launches;
   MG_CHECK(cudaGetLastError());
   AcceptParams ap{};
-  ap.buckets = static_cast<const uint32_t*>(buckets.ptr);
+  ap.buckets = static_cast<const unsigned long long*>(buckets.ptr);
   ap.shard_begin = meta;
   ap.shard_count = meta + 2 * kMaxShards;
   ap.shards = bucket_shards;
-  ap.shift = bucket_shift;
+  ap.work = meta + 3 * kMaxShards;
   ap.bitmap = p.bitmap;
   ap.next = p.next;
   ap.capacity = p.capacity;
@@ -690,7 +697,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   RouteFn route_fn = nullptr;
   AcceptFn accept_fn = nullptr;
   if (bucketed) {
-    pick_bucket(elements, &route_fn, &accept_fn);
+    pick_bucket(elements, bucket_prefix, &route_fn, &accept_fn);
     if (!route_fn) return MGBFS2_UNSUPPORTED;
   }
   shard_history.assign(bucket_shards, 0);

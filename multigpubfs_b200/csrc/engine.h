@@ -61,12 +61,12 @@ struct Graph {
   Control* host_control = nullptr;
   WideState* wide = nullptr;
 
-  // Bucketed (owner-routed) bitmap layers: shard s holds ranks
-  // [s << bucket_shift, (s + 1) << bucket_shift).
-  uint32_t bucket_shift = 0, bucket_shards = 0;
+  // Bucketed (owner-routed) bitmap layers: shard s holds the states whose
+  // first bucket_prefix Lehmer digits spell s, i.e. one contiguous rank range.
+  uint32_t bucket_prefix = 0, bucket_shards = 0;
   uint64_t bucket_margin = 4096, bucket_min_work = 1ull << 22;
   DeviceBuffer buckets, shard_meta;            // uint32 offsets; begin/cap/count per shard
-  unsigned long long* host_meta = nullptr;     // pinned: begin, cap, count (3 x kMaxShards)
+  unsigned long long* host_meta = nullptr;     // pinned: begin, cap, count (3 x kMaxShards), work
   std::vector<uint64_t> shard_history;         // last routed layer's per-shard counts
   uint64_t shard_history_total = 0;
   int bucket_setup(uint64_t work, bool exact);
