@@ -72,7 +72,14 @@ typedef struct {
   uint32_t planner;        /* MGBFS2_PLANNER_* */
   uint32_t bucket_margin;  /* extra entries per shard bucket, 0 = 4096; UINT32_MAX = none */
   uint64_t bucket_min_work; /* successors per layer from which layers are bucketed, 0 = 2^22 */
+  uint32_t options;        /* MGBFS2_OPTION_* bits */
+  uint32_t reserved;
 } mgbfs2_plan_request;
+
+/* Inverse-closed packed graphs tag every frontier state with the generator
+ * that produced it and skip that generator's inverse (the edge back to the
+ * previous layer) without a visited test; this option turns that off. */
+#define MGBFS2_OPTION_NO_PARENT_SKIP 1u
 
 typedef struct {
   uint32_t visited, dedup;
@@ -88,6 +95,8 @@ typedef struct {
   uint32_t shards, block;
   uint32_t inverse_closed;
   uint32_t planner;
+  uint32_t parent_skip;     /* 1 = parent-edge skip active */
+  uint32_t bucket_prefix;   /* bucket shards: states sharing their first k symbols */
 } mgbfs2_plan_info;
 
 typedef struct {
@@ -106,13 +115,14 @@ typedef struct {
   uint32_t fatal;        /* device ERR_* bits when reason = RESOURCE */
   uint32_t layers;       /* entries in the layer table (depth 0 included) */
   uint64_t states;       /* sum of layer sizes */
-  uint64_t successors;   /* successors generated */
+  uint64_t successors;   /* edges explored: generators x expanded states */
   double bfs_seconds;
   uint32_t redo_layers;  /* layers recomputed after an exact overflow */
   uint32_t kernel_launches;
   uint64_t peak_device_bytes;
   double device_seconds; /* CUDA-event time of the whole run on the engine stream */
   double kernel_seconds; /* CUDA-event time summed over the layer-expansion kernels */
+  uint64_t visited_tests; /* successors generated and tested (edges minus skipped parent edges) */
 } mgbfs2_status;
 
 /* Per-layer callback; return non-zero to stop (reason CANCELLED). */

@@ -48,6 +48,7 @@ struct RouteParams {
   const Term* terms;
   const uint32_t* term_begin;
   uint32_t gens, total_terms, ppt, group;  // group: generators per flush (group * ppt <= kMaxEntries)
+  uint32_t gen_shift, pad0;                // parent-edge tags, as in ExpandParams
   uint32_t shards, prefix;                 // shard = Horner of the first `prefix` Lehmer digits
   unsigned long long* buckets;             // all shards, shard s at [begin[s], begin[s] + cap[s])
   const unsigned long long* shard_begin;   // per shard
@@ -93,13 +94,14 @@ __device__ __forceinline__ uint32_t prefix_shard(uint64_t w) {
 }
 
 template <int N, int K>
-__global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
+__global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   RouteSmem& sm = *reinterpret_cast<RouteSmem*>(dyn_smem);
   Term* terms = reinterpret_cast<Term*>(dyn_smem + sizeof(RouteSmem));
   uint32_t* tbegin = reinterpret_cast<uint32_t*>(dyn_smem + sizeof(RouteSmem) + p.total_terms * sizeof(Term));
   for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
-  for (uint32_t i = threadIdx.x; i <= p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
+  for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
+  const uint32_t* inverse = tbegin + p.gens + 1;
   for (uint32_t i = threadIdx.x; i < kWarpsPerBlock * kMaxShards; i += blockDim.x) (&sm.hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -131,20 +133,27 @@ __global__ void __launch_bounds__(kBlock) route_lehmer(RouteParams p) {
         }
       }
     }
+    uint32_t skip[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
+      skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
+    }
     for (uint32_t g0 = 0; g0 < p.gens; g0 += p.group) {
       const uint32_t g1 = min(p.gens, g0 + p.group);
       const uint32_t entries = (g1 - g0) * p.ppt;
       // Produce: successor, its shard, its rank within (warp, shard).
       for (uint32_t g = g0; g < g1; ++g) {
         const uint32_t tb = tbegin[g], te = tbegin[g + 1];
+        const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           if (k >= static_cast<int>(p.ppt)) break;
           const uint32_t slot = ((g - g0) * p.ppt + k) * kBlock + tid;
-          if (val[k]) {
+          if (val[k] && g != skip[k]) {
             const uint64_t c = apply_terms(par[k], terms, tb, te);
             const uint32_t s = prefix_shard<N, K>(c);
-            sm.state[slot] = c;
+            sm.state[slot] = c | gtag;
             sm.tag[slot] = s | (atomicAdd(&sm.hist[warp][s], 1u) << 8);
           } else {
             sm.tag[slot] = kNoEntry;

@@ -272,6 +272,23 @@ void Graph::build_program() {
     }
     term_begin.push_back(static_cast<uint32_t>(terms.size()));
   }
+  // Parent-edge table, appended after the gens + 1 term offsets: inverse[g] =
+  // first generator equal to g^-1.  Tags need ceil(log2(gens + 1)) spare bits
+  // above the packed key; without them (or without inverse closure) the
+  // kernels tag nothing and skip nothing.
+  gen_shift = 0;
+  std::vector<uint32_t> inverse(gens, 0xffffffffu);
+  if (inverse_closed) {
+    for (uint32_t k = 0; k < gens; ++k) {
+      std::vector<uint32_t> inv(n);
+      for (uint32_t i = 0; i < n; ++i) inv[perms[static_cast<size_t>(k) * n + i]] = i;
+      for (uint32_t h = 0; h < gens && inverse[k] == 0xffffffffu; ++h)
+        if (std::equal(inv.begin(), inv.end(), perms.begin() + static_cast<size_t>(h) * n)) inverse[k] = h;
+    }
+    const uint32_t key_bits = n * bits, tag_bits = 32 - __builtin_clz(gens);
+    if (key_bits + tag_bits <= 64) gen_shift = key_bits;
+  }
+  term_begin.insert(term_begin.end(), inverse.begin(), inverse.end());
 }
 
 // graph_definition.py:93-108, restated over int64 with wrap-before-modulus.
@@ -473,6 +490,9 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   }
   p.visited = visited;
   p.dedup = dedup;
+  parent_skip = packed && gen_shift && !(r.options & MGBFS2_OPTION_NO_PARENT_SKIP);
+  p.parent_skip = parent_skip;
+  p.bucket_prefix = bucket_prefix;
   p.history_layers = visited == MGBFS2_VISITED_HASH3 ? 3 : 1;
   p.bitmap_bits = visited == MGBFS2_VISITED_BITMAP ? rank_total : 0;
   // Frontier capacity: the orbit bound (or the caller's cap) within memory.
@@ -611,6 +631,7 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   rp.term_begin = p.term_begin;
   rp.gens = p.gens;
   rp.total_terms = p.total_terms;
+  rp.gen_shift = p.gen_shift;
   // Parents per thread and generators per flush: at most kMaxEntries staged
   // successors per thread.
   rp.ppt = p.gens <= 3 ? 4 : (p.gens <= 6 ? 2 : 1);
@@ -708,6 +729,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   p.term_begin = reinterpret_cast<const uint32_t*>(static_cast<const char*>(program.ptr) + terms.size() * sizeof(Term));
   p.gens = gens;
   p.total_terms = static_cast<uint32_t>(terms.size());
+  p.gen_shift = parent_skip ? gen_shift : 0;
   p.control = static_cast<Control*>(control_buf.ptr);
   p.key_mask = key_mask;
   p.ppt = gens <= 4 ? 4 : 2;
@@ -851,6 +873,8 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       shard_history_total = work;
     }
     st.successors += count * gens;
+    // Every tagged parent (all but the start) skips exactly one generator.
+    st.visited_tests += count * gens - (parent_skip && depth > 0 ? count : 0);
     const Control c = *host_control;
     peak = std::max<uint64_t>(peak, bitmap.bytes + front.bytes + next.bytes + table.bytes + bank[0].bytes +
                                         bank[1].bytes + bank[2].bytes);

@@ -48,7 +48,9 @@ struct Graph {
   uint64_t rank_total = 0, state_bound = 0;
   std::vector<uint64_t> coxeter;   // certified layer sizes, empty if not Coxeter
   std::vector<Term> terms;
-  std::vector<uint32_t> term_begin;
+  std::vector<uint32_t> term_begin;  // gens + 1 term offsets, then inverse[gens]
+  uint32_t gen_shift = 0;            // parent-edge tag position, 0 = no tags
+  bool parent_skip = false;          // plan: use the tags
 
   // Plan and device state.
   bool planned = false;

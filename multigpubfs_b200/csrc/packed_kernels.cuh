@@ -23,8 +23,13 @@ struct ExpandParams {
   unsigned long long* next;
   unsigned long long capacity;
   const Term* terms;
-  const uint32_t* term_begin;
+  const uint32_t* term_begin;  // gens + 1 entries, followed by inverse[gens]
   uint32_t gens, total_terms;
+  // Parent-edge tags (inverse-closed graphs): a frontier word carries
+  // (g + 1) << gen_shift for the generator g that produced it; generator
+  // inverse[g] applied to it returns to the previous layer and is skipped.
+  // gen_shift = 0 disables tagging.
+  uint32_t gen_shift, pad0;
   Control* control;
   unsigned long long* bitmap;
   MultisetDomain ms;
@@ -123,8 +128,9 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
   __shared__ unsigned long long out_base;
   Term* terms = reinterpret_cast<Term*>(program_smem);
   uint32_t* begin = reinterpret_cast<uint32_t*>(program_smem + p.total_terms * sizeof(Term));
+  const uint32_t* inverse = begin + p.gens + 1;
   for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
-  for (uint32_t i = threadIdx.x; i <= p.gens; i += blockDim.x) begin[i] = p.term_begin[i];
+  for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) begin[i] = p.term_begin[i];
   if (threadIdx.x == 0) out_count = 0;
   __syncthreads();
 
@@ -152,20 +158,28 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
         }
       }
     }
+    uint32_t skip[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
+      skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
+    }
     for (uint32_t g = 0; g < p.gens; ++g) {
       const uint32_t tb = begin[g], te = begin[g + 1];
+      const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         if (k >= static_cast<int>(p.ppt)) break;
-        const uint64_t c = val[k] ? apply_terms(par[k], terms, tb, te) : 0;
-        const bool won = claim<V, N, WARP>(p, c, val[k]);
+        const bool v = val[k] && g != skip[k];
+        const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
+        const bool won = claim<V, N, WARP>(p, c, v);
         const unsigned m = __ballot_sync(kFullMask, won);
         if (m) {
           const int leader = __ffs(m) - 1;
           uint32_t wb = 0;
           if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
           wb = __shfl_sync(kFullMask, wb, leader);
-          if (won) out[wb + __popc(m & lanemask_lt())] = c;
+          if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
         }
       }
       if (g + 1 < p.gens) {

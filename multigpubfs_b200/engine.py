@@ -28,6 +28,7 @@ class RunResult:
     peak_device_bytes: int
     device_seconds: float = 0.0
     kernel_seconds: float = 0.0
+    visited_tests: int = 0
     fatal_names: list = field(default_factory=list)
 
 
@@ -90,8 +91,9 @@ class NativeGraph:
         self.close()
 
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
-             planner="plain", bucket_margin=None, bucket_min_work=None) -> dict:
+             planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True) -> dict:
         req = native.PlanRequest()
+        req.options = 0 if parent_skip else native.OPTION_NO_PARENT_SKIP
         req.bucket_margin = 0 if bucket_margin is None else (0xFFFFFFFF if bucket_margin == 0 else bucket_margin)
         req.bucket_min_work = bucket_min_work or 0
         req.visited = native.VISITED[visited]
@@ -126,7 +128,7 @@ class NativeGraph:
         return RunResult(bool(status.complete), native.REASONS.get(status.reason, str(status.reason)), status.fatal,
                          sizes, seconds, status.states, status.successors, status.bfs_seconds,
                          status.kernel_launches, status.redo_layers, status.peak_device_bytes,
-                         status.device_seconds, status.kernel_seconds, names)
+                         status.device_seconds, status.kernel_seconds, status.visited_tests, names)
 
     def layer_table(self):
         count = C.c_size_t()

@@ -48,7 +48,11 @@ class GraphDesc(C.Structure):
 class PlanRequest(C.Structure):
     _fields_ = [("visited", C.c_uint32), ("dedup", C.c_uint32), ("capacity", C.c_uint64),
                 ("reserve_bytes", C.c_uint64), ("shards", C.c_uint32), ("block", C.c_uint32),
-                ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64)]
+                ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64),
+                ("options", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+OPTION_NO_PARENT_SKIP = 1
 
 
 class PlanInfo(C.Structure):
@@ -56,7 +60,8 @@ class PlanInfo(C.Structure):
                 ("bits_per_symbol", C.c_uint32), ("key_words", C.c_uint32), ("history_layers", C.c_uint32),
                 ("capacity", C.c_uint64), ("table_slots", C.c_uint64), ("bitmap_bits", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("state_bound", C.c_uint64), ("shards", C.c_uint32),
-                ("block", C.c_uint32), ("inverse_closed", C.c_uint32), ("planner", C.c_uint32)]
+                ("block", C.c_uint32), ("inverse_closed", C.c_uint32), ("planner", C.c_uint32),
+                ("parent_skip", C.c_uint32), ("bucket_prefix", C.c_uint32)]
 
     def to_dict(self):
         d = {name: getattr(self, name) for name, _ in self._fields_}
@@ -75,7 +80,7 @@ class RunStatus(C.Structure):
     _fields_ = [("complete", C.c_uint32), ("reason", C.c_uint32), ("fatal", C.c_uint32), ("layers", C.c_uint32),
                 ("states", C.c_uint64), ("successors", C.c_uint64), ("bfs_seconds", C.c_double),
                 ("redo_layers", C.c_uint32), ("kernel_launches", C.c_uint32), ("peak_device_bytes", C.c_uint64),
-                ("device_seconds", C.c_double), ("kernel_seconds", C.c_double)]
+                ("device_seconds", C.c_double), ("kernel_seconds", C.c_double), ("visited_tests", C.c_uint64)]
 
 
 LAYER_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint64, C.c_double)

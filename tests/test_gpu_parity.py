@@ -46,12 +46,15 @@ VARIANTS = {
     "bitmap_bucket": dict(visited="bitmap", dedup="bucket", bucket_min_work=1),
     # no bucket slack: first attempts overflow and are redone with exact counts
     "bitmap_bucket_tight": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, bucket_margin=0),
+    # every generator applied, no parent-edge skip
+    "bitmap_bucket_noskip": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, parent_skip=False),
+    "hash3_noskip": dict(visited="hash3", parent_skip=False),
 }
 
 
 def _applicable(case, variant):
     g = case["graph"]
-    if variant == "hash3":
+    if variant.startswith("hash3"):
         return case["inverse_closed"]
     if variant.startswith("bitmap"):
         return g["action"]["kind"] == "permutation" and len(set(g["start"])) <= 16 and \
@@ -87,8 +90,21 @@ def test_golden_cases(exact_cases, variant):
     assert ran >= 8
 
 
+def test_parent_skip_accounting(lrx_layers):
+    """With parent-edge tags every state but the start skips one of its g
+    generators; the layer tables are identical with and without the skip."""
+    g = G.permutation_graph(G.lrx_generators(10), list(range(10)))
+    info, skip, _, _ = run(g, visited="bitmap", dedup="bucket", bucket_min_work=1)
+    info0, noskip, _, _ = run(g, visited="bitmap", dedup="bucket", bucket_min_work=1, parent_skip=False)
+    assert info["parent_skip"] == 1 and info0["parent_skip"] == 0
+    assert skip.layer_sizes == noskip.layer_sizes == lrx_layers[10]
+    n = sum(lrx_layers[10])
+    assert skip.successors == noskip.successors == 3 * n
+    assert noskip.visited_tests == 3 * n and skip.visited_tests == 3 * n - (n - 1)
+
+
 @pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3", "bitmap_bucket",
-                                     "bitmap_bucket_tight"])
+                                     "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip"])
 def test_lrx_small(lrx_layers, variant):
     redo = 0
     for n in range(3, 12):
