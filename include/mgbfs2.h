@@ -216,6 +216,25 @@ MGBFS2_API int mgbfs2_sort_unique_tiles(const uint64_t* keys, uint64_t count, ui
 MGBFS2_API int mgbfs2_bucket_keys(const uint64_t* keys, uint64_t count, uint32_t shift, uint32_t shards, uint64_t* buckets,
                        uint64_t capacity, unsigned long long* counts, uint32_t* error, void* stream);
 
+/* One exact BFS layer of a packed permutation frontier (4-bit codes, degree
+ * 2..16, all codes distinct, <= 64 generators) against a caller-owned
+ * Lehmer-rank bitmap of ceil(degree!/64) words, through the bucketed
+ * route/accept kernels: successors are routed into rank-range shards of the
+ * bitmap (exactly sized by a counting pass) and tested shard by shard.
+ * New states are written to next[0 .. next_capacity); *next_count (device)
+ * receives their exact number (bit 0 of *error when it exceeds the capacity).
+ * All temporaries live in `scratch` (device, >= mgbfs2_expand_layer_scratch_bytes
+ * bytes, 256-byte aligned); asynchronous on `stream`; allocates nothing.
+ * Replaces the route + accept pair mgbfs_bitmap_route / mgbfs_bitmap_accept,
+ * cuda/permutation_bitmap.cu:27-48 and :105-133. */
+MGBFS2_API int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                                          const uint64_t* frontier, uint64_t count, uint64_t* bitmap,
+                                          uint64_t* next, uint64_t next_capacity, uint64_t* next_count,
+                                          uint32_t* error, void* scratch, uint64_t scratch_bytes, void* stream);
+
+/* Scratch bytes mgbfs2_expand_layer_bitmap needs for `count` parents. */
+MGBFS2_API uint64_t mgbfs2_expand_layer_scratch_bytes(uint32_t degree, uint32_t generators, uint64_t count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -233,6 +233,32 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
   }
 }
 
+// Counting pass for exactly sized buckets: the shard histogram of all
+// successors of the frontier (same generation and shard rule as route).
+template <int N, int K>
+__global__ void __launch_bounds__(kBlock) count_lehmer(RouteParams p) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  uint32_t* hist = reinterpret_cast<uint32_t*>(dyn_smem);
+  Term* terms = reinterpret_cast<Term*>(dyn_smem + kMaxShards * sizeof(uint32_t));
+  uint32_t* tbegin = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(terms) + p.total_terms * sizeof(Term));
+  for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
+  for (uint32_t s = threadIdx.x; s < p.shards; s += blockDim.x) hist[s] = 0;
+  __syncthreads();
+  const uint32_t* inverse = tbegin + p.gens + 1;
+  for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < p.count;
+       i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned long long w = p.frontier[i];
+    const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(w >> p.gen_shift) : 0u;
+    const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
+    for (uint32_t g = 0; g < p.gens; ++g)
+      if (g != skip) atomicAdd(&hist[prefix_shard<N, K>(apply_terms(w, terms, tbegin[g], tbegin[g + 1]))], 1u);
+  }
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < p.shards; s += blockDim.x)
+    if (hist[s]) atomicAdd(&p.shard_count[s], static_cast<unsigned long long>(hist[s]));
+}
+
 template <int N>
 __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
   __shared__ unsigned long long win[kAcceptChunk];

@@ -1,0 +1,235 @@
+// Kernel-level entry point: one exact BFS layer of a packed permutation
+// frontier against a caller-owned Lehmer-rank bitmap, through the bucketed
+// route/accept kernels (bucket_kernels.cuh).  Stand-alone and asynchronous:
+// bucket sizes come from an exact counting pass and an on-device scan, so no
+// host round trip and no overflow redo are needed.  All temporaries live in
+// caller-provided scratch.
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "../../include/mgbfs2.h"
+#include "bucket_kernels.cuh"
+#include "engine.h"
+
+namespace mgbfs2 {
+namespace {
+
+constexpr uint32_t kLayerMaxGens = 64;
+constexpr size_t kAlign = 256;
+
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// Byte offsets of the scratch regions.
+struct LayerLayout {
+  size_t control, meta, program, buckets, total;
+};
+
+LayerLayout layer_layout(uint64_t entries) {
+  LayerLayout l{};
+  l.control = 0;
+  l.meta = align_up(sizeof(Control));
+  l.program = l.meta + align_up((3 * kMaxShards + 1) * sizeof(unsigned long long));
+  l.buckets = l.program + align_up(kLayerMaxGens * 16 * sizeof(Term) + (2 * kLayerMaxGens + 1) * sizeof(uint32_t));
+  l.total = l.buckets + align_up(entries * sizeof(unsigned long long));
+  return l;
+}
+
+// Single block: begin = exclusive scan of the counts, cap = counts (exact),
+// then the counts and the accept work counter restart at zero.
+__global__ void layout_shards(unsigned long long* meta, uint32_t shards) {
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint32_t s = 0; s < shards; ++s) {
+      const unsigned long long c = meta[2 * kMaxShards + s];
+      meta[s] = run;
+      meta[kMaxShards + s] = c;
+      meta[2 * kMaxShards + s] = 0;
+      run += c;
+    }
+    meta[3 * kMaxShards] = 0;
+  }
+}
+
+__global__ void publish_layer(const Control* control, unsigned long long* next_count, unsigned int* error) {
+  if (threadIdx.x == 0) {
+    *next_count = control->next_count;
+    if (error && control->error) atomicOr(error, control->error);
+  }
+}
+
+using CountFn = void (*)(RouteParams);
+using RouteFn = void (*)(RouteParams);
+using AcceptFn = void (*)(AcceptParams);
+
+struct LayerKernels {
+  CountFn count;
+  RouteFn route;
+  AcceptFn accept;
+};
+
+template <int N>
+LayerKernels kernels_for(uint32_t prefix) {
+  if (prefix == 1) return {count_lehmer<N, 1>, route_lehmer<N, 1>, accept_lehmer<N>};
+  return {count_lehmer<N, 2>, route_lehmer<N, 2>, accept_lehmer<N>};
+}
+
+bool pick_layer_kernels(uint32_t n, uint32_t prefix, LayerKernels* k) {
+  switch (n) {
+#define MG_CASE(K)                   \
+  case K:                            \
+    *k = kernels_for<K>(prefix);     \
+    return true;
+    MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
+    MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
+#undef MG_CASE
+    default:
+      return false;
+  }
+}
+
+uint32_t layer_prefix(uint32_t n) {
+  uint64_t f = 1;
+  for (uint32_t i = 2; i < n; ++i) f *= i;  // (n-1)!
+  return (f / 8 > (8ull << 20) && n * (n - 1) <= kMaxShards) ? 2u : 1u;
+}
+
+// Host-side program: displacement terms, term offsets, then the (unused)
+// parent-edge table.
+bool build_layer_program(uint32_t n, uint32_t gens, const uint32_t* perms, std::vector<Term>* terms,
+                         std::vector<uint32_t>* begin) {
+  terms->clear();
+  begin->assign(1, 0);
+  for (uint32_t k = 0; k < gens; ++k) {
+    std::map<int, uint64_t> groups;
+    std::vector<uint8_t> seen(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t src = perms[static_cast<size_t>(k) * n + i];
+      if (src >= n || seen[src]) return false;
+      seen[src] = 1;
+      groups[static_cast<int>(src) - static_cast<int>(i)] |= 15ull << (4 * i);
+    }
+    for (auto& kv : groups) {
+      const int shift = kv.first * 4;
+      terms->push_back(Term{kv.second, shift > 0 ? static_cast<uint32_t>(shift) : 0u,
+                            shift < 0 ? static_cast<uint32_t>(-shift) : 0u});
+    }
+    begin->push_back(static_cast<uint32_t>(terms->size()));
+  }
+  begin->insert(begin->end(), gens, 0xffffffffu);
+  return true;
+}
+
+uint32_t occupancy_grid(const void* fn, size_t smem, int device) {
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return static_cast<uint32_t>(sms * per_sm);
+}
+
+}  // namespace
+
+// Enqueues the layer expansion into `scratch` (device memory laid out by
+// layer_layout).  Shared by the caller-scratch entry point.
+int expand_layer_into(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                      const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
+                      uint64_t next_capacity, uint64_t* next_count, uint32_t* error, unsigned char* scratch,
+                      uint64_t scratch_bytes, cudaStream_t stream) {
+  if (degree < 2 || degree > 16 || !generators || generators > kLayerMaxGens || !permutations_host || !bitmap ||
+      !next_count || !scratch || (count && (!frontier || !next)))
+    return MGBFS2_INVALID_ARGUMENT;
+  const LayerLayout l = layer_layout(count * generators);
+  if (scratch_bytes < l.total) return MGBFS2_CAPACITY;
+  std::vector<Term> terms;
+  std::vector<uint32_t> begin;
+  if (!build_layer_program(degree, generators, permutations_host, &terms, &begin)) return MGBFS2_INVALID_ARGUMENT;
+  const uint32_t prefix = layer_prefix(degree);
+  LayerKernels k{};
+  if (!pick_layer_kernels(degree, prefix, &k)) return MGBFS2_UNSUPPORTED;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_status(e);
+  Control* control = reinterpret_cast<Control*>(scratch + l.control);
+  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  Term* program = reinterpret_cast<Term*>(scratch + l.program);
+  uint32_t* program_begin = reinterpret_cast<uint32_t*>(scratch + l.program + terms.size() * sizeof(Term));
+  if ((e = cudaMemsetAsync(control, 0, sizeof(Control), stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(meta, 0, (3 * kMaxShards + 1) * sizeof(unsigned long long), stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(program, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, stream)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(program_begin, begin.data(), begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           stream)) != cudaSuccess)
+    return cuda_status(e);
+  uint64_t fact = 1;
+  for (uint32_t i = degree - prefix + 1; i <= degree; ++i) fact *= i;
+  RouteParams rp{};
+  rp.frontier = reinterpret_cast<const unsigned long long*>(frontier);
+  rp.count = count;
+  rp.terms = program;
+  rp.term_begin = program_begin;
+  rp.gens = generators;
+  rp.total_terms = static_cast<uint32_t>(terms.size());
+  rp.ppt = generators <= 3 ? 4 : (generators <= 6 ? 2 : 1);
+  rp.group = kMaxEntries / rp.ppt;
+  rp.gen_shift = 0;
+  rp.shards = static_cast<uint32_t>(fact);  // n!/(n-prefix)!
+  rp.prefix = prefix;
+  rp.buckets = reinterpret_cast<unsigned long long*>(scratch + l.buckets);
+  rp.shard_begin = meta;
+  rp.shard_cap = meta + kMaxShards;
+  rp.shard_count = meta + 2 * kMaxShards;
+  rp.control = control;
+  const size_t program_bytes = terms.size() * sizeof(Term) + begin.size() * sizeof(uint32_t);
+  if (count) {
+    const size_t count_smem = kMaxShards * sizeof(uint32_t) + program_bytes;
+    k.count<<<occupancy_grid(reinterpret_cast<const void*>(k.count), count_smem, device), kBlock, count_smem,
+              stream>>>(rp);
+    layout_shards<<<1, 32, 0, stream>>>(meta, rp.shards);
+    const size_t route_smem = sizeof(RouteSmem) + program_bytes;
+    if ((e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k.route), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(route_smem))) != cudaSuccess)
+      return cuda_status(e);
+    k.route<<<occupancy_grid(reinterpret_cast<const void*>(k.route), route_smem, device), kBlock, route_smem,
+              stream>>>(rp);
+    AcceptParams ap{};
+    ap.buckets = rp.buckets;
+    ap.shard_begin = meta;
+    ap.shard_count = meta + 2 * kMaxShards;
+    ap.shards = rp.shards;
+    ap.bitmap = reinterpret_cast<unsigned long long*>(bitmap);
+    ap.next = reinterpret_cast<unsigned long long*>(next);
+    ap.capacity = next_capacity;
+    ap.work = meta + 3 * kMaxShards;
+    ap.control = control;
+    k.accept<<<occupancy_grid(reinterpret_cast<const void*>(k.accept), 0, device), kBlock, 0, stream>>>(ap);
+  }
+  publish_layer<<<1, 32, 0, stream>>>(control, reinterpret_cast<unsigned long long*>(next_count), error);
+  return cuda_status(cudaGetLastError());
+}
+
+uint64_t expand_layer_scratch_bytes(uint64_t count, uint32_t generators) {
+  return layer_layout(count * generators).total;
+}
+
+}  // namespace mgbfs2
+
+extern "C" {
+
+uint64_t mgbfs2_expand_layer_scratch_bytes(uint32_t degree, uint32_t generators, uint64_t count) {
+  (void)degree;
+  return mgbfs2::expand_layer_scratch_bytes(count, generators);
+}
+
+int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                               const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
+                               uint64_t next_capacity, uint64_t* next_count, uint32_t* error, void* scratch,
+                               uint64_t scratch_bytes, void* stream) {
+  return mgbfs2::expand_layer_into(degree, generators, permutations_host, frontier, count, bitmap, next,
+                                   next_capacity, next_count, error, static_cast<unsigned char*>(scratch),
+                                   scratch_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
 }
 
 // Marks the start state visited (and, for the hash paths, inserts it).
-__global__ void seed_packed(ExpandParams p, unsigned long long start, int kind, uint32_t n) {
+static __global__ void seed_packed(ExpandParams p, unsigned long long start, int kind, uint32_t n) {
   if (threadIdx.x || blockIdx.x) return;
   uint64_t r = 0;
   if (kind == V_LEHMER) {
@@ -210,7 +210,7 @@ __global__ void seed_packed(ExpandParams p, unsigned long long start, int kind, 
 }
 
 // Re-inserts every key of an old all-visited table into a larger one.
-__global__ void rehash_table(const unsigned long long* old_table, unsigned long long old_slots,
+static __global__ void rehash_table(const unsigned long long* old_table, unsigned long long old_slots,
                              unsigned long long* table, unsigned long long mask, unsigned long long key_mask,
                              unsigned int* error) {
   for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < old_slots;

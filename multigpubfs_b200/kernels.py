@@ -106,6 +106,29 @@ def sort_unique_tiles(keys, key_bits, tile=4096):
     return out, counts
 
 
+def expand_layer_bitmap(degree, generators, frontier, bitmap, next_capacity, scratch=None):
+    """One bucketed BFS layer: frontier (packed words, int64 tensor) against
+    `bitmap` (int64 tensor of ceil(degree!/64) words, updated in place).
+    Returns (next words [count], error bits)."""
+    import torch
+    lib = _lib()
+    flat = (C.c_uint32 * (degree * len(generators)))(*[x for g in generators for x in g])
+    count = frontier.numel()
+    need = lib.mgbfs2_expand_layer_scratch_bytes(degree, len(generators), count)
+    if scratch is None:
+        scratch = torch.empty(need, dtype=torch.uint8, device=frontier.device)
+    nxt = torch.empty(max(next_capacity, 1), dtype=torch.int64, device=frontier.device)
+    out_count = torch.zeros(1, dtype=torch.int64, device=frontier.device)
+    err = _error_word(frontier.device)
+    native.check(lib.mgbfs2_expand_layer_bitmap(degree, len(generators), flat, frontier.data_ptr(), count,
+                                                bitmap.data_ptr(), nxt.data_ptr(), next_capacity,
+                                                out_count.data_ptr(), err.data_ptr(), scratch.data_ptr(),
+                                                scratch.numel(), native.stream_handle()),
+                 "mgbfs2_expand_layer_bitmap")
+    n = int(out_count.item())
+    return nxt[:min(n, next_capacity)], int(err.item())
+
+
 def bucket_keys(keys, shift, shards, capacity):
     import torch
     lib = _lib()

@@ -108,6 +108,10 @@ _SIGNATURES = {
                                            C.c_void_p]),
     "mgbfs2_bucket_keys": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mgbfs2_expand_layer_bitmap": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint64,
+                                             C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_uint64, C.c_void_p]),
+    "mgbfs2_expand_layer_scratch_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
 }
 
 

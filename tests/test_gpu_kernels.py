@@ -173,3 +173,73 @@ def test_bucket_keys():
     buckets, counts, err = bucket_keys(torch.tensor(raw, device="cuda"), 20, 64, 16)
     assert int(err.item()) & 8
     assert counts.sum().item() == len(raw)
+
+
+def _layer_bfs(n, gens):
+    """BFS driven entirely by mgbfs2_expand_layer_bitmap calls."""
+    torch = _torch()
+    from multigpubfs_b200.kernels import expand_layer_bitmap
+    bitmap = torch.zeros((math.factorial(n) + 63) // 64, dtype=torch.int64, device="cuda")
+    start = P.pack(list(range(n)), 4)
+    bitmap[0] = 1  # rank of the identity is 0
+    frontier = torch.tensor([start], dtype=torch.int64, device="cuda")
+    layers = [frontier.cpu().tolist()]
+    while frontier.numel():
+        nxt, err = expand_layer_bitmap(n, gens, frontier, bitmap, frontier.numel() * len(gens))
+        assert err == 0
+        frontier = nxt.clone()
+        if frontier.numel():
+            layers.append(frontier.cpu().tolist())
+    return layers
+
+
+@pytest.mark.parametrize("n,family", [(9, "lrx"), (8, "coxeter"), (13, "lrx_prefix")])
+def test_expand_layer_bitmap_bfs(n, family, lrx_layers):
+    if family == "lrx_prefix":
+        # S13 uses two-symbol shards; run the first 20 layers only.
+        torch = _torch()
+        from multigpubfs_b200.kernels import expand_layer_bitmap
+        gens = G.lrx_generators(n)
+        bitmap = torch.zeros((math.factorial(n) + 63) // 64, dtype=torch.int64, device="cuda")
+        bitmap[0] = 1
+        frontier = torch.tensor([P.pack(list(range(n)), 4)], dtype=torch.int64, device="cuda")
+        sizes = [1]
+        for _ in range(19):
+            frontier, err = expand_layer_bitmap(n, gens, frontier, bitmap, frontier.numel() * 3)
+            frontier = frontier.clone()
+            assert err == 0
+            sizes.append(frontier.numel())
+        from tests.conftest import golden
+        assert sizes == golden("lrx13_layers.json")["layers"][:20]
+        return
+    gens = G.lrx_generators(n) if family == "lrx" else G.coxeter_generators(n)
+    layers = _layer_bfs(n, gens)
+    expect = lrx_layers[n] if family == "lrx" else G.coxeter_layers(n)
+    assert [len(x) for x in layers] == expect
+    assert all(len(set(x)) == len(x) for x in layers)
+
+
+def test_expand_layer_bitmap_states_match_oracle():
+    n = 7
+    gens = G.lrx_generators(n)
+    exact = G.exact_layers(G.permutation_graph(gens, list(range(n))), 1 << 16)
+    layers = _layer_bfs(n, gens)
+    assert len(layers) == len(exact)
+    for got, want in zip(layers, exact):
+        assert sorted(P.unpack(w & ((1 << 64) - 1), n, 4) for w in got) == want
+
+
+def test_expand_layer_bitmap_capacity_and_scratch_checks():
+    torch = _torch()
+    from multigpubfs_b200 import native
+    from multigpubfs_b200.kernels import expand_layer_bitmap
+    n = 8
+    gens = G.lrx_generators(n)
+    bitmap = torch.zeros((math.factorial(n) + 63) // 64, dtype=torch.int64, device="cuda")
+    bitmap[0] = 1
+    frontier = torch.tensor([P.pack(list(range(n)), 4)], dtype=torch.int64, device="cuda")
+    nxt, err = expand_layer_bitmap(n, gens, frontier, bitmap, 1)  # 3 new states, room for 1
+    assert err & 1 and nxt.numel() == 1
+    small = torch.empty(16, dtype=torch.uint8, device="cuda")
+    with pytest.raises(native.NativeError):
+        expand_layer_bitmap(n, gens, frontier, bitmap, 8, scratch=small)
