@@ -235,6 +235,25 @@ MGBFS2_API int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, 
 /* Scratch bytes mgbfs2_expand_layer_bitmap needs for `count` parents. */
 MGBFS2_API uint64_t mgbfs2_expand_layer_scratch_bytes(uint32_t degree, uint32_t generators, uint64_t count);
 
+/* mgbfs2_expand_layer_bitmap for callers that cannot allocate device memory:
+ * hosts that reserve the whole GPU in their own pool and forbid any other
+ * allocator, and search loops that must not stall or fail in an allocator in
+ * the middle of a BFS.  Same inputs, outputs and results, but the scratch is a
+ * 32 MiB array inside the library (every GPU that loads the library holds it
+ * until the process exits), so the call allocates nothing and copies nothing
+ * from the host.  Limit: count * generators <= 4,191,328 successors per call
+ * (MGBFS2_CAPACITY above it, before anything is launched).  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current, so make it before any stream capture.  All calls on a device
+ * share the array and it keeps the last call's contents (each call clears what
+ * must start at zero); calls that overlap on the GPU race on it and must be
+ * serialised by the caller.  No counterpart in the reference. */
+MGBFS2_API int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t generators,
+                                                 const uint32_t* permutations_host, const uint64_t* frontier,
+                                                 uint64_t count, uint64_t* bitmap, uint64_t* next,
+                                                 uint64_t next_capacity, uint64_t* next_count, uint32_t* error,
+                                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

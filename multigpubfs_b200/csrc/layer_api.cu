@@ -6,6 +6,7 @@
 // caller-provided scratch.
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "../../include/mgbfs2.h"
@@ -214,6 +215,148 @@ uint64_t expand_layer_scratch_bytes(uint64_t count, uint32_t generators) {
   return layer_layout(count * generators).total;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant for callers that cannot allocate device memory.
+//
+// Some callers of this library cannot call cudaMalloc (or any allocator) per
+// layer: a host framework that reserves all of the GPU's memory in its own
+// pool up front and forbids any other allocation (a second allocator would
+// fail or fragment that pool), and search loops that must not stall, since
+// cudaMalloc may synchronise the device and can fail under memory pressure
+// in the middle of a BFS.  For them the layer's scratch lives in one
+// file-scope __device__ array of kStaticScratchBytes that every GPU loading
+// this library holds until the process exits.  The generator program and the
+// zeroed counters are written into it by one staging kernel from its
+// parameters, so a call issues only kernel launches: no allocation, no host
+// copy.  All calls on a device share the array and it keeps the last call's
+// contents (each call re-zeroes what must start at zero); two calls that
+// overlap on the GPU -- concurrent streams, or host threads on one device --
+// race on it and must be serialised by the caller.
+constexpr size_t kStaticScratchBytes = 32ull << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_lock;
+unsigned char* g_static_address[kStaticMaxDevices] = {};
+
+// Device address of g_static_scratch on `device` (the current device).  The
+// host-side name is only a stand-in for the symbol, never a device address,
+// so it is resolved once per device with cudaGetSymbolAddress.
+int static_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kStaticMaxDevices) return MGBFS2_UNSUPPORTED;
+  std::lock_guard<std::mutex> hold(g_static_lock);
+  if (!g_static_address[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_status(e);
+    g_static_address[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_static_address[device];
+  return MGBFS2_OK;
+}
+
+struct StagedProgram {
+  Term terms[kLayerMaxGens * 16];
+  uint32_t begin[2 * kLayerMaxGens + 1];
+  uint32_t total_terms, begin_entries;
+};
+
+// Writes the program into scratch and zeroes the control block and shard
+// metadata (counts, capacities, work counter).
+__global__ void stage_static_layer(StagedProgram prog, Term* terms, uint32_t* begin, Control* control,
+                                   unsigned long long* meta) {
+  for (uint32_t i = threadIdx.x; i < prog.total_terms; i += blockDim.x) terms[i] = prog.terms[i];
+  for (uint32_t i = threadIdx.x; i < prog.begin_entries; i += blockDim.x) begin[i] = prog.begin[i];
+  for (uint32_t i = threadIdx.x; i < 3 * kMaxShards + 1; i += blockDim.x) meta[i] = 0;
+  if (threadIdx.x == 0) {
+    control->next_count = 0;
+    control->aux = 0;
+    control->error = 0;
+    control->pad = 0;
+  }
+}
+
+}  // namespace
+
+int expand_layer_static(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                        const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
+                        uint64_t next_capacity, uint64_t* next_count, uint32_t* error, cudaStream_t stream) {
+  if (degree < 2 || degree > 16 || !generators || generators > kLayerMaxGens || !permutations_host || !bitmap ||
+      !next_count || (count && (!frontier || !next)))
+    return MGBFS2_INVALID_ARGUMENT;
+  const LayerLayout l = layer_layout(count * generators);
+  if (l.total > kStaticScratchBytes) return MGBFS2_CAPACITY;  // count * generators above the static bucket room
+  static thread_local StagedProgram prog;
+  std::vector<Term> terms;
+  std::vector<uint32_t> begin;
+  if (!build_layer_program(degree, generators, permutations_host, &terms, &begin)) return MGBFS2_INVALID_ARGUMENT;
+  std::copy(terms.begin(), terms.end(), prog.terms);
+  std::copy(begin.begin(), begin.end(), prog.begin);
+  prog.total_terms = static_cast<uint32_t>(terms.size());
+  prog.begin_entries = static_cast<uint32_t>(begin.size());
+  const uint32_t prefix = layer_prefix(degree);
+  LayerKernels k{};
+  if (!pick_layer_kernels(degree, prefix, &k)) return MGBFS2_UNSUPPORTED;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_status(e);
+  unsigned char* scratch = nullptr;
+  int rc = static_scratch(device, &scratch);
+  if (rc) return rc;
+  Control* control = reinterpret_cast<Control*>(scratch + l.control);
+  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  Term* program = reinterpret_cast<Term*>(scratch + l.program);
+  uint32_t* program_begin = reinterpret_cast<uint32_t*>(scratch + l.program + terms.size() * sizeof(Term));
+  stage_static_layer<<<1, kBlock, 0, stream>>>(prog, program, program_begin, control, meta);
+  uint64_t fact = 1;
+  for (uint32_t i = degree - prefix + 1; i <= degree; ++i) fact *= i;
+  RouteParams rp{};
+  rp.frontier = reinterpret_cast<const unsigned long long*>(frontier);
+  rp.count = count;
+  rp.terms = program;
+  rp.term_begin = program_begin;
+  rp.gens = generators;
+  rp.total_terms = prog.total_terms;
+  rp.ppt = generators <= 3 ? 4 : (generators <= 6 ? 2 : 1);
+  rp.group = kMaxEntries / rp.ppt;
+  rp.gen_shift = 0;
+  rp.shards = static_cast<uint32_t>(fact);
+  rp.prefix = prefix;
+  rp.buckets = reinterpret_cast<unsigned long long*>(scratch + l.buckets);
+  rp.shard_begin = meta;
+  rp.shard_cap = meta + kMaxShards;
+  rp.shard_count = meta + 2 * kMaxShards;
+  rp.control = control;
+  const size_t program_bytes = terms.size() * sizeof(Term) + begin.size() * sizeof(uint32_t);
+  if (count) {
+    const size_t count_smem = kMaxShards * sizeof(uint32_t) + program_bytes;
+    k.count<<<occupancy_grid(reinterpret_cast<const void*>(k.count), count_smem, device), kBlock, count_smem,
+              stream>>>(rp);
+    layout_shards<<<1, 32, 0, stream>>>(meta, rp.shards);
+    const size_t route_smem = sizeof(RouteSmem) + program_bytes;
+    if ((e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k.route), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(route_smem))) != cudaSuccess)
+      return cuda_status(e);
+    k.route<<<occupancy_grid(reinterpret_cast<const void*>(k.route), route_smem, device), kBlock, route_smem,
+              stream>>>(rp);
+    AcceptParams ap{};
+    ap.buckets = rp.buckets;
+    ap.shard_begin = meta;
+    ap.shard_count = meta + 2 * kMaxShards;
+    ap.shards = rp.shards;
+    ap.bitmap = reinterpret_cast<unsigned long long*>(bitmap);
+    ap.next = reinterpret_cast<unsigned long long*>(next);
+    ap.capacity = next_capacity;
+    ap.work = meta + 3 * kMaxShards;
+    ap.control = control;
+    k.accept<<<occupancy_grid(reinterpret_cast<const void*>(k.accept), 0, device), kBlock, 0, stream>>>(ap);
+  }
+  publish_layer<<<1, 32, 0, stream>>>(control, reinterpret_cast<unsigned long long*>(next_count), error);
+  return cuda_status(cudaGetLastError());
+}
+
 }  // namespace mgbfs2
 
 extern "C" {
@@ -230,6 +373,17 @@ int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, const uint3
   return mgbfs2::expand_layer_into(degree, generators, permutations_host, frontier, count, bitmap, next,
                                    next_capacity, next_count, error, static_cast<unsigned char*>(scratch),
                                    scratch_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                                      const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
+                                      uint64_t next_capacity, uint64_t* next_count, uint32_t* error, void* stream) {
+  return mgbfs2::expand_layer_static(degree, generators, permutations_host, frontier, count, bitmap, next,
+                                     next_capacity, next_count, error, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

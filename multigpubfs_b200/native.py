@@ -112,6 +112,9 @@ _SIGNATURES = {
                                              C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_uint64, C.c_void_p]),
     "mgbfs2_expand_layer_scratch_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
+    "mgbfs2_expand_layer_bitmap_static": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
+                                                    C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p]),
 }
 
 
