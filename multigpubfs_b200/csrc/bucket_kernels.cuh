@@ -40,7 +40,6 @@ constexpr uint32_t kMaxEntries = 12;                 // staged successors per th
 constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kStageCap = kBlock * kMaxEntries;  // 3072
 constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per accept work item
-constexpr uint32_t kNoEntry = 0xffffffffu;
 
 struct RouteParams {
   const unsigned long long* frontier;
@@ -141,22 +140,22 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
     }
     for (uint32_t g0 = 0; g0 < p.gens; g0 += p.group) {
       const uint32_t g1 = min(p.gens, g0 + p.group);
-      const uint32_t entries = (g1 - g0) * p.ppt;
-      // Produce: successor, its shard, its rank within (warp, shard).
+      // Produce: successor, its shard, its rank within (warp, shard).  Only
+      // live successors take a slot: slot m of this thread is m*kBlock + tid.
+      uint32_t live = 0;
       for (uint32_t g = g0; g < g1; ++g) {
         const uint32_t tb = tbegin[g], te = tbegin[g + 1];
         const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           if (k >= static_cast<int>(p.ppt)) break;
-          const uint32_t slot = ((g - g0) * p.ppt + k) * kBlock + tid;
           if (val[k] && g != skip[k]) {
             const uint64_t c = apply_terms(par[k], terms, tb, te);
             const uint32_t s = prefix_shard<N, K>(c);
+            const uint32_t slot = live * kBlock + tid;
             sm.state[slot] = c | gtag;
             sm.tag[slot] = s | (atomicAdd(&sm.hist[warp][s], 1u) << 8);
-          } else {
-            sm.tag[slot] = kNoEntry;
+            ++live;
           }
         }
       }
@@ -197,21 +196,18 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
       uint32_t tg[kMaxEntries], pos[kMaxEntries];
 #pragma unroll
       for (uint32_t e = 0; e < kMaxEntries; ++e) {
-        tg[e] = kNoEntry;
-        if (e < entries) {
+        if (e < live) {
           const uint32_t slot = e * kBlock + tid;
           tg[e] = sm.tag[slot];
           st[e] = sm.state[slot];
-          if (tg[e] != kNoEntry) {
-            const uint32_t s = tg[e] & 0xffu;
-            pos[e] = sm.start[s] + sm.hist[warp][s] + (tg[e] >> 8);
-          }
+          const uint32_t s = tg[e] & 0xffu;
+          pos[e] = sm.start[s] + sm.hist[warp][s] + (tg[e] >> 8);
         }
       }
       __syncthreads();
 #pragma unroll
       for (uint32_t e = 0; e < kMaxEntries; ++e) {
-        if (tg[e] != kNoEntry) {
+        if (e < live) {
           sm.state[pos[e]] = st[e];
           sm.tag[pos[e]] = tg[e] & 0xffu;
         }
@@ -230,6 +226,28 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
       for (uint32_t i = tid; i < kWarpsPerBlock * kMaxShards; i += kBlock) (&sm.hist[0][0])[i] = 0;
       __syncthreads();
     }
+  }
+}
+
+// Lehmer rank of a state of shard `shard` (its first K digits): the shard's
+// base rank shard * (N-K)! plus the Horner sum of the remaining digits, which
+// stays below (N-K)! and so in 32 bits while N-K <= 12.
+template <int N, int K>
+__device__ __forceinline__ uint64_t lehmer_rank4_in_shard(uint64_t w, uint32_t shard) {
+  if constexpr (N - K > 12) {
+    return lehmer_rank4<N>(w);
+  } else {
+    constexpr uint32_t kFact[13] = {1u, 1u, 2u, 6u, 24u, 120u, 720u, 5040u, 40320u, 362880u, 3628800u, 39916800u,
+                                    479001600u};
+    const uint32_t lo_word = static_cast<uint32_t>(w), hi_word = static_cast<uint32_t>(w >> 32);
+    uint32_t used = 0, tail = 0;
+#pragma unroll
+    for (int i = 0; i < N - 1; ++i) {
+      const uint32_t s = (i < 8 ? (lo_word >> (4 * i)) : (hi_word >> (4 * (i - 8)))) & 15u;
+      if (i >= K) tail = tail * static_cast<uint32_t>(N - i) + (s - __popc(used & ((1u << s) - 1u)));
+      used |= 1u << s;
+    }
+    return static_cast<uint64_t>(shard) * kFact[N - K] + tail;
   }
 }
 
@@ -259,7 +277,7 @@ __global__ void __launch_bounds__(kBlock) count_lehmer(RouteParams p) {
     if (hist[s]) atomicAdd(&p.shard_count[s], static_cast<unsigned long long>(hist[s]));
 }
 
-template <int N>
+template <int N, int K>
 __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
   __shared__ unsigned long long win[kAcceptChunk];
   __shared__ unsigned long long item_prefix[kMaxShards + 1];
@@ -308,7 +326,7 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = round + k * kBlock + tid;
-        r[k] = lehmer_rank4<N>(w[k]);
+        r[k] = lehmer_rank4_in_shard<N, K>(w[k], s);
         old[k] = i < n ? atomicOr(&p.bitmap[r[k] >> 6], 1ull << (r[k] & 63)) : ~0ull;
       }
 #pragma unroll

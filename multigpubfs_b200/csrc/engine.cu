@@ -574,7 +574,7 @@ static void pick_bucket(uint32_t n, uint32_t prefix, RouteFn* route, AcceptFn* a
 #define MG_CASE(K)                                                       \
   case K:                                                                \
     *route = prefix == 1 ? route_lehmer<K, 1> : route_lehmer<K, 2>;      \
-    *accept = accept_lehmer<K>;                                          \
+    *accept = prefix == 1 ? accept_lehmer<K, 1> : accept_lehmer<K, 2>;   \
     return;
     MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
     MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)

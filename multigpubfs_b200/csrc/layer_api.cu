@@ -71,8 +71,8 @@ struct LayerKernels {
 
 template <int N>
 LayerKernels kernels_for(uint32_t prefix) {
-  if (prefix == 1) return {count_lehmer<N, 1>, route_lehmer<N, 1>, accept_lehmer<N>};
-  return {count_lehmer<N, 2>, route_lehmer<N, 2>, accept_lehmer<N>};
+  if (prefix == 1) return {count_lehmer<N, 1>, route_lehmer<N, 1>, accept_lehmer<N, 1>};
+  return {count_lehmer<N, 2>, route_lehmer<N, 2>, accept_lehmer<N, 2>};
 }
 
 bool pick_layer_kernels(uint32_t n, uint32_t prefix, LayerKernels* k) {

@@ -6,6 +6,7 @@ is present, every entry point raises ``NativeUnavailable``.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
@@ -129,7 +130,7 @@ def load(path: str | Path | None = None):
     with _LOCK:
         if _LIB is not None and path is None:
             return _LIB
-        target = Path(path) if path else LIBRARY
+        target = Path(path) if path else Path(os.environ.get("MGBFS2_LIBRARY", LIBRARY))
         if not target.exists():
             raise NativeUnavailable(f"libmgbfs2 not built: {target} (run python -m multigpubfs_b200.build)")
         try:
