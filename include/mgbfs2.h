@@ -254,6 +254,49 @@ MGBFS2_API int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t gener
                                                  uint64_t next_capacity, uint64_t* next_count, uint32_t* error,
                                                  void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched sweep: many BFS instances in one device-driven CUDA-graph loop.   */
+
+typedef struct mgbfs2_batch mgbfs2_batch;
+
+typedef struct {
+  uint32_t max_depth;       /* layer-table capacity per instance, 0 = 1024 */
+  uint32_t blocks_per_sm;   /* batch_expand blocks per SM, 0 = occupancy limit (the tuned shape) */
+  uint32_t host_loop;       /* 1 = host-driven layer loop (one sync per layer) instead of the graph loop */
+  uint32_t reserved;
+  uint64_t memory_bytes;    /* device bytes available to the waves, 0 = free memory minus reserve */
+  uint64_t reserve_bytes;   /* 0 = 2 GiB */
+  const uint64_t* predicted_capacity; /* per instance frontier capacity (learned planner); NULL or 0 = orbit bound */
+} mgbfs2_batch_options;
+
+typedef struct {
+  uint32_t instances, complete_instances, waves, redo_instances;
+  uint32_t graph_launches, kernel_launches, layer_steps, fatal;
+  uint64_t states, successors;
+  double seconds;           /* wall time of mgbfs2_batch_run */
+  double device_seconds;    /* CUDA-event time of the waves' layer loops */
+} mgbfs2_batch_status;
+
+/* Instances: permutation graphs of degree 2..15 with distinct labels and at
+ * most 16 generators (each gets an exact n!-bit Lehmer bitmap).  No reference
+ * counterpart as one launch: the reference runs graphs one after another
+ * through its resident worker pool, multigpubfs/generic_session.py:139. */
+MGBFS2_API int mgbfs2_batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int device, mgbfs2_batch** out,
+                                   char* error, size_t error_capacity);
+
+/* Runs every instance to completion in waves that fit the memory budget; each
+ * wave is ONE CUDA-graph launch whose WHILE node repeats {expand every active
+ * instance's layer, finalize} until the device finds no active instance.  An
+ * instance that overflows its (predicted) frontier capacity is rerun from depth
+ * 0 with its orbit bound, so tables never change. */
+MGBFS2_API int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, mgbfs2_batch_status* status);
+
+/* Layer table of one instance after mgbfs2_batch_run. */
+MGBFS2_API int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint64_t* sizes,
+                                        size_t capacity, size_t* count);
+
+MGBFS2_API void mgbfs2_batch_destroy(mgbfs2_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

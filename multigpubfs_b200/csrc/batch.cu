@@ -1,0 +1,611 @@
+// Batched sweep: many independent BFS instances (different degrees and
+// generator sets, very uneven sizes) advance together, one layer of all of
+// them per step, inside ONE CUDA-graph launch per wave:
+//
+//     WHILE (any instance active) { batch_expand ; batch_finalize }
+//
+// The loop condition is set on the device by batch_finalize
+// (cudaGraphSetConditional), so a wave costs one graph launch and one host
+// synchronisation, whatever its depth.  (The reference runs instances one
+// after another, multigpubfs/generic_session.py:139; its device-driven graph
+// loop precedent is cuda/generic_sorted_carry_graph.cuh:62-84.)
+//
+// Layout: every instance owns a Lehmer bitmap of n!/64 words and a segment of
+// `cap` words in each of the two frontier buffers.  The current frontier is
+// the concatenation of the instances' segments; a block maps its tile of the
+// virtual index space to (instance, local index) through an exclusive prefix
+// of the per-instance counts.  Winners are appended to their instance's
+// segment with one reservation per (warp, instance).  A segment overflow
+// stops that instance and marks it; the host reruns it from depth 0 with its
+// plain (orbit-bound) capacity in a later wave, so results never change.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/mgbfs2.h"
+#include "engine.h"
+
+#define MG_CHECK_BATCH(expr)                          \
+  do {                                                \
+    cudaError_t _e = (expr);                          \
+    if (_e != cudaSuccess) return cuda_status(_e);    \
+  } while (0)
+
+namespace mgbfs2 {
+namespace {
+
+constexpr uint32_t kBatchBlock = 256;
+constexpr uint32_t kMaxBatchGens = 16;
+enum : uint32_t { INST_ACTIVE = 0, INST_DONE = 1, INST_OVERFLOW = 2, INST_IDLE = 3 };
+
+struct BatchInst {
+  uint32_t n, gens, term_off, inv_off;  // term_off: first of gens + 1 offsets in tbegin
+  uint32_t gen_shift, status;           // parent-edge tag position (0 = none)
+  unsigned long long bitmap_off;        // first bitmap word
+  unsigned long long seg_off, seg_cap;  // frontier segment (same in both buffers)
+};
+
+struct BatchCtl {
+  unsigned long long total;  // entries in the current frontier (prefix[count])
+  uint32_t parity, depth, max_depth, error;
+};
+
+struct BatchParams {
+  BatchInst* inst;
+  uint32_t count, ppt;
+  const Term* terms;
+  const uint32_t* tbegin;   // absolute term offsets
+  const uint32_t* inverse;  // absolute generator index -> inverse generator index (within the instance)
+  unsigned long long* bitmap;
+  unsigned long long* buf[2];
+  unsigned long long* prefix;      // count + 1 entries: exclusive prefix of current counts
+  unsigned long long* next_count;  // per instance
+  unsigned long long* layers;      // count x max_depth
+  BatchCtl* ctl;
+};
+
+__device__ __forceinline__ uint32_t find_instance(const unsigned long long* prefix, uint32_t count,
+                                                  unsigned long long idx) {
+  uint32_t lo = 0, hi = count;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (prefix[mid] <= idx) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
+  const uint32_t parity = p.ctl->parity;
+  const unsigned long long total = p.ctl->total;
+  const unsigned long long* front = p.buf[parity];
+  unsigned long long* next = p.buf[parity ^ 1];
+  const uint32_t lane = lane_id();
+  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  // Uniform trip count per warp: lanes past the end stay in with valid = false.
+  for (unsigned long long base = (blockIdx.x * static_cast<unsigned long long>(blockDim.x)) + (threadIdx.x & ~31u);
+       base < total; base += stride) {
+    const unsigned long long idx = base + lane;
+    const bool valid = idx < total;
+    uint32_t i = 0, n = 0, gens = 0, toff = 0, ioff = 0, shift = 0, skip = 0xffffffffu;
+    unsigned long long w = 0;
+    BatchInst in{};
+    if (valid) {
+      i = find_instance(p.prefix, p.count, idx);
+      in = p.inst[i];
+      n = in.n;
+      gens = in.gens;
+      toff = in.term_off;
+      ioff = in.inv_off;
+      shift = in.gen_shift;
+      w = front[in.seg_off + (idx - p.prefix[i])];
+      const uint32_t tag = shift ? static_cast<uint32_t>(w >> shift) : 0u;
+      if (tag) skip = p.inverse[ioff + tag - 1];
+    }
+    // Generator loop bound: the warp's largest generator count.
+    uint32_t gmax = gens;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gmax = max(gmax, __shfl_xor_sync(kFullMask, gmax, o));
+    for (uint32_t g = 0; g < gmax; ++g) {
+      const bool live = valid && g < gens && g != skip;
+      bool won = false;
+      unsigned long long c = 0;
+      if (live) {
+        c = apply_terms(w, p.terms, p.tbegin[toff + g], p.tbegin[toff + g + 1]);
+        const uint64_t r = lehmer_rank4_n(c, n);
+        const unsigned long long bit = 1ull << (r & 63);
+        won = !(atomicOr(&p.bitmap[in.bitmap_off + (r >> 6)], bit) & bit);
+      }
+      // One reservation per (warp, instance) among the winners.
+      const unsigned winners = __ballot_sync(kFullMask, won);
+      if (winners) {
+        const unsigned peers = __match_any_sync(kFullMask, won ? i : 0xffffffffu) & winners;
+        if (won) {
+          const int leader = __ffs(peers) - 1;
+          unsigned long long at = 0;
+          if (static_cast<int>(lane) == leader)
+            at = atomicAdd(&p.next_count[i], static_cast<unsigned long long>(__popc(peers)));
+          at = __shfl_sync(peers, at, leader) + __popc(peers & lanemask_lt());
+          if (at < in.seg_cap)
+            next[in.seg_off + at] = c | (shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull);
+        }
+      }
+    }
+  }
+}
+
+// One block: record the layer, retire finished or overflowed instances, build
+// the prefix of the new counts, flip the buffers, decide whether to loop.
+__global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphConditionalHandle handle,
+                                                       int use_handle) {
+  __shared__ unsigned long long warp_sums[32];
+  __shared__ unsigned long long carry;
+  const uint32_t depth = p.ctl->depth;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < p.count; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    unsigned long long c = 0;
+    if (i < p.count) {
+      BatchInst& in = p.inst[i];
+      const unsigned long long produced = p.next_count[i];
+      p.next_count[i] = 0;
+      if (in.status == INST_ACTIVE) {
+        if (produced > in.seg_cap) {
+          in.status = INST_OVERFLOW;
+        } else if (produced == 0) {
+          in.status = INST_DONE;
+        } else if (depth + 1 >= p.ctl->max_depth) {
+          in.status = INST_OVERFLOW;
+          atomicOr(&p.ctl->error, ERR_FRONTIER_OVERFLOW);
+        } else {
+          p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth + depth + 1] = produced;
+          c = produced;
+        }
+      }
+    }
+    // Block-wide exclusive scan of c.
+    unsigned long long incl = c;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long up = __shfl_up_sync(kFullMask, incl, o);
+      if (lane >= static_cast<uint32_t>(o)) incl += up;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long v = lane < blockDim.x / 32 ? warp_sums[lane] : 0ull, x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long up = __shfl_up_sync(kFullMask, x, o);
+        if (lane >= static_cast<uint32_t>(o)) x += up;
+      }
+      if (lane < blockDim.x / 32) warp_sums[lane] = x - v;
+    }
+    __syncthreads();
+    if (i < p.count) p.prefix[i] = carry + warp_sums[warp] + incl - c;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += warp_sums[warp] + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    p.prefix[p.count] = carry;
+    p.ctl->total = carry;
+    p.ctl->parity ^= 1u;
+    p.ctl->depth = depth + 1;
+    if (use_handle) cudaGraphSetConditional(handle, carry > 0 ? 1u : 0u);
+  }
+}
+
+__global__ void batch_seed(BatchParams p) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.count; i += gridDim.x * blockDim.x) {
+    const BatchInst in = p.inst[i];
+    // Identity-coded start: code c at position c.  Its rank is 0.
+    unsigned long long start = 0;
+    for (uint32_t e = 0; e < in.n; ++e) start |= static_cast<unsigned long long>(e) << (4 * e);
+    p.buf[0][in.seg_off] = start;
+    p.bitmap[in.bitmap_off] |= 1ull;
+    p.prefix[i] = i;
+    p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth] = 1;
+    p.next_count[i] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    p.prefix[p.count] = p.count;
+    p.ctl->total = p.count;
+    p.ctl->parity = 0;
+    p.ctl->depth = 0;
+    p.ctl->error = 0;
+  }
+}
+
+uint64_t factorial(uint32_t n) {
+  uint64_t f = 1;
+  for (uint32_t i = 2; i <= n; ++i) f *= i;
+  return f;
+}
+
+}  // namespace
+
+// Host side of one batch.
+struct Batch {
+  struct Instance {
+    uint32_t n = 0, gens = 0;
+    std::vector<Term> terms;
+    std::vector<uint32_t> begin;   // gens + 1 relative offsets
+    std::vector<uint32_t> inverse; // gens entries
+    bool inverse_closed = false;
+    uint64_t orbit = 0;            // n!
+    std::vector<uint64_t> layers;
+    uint32_t status = INST_IDLE;
+    uint32_t runs = 0;
+  };
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 148;
+  std::vector<Instance> inst;
+  DeviceBuffer arena;
+  mgbfs2_batch_status last{};
+};
+
+static int validate_instance(const mgbfs2_graph_desc& d, Batch::Instance* out, std::string* why) {
+  if (d.kind != 0 || !d.permutations || !d.start) { *why = "BATCH_REQUIRES_PERMUTATION_ACTION"; return MGBFS2_UNSUPPORTED; }
+  const uint32_t n = d.elements;
+  if (n < 2 || n > 15) { *why = "BATCH_DEGREE"; return MGBFS2_UNSUPPORTED; }
+  if (!d.generators || d.generators > kMaxBatchGens) { *why = "BATCH_GENERATORS"; return MGBFS2_UNSUPPORTED; }
+  // Distinct labels: the instance is coded by sorted label order.
+  std::vector<int64_t> labels(d.start, d.start + n);
+  std::vector<int64_t> sorted = labels;
+  std::sort(sorted.begin(), sorted.end());
+  if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end()) {
+    *why = "BATCH_REQUIRES_DISTINCT_LABELS";
+    return MGBFS2_UNSUPPORTED;
+  }
+  // With distinct labels the layer table does not depend on the start: a
+  // state x (as codes) evolves by x -> x o g, and x = c o y maps the BFS from
+  // the start's coding c bijectively, layer by layer, onto the BFS of y from
+  // the identity.  Every instance therefore runs from the identity coding.
+  Batch::Instance in;
+  in.n = n;
+  in.gens = d.generators;
+  in.orbit = factorial(n);
+  in.begin.assign(1, 0);
+  std::map<std::vector<uint32_t>, uint32_t> index;
+  for (uint32_t k = 0; k < in.gens; ++k) {
+    std::vector<uint32_t> g(d.permutations + static_cast<size_t>(k) * n, d.permutations + static_cast<size_t>(k + 1) * n);
+    std::vector<uint8_t> seen(n, 0);
+    for (uint32_t v : g) {
+      if (v >= n || seen[v]) { *why = "GRAPH_PERMUTATION_GENERATOR"; return MGBFS2_INVALID_ARGUMENT; }
+      seen[v] = 1;
+    }
+    if (!index.count(g)) index[g] = k;
+    std::map<int, uint64_t> groups;
+    for (uint32_t i = 0; i < n; ++i) groups[static_cast<int>(g[i]) - static_cast<int>(i)] |= 15ull << (4 * i);
+    for (auto& kv : groups) {
+      const int shift = kv.first * 4;
+      in.terms.push_back(Term{kv.second, shift > 0 ? static_cast<uint32_t>(shift) : 0u,
+                              shift < 0 ? static_cast<uint32_t>(-shift) : 0u});
+    }
+    in.begin.push_back(static_cast<uint32_t>(in.terms.size()));
+  }
+  in.inverse_closed = true;
+  in.inverse.assign(in.gens, 0xffffffffu);
+  for (uint32_t k = 0; k < in.gens; ++k) {
+    std::vector<uint32_t> inv(n);
+    for (uint32_t i = 0; i < n; ++i) inv[d.permutations[static_cast<size_t>(k) * n + i]] = i;
+    auto it = index.find(inv);
+    if (it == index.end()) in.inverse_closed = false;
+    else in.inverse[k] = it->second;
+  }
+  if (!in.inverse_closed) std::fill(in.inverse.begin(), in.inverse.end(), 0xffffffffu);
+  *out = in;
+  return MGBFS2_OK;
+}
+
+static int batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int device, Batch** out, char* error,
+                        size_t cap) {
+  auto fail = [&](int rc, const std::string& why) {
+    if (error && cap) std::snprintf(error, cap, "%s", why.c_str());
+    return rc;
+  };
+  if (!graphs || !count || !out) return fail(MGBFS2_INVALID_ARGUMENT, "BATCH_ARGUMENT");
+  auto b = new Batch();
+  b->device = device;
+  b->inst.resize(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    std::string why;
+    const int rc = validate_instance(graphs[i], &b->inst[i], &why);
+    if (rc) {
+      delete b;
+      return fail(rc, "instance " + std::to_string(i) + ": " + why);
+    }
+  }
+  int rc = cuda_status(cudaSetDevice(device));
+  if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  if (rc) {
+    delete b;
+    return fail(rc, "CUDA_SETUP");
+  }
+  b->arena.stream = b->stream;
+  retain_pool_memory(device);
+  cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+  *out = b;
+  return MGBFS2_OK;
+}
+
+// Runs one wave (the instances in `ids`, with segment capacities `caps`).
+static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& caps, uint32_t max_depth,
+                    uint32_t ppt, bool use_graph, mgbfs2_batch_status* st, double* kernel_seconds) {
+  const uint32_t W = static_cast<uint32_t>(ids.size());
+  std::vector<BatchInst> host(W);
+  std::vector<Term> terms;
+  std::vector<uint32_t> tbegin, inverse;
+  uint64_t bitmap_words = 0, seg = 0;
+  for (uint32_t k = 0; k < W; ++k) {
+    const auto& in = b->inst[ids[k]];
+    BatchInst& h = host[k];
+    h.n = in.n;
+    h.gens = in.gens;
+    h.term_off = static_cast<uint32_t>(tbegin.size());
+    for (uint32_t x : in.begin) tbegin.push_back(static_cast<uint32_t>(terms.size()) + x);
+    terms.insert(terms.end(), in.terms.begin(), in.terms.end());
+    h.inv_off = static_cast<uint32_t>(inverse.size());
+    inverse.insert(inverse.end(), in.inverse.begin(), in.inverse.end());
+    h.gen_shift = in.inverse_closed ? 4 * in.n : 0;
+    h.status = INST_ACTIVE;
+    h.bitmap_off = bitmap_words;
+    bitmap_words += (in.orbit + 63) / 64;
+    h.seg_off = seg;
+    h.seg_cap = caps[k];
+    seg += caps[k] + 1;  // +1 keeps every segment non-empty
+  }
+  // Arena: instance table | terms | tbegin | inverse | prefix | next_count | layers | ctl | bitmaps | buf0 | buf1
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  size_t off = 0;
+  const size_t o_inst = off; off = al(off + W * sizeof(BatchInst));
+  const size_t o_terms = off; off = al(off + terms.size() * sizeof(Term) + 16);
+  const size_t o_tbegin = off; off = al(off + tbegin.size() * 4 + 4);
+  const size_t o_inv = off; off = al(off + inverse.size() * 4 + 4);
+  const size_t o_prefix = off; off = al(off + (W + 1) * 8);
+  const size_t o_next = off; off = al(off + W * 8);
+  const size_t o_layers = off; off = al(off + static_cast<size_t>(W) * max_depth * 8);
+  const size_t o_ctl = off; off = al(off + sizeof(BatchCtl));
+  const size_t o_bitmap = off; off = al(off + bitmap_words * 8);
+  const size_t o_buf0 = off; off = al(off + seg * 8);
+  const size_t o_buf1 = off; off = al(off + seg * 8);
+  int rc = b->arena.ensure(off);
+  if (rc) return rc;
+  char* base = static_cast<char*>(b->arena.ptr);
+  BatchCtl ctl{0, 0, 0, max_depth, 0};
+  MG_CHECK_BATCH(cudaMemcpyAsync(base + o_inst, host.data(), W * sizeof(BatchInst), cudaMemcpyHostToDevice, b->stream));
+  if (!terms.empty())
+    MG_CHECK_BATCH(cudaMemcpyAsync(base + o_terms, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
+  MG_CHECK_BATCH(cudaMemcpyAsync(base + o_tbegin, tbegin.data(), tbegin.size() * 4, cudaMemcpyHostToDevice, b->stream));
+  if (!inverse.empty())
+    MG_CHECK_BATCH(cudaMemcpyAsync(base + o_inv, inverse.data(), inverse.size() * 4, cudaMemcpyHostToDevice, b->stream));
+  MG_CHECK_BATCH(cudaMemcpyAsync(base + o_ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, b->stream));
+  MG_CHECK_BATCH(cudaMemsetAsync(base + o_layers, 0, static_cast<size_t>(W) * max_depth * 8, b->stream));
+  MG_CHECK_BATCH(cudaMemsetAsync(base + o_bitmap, 0, bitmap_words * 8, b->stream));
+  BatchParams p{};
+  p.inst = reinterpret_cast<BatchInst*>(base + o_inst);
+  p.count = W;
+  p.ppt = ppt;
+  p.terms = reinterpret_cast<const Term*>(base + o_terms);
+  p.tbegin = reinterpret_cast<const uint32_t*>(base + o_tbegin);
+  p.inverse = reinterpret_cast<const uint32_t*>(base + o_inv);
+  p.bitmap = reinterpret_cast<unsigned long long*>(base + o_bitmap);
+  p.buf[0] = reinterpret_cast<unsigned long long*>(base + o_buf0);
+  p.buf[1] = reinterpret_cast<unsigned long long*>(base + o_buf1);
+  p.prefix = reinterpret_cast<unsigned long long*>(base + o_prefix);
+  p.next_count = reinterpret_cast<unsigned long long*>(base + o_next);
+  p.layers = reinterpret_cast<unsigned long long*>(base + o_layers);
+  p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);
+  batch_seed<<<std::max<uint32_t>(1, (W + 255) / 256), 256, 0, b->stream>>>(p);
+  ++st->kernel_launches;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(batch_expand), kBatchBlock, 0);
+  // `ppt` here is the tuned blocks-per-SM of batch_expand (0 = occupancy limit).
+  const uint32_t grid = static_cast<uint32_t>((ppt ? static_cast<int>(ppt) : std::max(1, per_sm)) * b->sm_count);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, b->stream);
+  uint32_t layers_run = 0;
+  if (use_graph) {
+    cudaGraph_t graph;
+    MG_CHECK_BATCH(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle;
+    MG_CHECK_BATCH(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    MG_CHECK_BATCH(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t cap_stream;
+    MG_CHECK_BATCH(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    MG_CHECK_BATCH(cudaStreamBeginCaptureToGraph(cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    batch_expand<<<grid, kBatchBlock, 0, cap_stream>>>(p);
+    batch_finalize<<<1, 1024, 0, cap_stream>>>(p, handle, 1);
+    MG_CHECK_BATCH(cudaStreamEndCapture(cap_stream, &body));
+    cudaGraphExec_t exec;
+    MG_CHECK_BATCH(cudaGraphInstantiate(&exec, graph, 0));
+    MG_CHECK_BATCH(cudaGraphLaunch(exec, b->stream));
+    ++st->graph_launches;
+    MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap_stream);
+  } else {
+    for (;;) {
+      batch_expand<<<grid, kBatchBlock, 0, b->stream>>>(p);
+      batch_finalize<<<1, 1024, 0, b->stream>>>(p, cudaGraphConditionalHandle{}, 0);
+      st->kernel_launches += 2;
+      BatchCtl h{};
+      MG_CHECK_BATCH(cudaMemcpyAsync(&h, p.ctl, sizeof(h), cudaMemcpyDeviceToHost, b->stream));
+      MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
+      ++layers_run;
+      if (!h.total) break;
+    }
+  }
+  cudaEventRecord(e1, b->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  *kernel_seconds += ms * 1e-3;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // Results.
+  std::vector<BatchInst> done(W);
+  std::vector<unsigned long long> layers(static_cast<size_t>(W) * max_depth);
+  BatchCtl hc{};
+  MG_CHECK_BATCH(cudaMemcpyAsync(done.data(), p.inst, W * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream));
+  MG_CHECK_BATCH(cudaMemcpyAsync(layers.data(), p.layers, layers.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  MG_CHECK_BATCH(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, b->stream));
+  MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
+  if (use_graph) st->kernel_launches += 2 * hc.depth;
+  st->layer_steps += hc.depth;
+  for (uint32_t k = 0; k < W; ++k) {
+    auto& in = b->inst[ids[k]];
+    in.status = done[k].status;
+    in.runs++;
+    in.layers.clear();
+    if (in.status == INST_DONE) {
+      for (uint32_t d = 0; d < max_depth && layers[static_cast<size_t>(k) * max_depth + d]; ++d)
+        in.layers.push_back(layers[static_cast<size_t>(k) * max_depth + d]);
+    }
+  }
+  if (hc.error) st->fatal |= hc.error;
+  return MGBFS2_OK;
+}
+
+}  // namespace mgbfs2
+
+using mgbfs2::Batch;
+
+struct mgbfs2_batch {
+  Batch* impl;
+};
+
+extern "C" {
+
+int mgbfs2_batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int device, mgbfs2_batch** out, char* error,
+                        size_t error_capacity) {
+  if (!out) return MGBFS2_INVALID_ARGUMENT;
+  *out = nullptr;
+  Batch* b = nullptr;
+  const int rc = mgbfs2::batch_create(graphs, count, device, &b, error, error_capacity);
+  if (rc) return rc;
+  *out = new mgbfs2_batch{b};
+  return MGBFS2_OK;
+}
+
+int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, mgbfs2_batch_status* status) {
+  using namespace mgbfs2;
+  if (!batch) return MGBFS2_INVALID_ARGUMENT;
+  Batch* b = batch->impl;
+  mgbfs2_batch_options o{};
+  if (options) o = *options;
+  const uint32_t max_depth = o.max_depth ? o.max_depth : 1024;
+  const uint32_t ppt = o.blocks_per_sm;
+  const bool use_graph = o.host_loop == 0;
+  MG_CHECK_BATCH(cudaSetDevice(b->device));
+  size_t free_bytes = 0, total_bytes = 0;
+  MG_CHECK_BATCH(cudaMemGetInfo(&free_bytes, &total_bytes));
+  free_bytes += pool_idle_bytes(b->device) + b->arena.bytes;
+  const uint64_t reserve = o.reserve_bytes ? o.reserve_bytes : (2ull << 30);
+  uint64_t budget = o.memory_bytes ? o.memory_bytes : (free_bytes > reserve ? free_bytes - reserve : 0);
+  mgbfs2_batch_status st{};
+  const auto started = std::chrono::steady_clock::now();
+  double kernel_seconds = 0.0;
+  const uint32_t I = static_cast<uint32_t>(b->inst.size());
+  // Capacities: the plain planner reserves each instance's orbit bound; a
+  // caller-provided prediction (the learned planner) reserves less, and an
+  // instance that overflows it is rerun with the plain bound.
+  std::vector<uint64_t> cap(I);
+  for (uint32_t i = 0; i < I; ++i) {
+    cap[i] = b->inst[i].orbit;
+    if (o.predicted_capacity && o.predicted_capacity[i] > 0)
+      cap[i] = std::min<uint64_t>(cap[i], o.predicted_capacity[i]);
+    b->inst[i].status = INST_IDLE;
+    b->inst[i].runs = 0;
+    b->inst[i].layers.clear();
+  }
+  std::vector<uint32_t> pending(I);
+  for (uint32_t i = 0; i < I; ++i) pending[i] = i;
+  int rc = MGBFS2_OK;
+  while (!pending.empty() && !rc) {
+    // Fill a wave up to the memory budget (bitmap + two segments + tables).
+    std::vector<uint32_t> wave;
+    std::vector<uint64_t> caps;
+    uint64_t used = 1 << 20;
+    std::vector<uint32_t> later;
+    for (uint32_t i : pending) {
+      const uint64_t need = (b->inst[i].orbit + 63) / 64 * 8 + 2 * (cap[i] + 1) * 8 + 8ull * max_depth + 128;
+      if (wave.empty() || used + need <= budget) {
+        wave.push_back(i);
+        caps.push_back(cap[i]);
+        used += need;
+      } else {
+        later.push_back(i);
+      }
+    }
+    rc = run_wave(b, wave, caps, max_depth, ppt, use_graph, &st, &kernel_seconds);
+    ++st.waves;
+    for (uint32_t i : wave) {
+      if (b->inst[i].status == INST_OVERFLOW) {
+        if (cap[i] >= b->inst[i].orbit) {
+          rc = MGBFS2_CAPACITY;  // cannot happen with the orbit bound; keeps the loop finite
+          break;
+        }
+        cap[i] = b->inst[i].orbit;  // exact rerun with the plain bound
+        ++st.redo_instances;
+        later.push_back(i);
+      }
+    }
+    pending.swap(later);
+  }
+  for (uint32_t i = 0; i < I; ++i) {
+    for (uint64_t s : b->inst[i].layers) st.states += s;
+    st.successors += [&] {
+      uint64_t e = 0;
+      for (uint64_t s : b->inst[i].layers) e += s * b->inst[i].gens;
+      return e;
+    }();
+    if (b->inst[i].status == INST_DONE) ++st.complete_instances;
+  }
+  st.instances = I;
+  st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
+  st.device_seconds = kernel_seconds;
+  b->last = st;
+  if (status) *status = st;
+  return rc;
+}
+
+int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint64_t* sizes, size_t capacity,
+                             size_t* count) {
+  if (!batch || !count || instance >= batch->impl->inst.size()) return MGBFS2_INVALID_ARGUMENT;
+  const auto& layers = batch->impl->inst[instance].layers;
+  *count = layers.size();
+  for (size_t d = 0; d < layers.size() && d < capacity; ++d)
+    if (sizes) sizes[d] = layers[d];
+  return MGBFS2_OK;
+}
+
+void mgbfs2_batch_destroy(mgbfs2_batch* batch) {
+  if (!batch) return;
+  Batch* b = batch->impl;
+  cudaSetDevice(b->device);
+  b->arena.free();
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  delete batch;
+}
+
+}  // extern "C"

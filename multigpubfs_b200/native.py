@@ -84,6 +84,22 @@ class RunStatus(C.Structure):
                 ("device_seconds", C.c_double), ("kernel_seconds", C.c_double), ("visited_tests", C.c_uint64)]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("max_depth", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("host_loop", C.c_uint32),
+                ("reserved", C.c_uint32), ("memory_bytes", C.c_uint64), ("reserve_bytes", C.c_uint64),
+                ("predicted_capacity", C.POINTER(C.c_uint64))]
+
+
+class BatchStatus(C.Structure):
+    _fields_ = [("instances", C.c_uint32), ("complete_instances", C.c_uint32), ("waves", C.c_uint32),
+                ("redo_instances", C.c_uint32), ("graph_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
+                ("layer_steps", C.c_uint32), ("fatal", C.c_uint32), ("states", C.c_uint64),
+                ("successors", C.c_uint64), ("seconds", C.c_double), ("device_seconds", C.c_double)]
+
+    def to_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 LAYER_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint64, C.c_double)
 
 _SIGNATURES = {
@@ -116,6 +132,12 @@ _SIGNATURES = {
     "mgbfs2_expand_layer_bitmap_static": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
                                                     C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                                     C.c_void_p, C.c_void_p]),
+    "mgbfs2_batch_create": (C.c_int, [C.POINTER(GraphDesc), C.c_uint32, C.c_int, C.POINTER(C.c_void_p), C.c_char_p,
+                                      C.c_size_t]),
+    "mgbfs2_batch_run": (C.c_int, [C.c_void_p, C.POINTER(BatchOptions), C.POINTER(BatchStatus)]),
+    "mgbfs2_batch_layer_table": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.c_size_t,
+                                           C.POINTER(C.c_size_t)]),
+    "mgbfs2_batch_destroy": (None, [C.c_void_p]),
 }
 
 
