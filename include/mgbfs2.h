@@ -297,6 +297,27 @@ MGBFS2_API int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t inst
 
 MGBFS2_API void mgbfs2_batch_destroy(mgbfs2_batch* batch);
 
+/* ------------------------------------------------------------------------ */
+/* Planner network (learned planner): inputs -> 64 -> 64 -> 2, ReLU, one flat */
+/* fp32 parameter buffer W1[64][in] | b1 | W2[64][64] | b2 | W3[2][64] | b3.  */
+/* No reference counterpart (the reference plans with worst-case bounds and   */
+/* timed pilots: crates/mgbfs-runtime/src/generic_memory.rs:36-49,            */
+/* multigpubfs/autotune.py:276).  All device pointers, rows of `inputs` fp32. */
+
+MGBFS2_API uint32_t mgbfs2_mlp_param_count(uint32_t inputs);
+MGBFS2_API int mgbfs2_mlp_forward(uint32_t inputs, const float* params, const float* x, uint64_t batch, float* y,
+                                  void* stream);
+/* grad += d/dparams of sum_s (w0 (y_s0 - t_s0)^2 + w1 (y_s1 - t_s1)^2) / batch; *loss += that sum. */
+MGBFS2_API int mgbfs2_mlp_loss_grad(uint32_t inputs, const float* params, const float* x, const float* target,
+                                    float weight0, float weight1, uint64_t batch, float* grad, float* loss,
+                                    void* stream);
+MGBFS2_API int mgbfs2_mlp_adam(uint32_t count, float* params, const float* grad, float* m, float* v, float lr,
+                               float beta1, float beta2, float eps, uint32_t step, void* stream);
+MGBFS2_API int mgbfs2_mlp_to_bf16(uint32_t count, const float* params, void* params_bf16, void* stream);
+/* bf16 parameters and activations, fp32 accumulation. */
+MGBFS2_API int mgbfs2_mlp_infer_bf16(uint32_t inputs, const void* params_bf16, const float* x, uint64_t batch,
+                                     float* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -138,6 +138,14 @@ _SIGNATURES = {
     "mgbfs2_batch_layer_table": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.c_size_t,
                                            C.POINTER(C.c_size_t)]),
     "mgbfs2_batch_destroy": (None, [C.c_void_p]),
+    "mgbfs2_mlp_param_count": (C.c_uint32, [C.c_uint32]),
+    "mgbfs2_mlp_forward": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "mgbfs2_mlp_loss_grad": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                       C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mgbfs2_mlp_adam": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                  C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
+    "mgbfs2_mlp_to_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mgbfs2_mlp_infer_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
 }
 
 

@@ -1,0 +1,265 @@
+"""Learned planner: a small MLP that predicts the next BFS layer from the last
+layers and the generators, trained and evaluated by libmgbfs2's own kernels
+(csrc/mlp.cu); the plain worst-case planner stays the exact fallback.
+
+Features of instance i at depth d (16, all O(1)):
+    log1p |L_d|, log1p |L_{d-1}|, log1p |L_{d-2}|, log1p |L_{d-3}|,
+    log1p visited, log orbit bound, n/16, g/8, inverse-closed,
+    mean and max log generator order, mean fixed-point fraction,
+    mean cycle count / n, d/64, visited/orbit, log1p(g |L_d|)
+Targets: log1p |L_{d+1}| - log1p |L_d| (log growth) and the duplicate ratio
+1 - |L_{d+1}| / (g |L_d|).
+
+A rollout from |L_0| = 1 gives each instance's predicted layer profile; its
+peak times a margin sizes the instance's frontier in the batched sweep (an
+instance that overflows is rerun exactly with its orbit bound), and the
+profile picks the visited-set path of a single run.  Results never depend on
+the prediction.  There is no counterpart in the reference, which sizes
+buffers from worst-case bounds and timed pilot runs
+(crates/mgbfs-runtime/src/generic_memory.rs:36-49, multigpubfs/autotune.py:276).
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native
+
+INPUTS = 16
+
+
+# ---------------------------------------------------------------------------
+# Features.
+
+def _cycles(perm):
+    seen = [False] * len(perm)
+    lengths = []
+    for i in range(len(perm)):
+        if not seen[i]:
+            j, length = i, 0
+            while not seen[j]:
+                seen[j] = True
+                j = perm[j]
+                length += 1
+            lengths.append(length)
+    return lengths
+
+
+@dataclass
+class GraphStatics:
+    n: int
+    gens: int
+    inverse_closed: bool
+    log_orbit: float
+    mean_log_order: float
+    max_log_order: float
+    fixed_fraction: float
+    cycle_fraction: float
+
+    @property
+    def orbit(self):
+        return math.exp(self.log_orbit)
+
+
+def graph_statics(generators, start) -> GraphStatics:
+    n = len(start)
+    orders, fixed, cycles = [], [], []
+    for g in generators:
+        c = _cycles(g)
+        order = 1
+        for length in c:
+            order = order * length // math.gcd(order, length)
+        orders.append(math.log(order))
+        fixed.append(sum(1 for length in c if length == 1) / n)
+        cycles.append(len(c) / n)
+    gens = {tuple(g) for g in generators}
+    closed = all(tuple(np.argsort(g).tolist()) in gens for g in generators)
+    counts = {}
+    for v in start:
+        counts[v] = counts.get(v, 0) + 1
+    log_orbit = math.lgamma(n + 1) - sum(math.lgamma(c + 1) for c in counts.values())
+    return GraphStatics(n, len(generators), closed, log_orbit, float(np.mean(orders)), float(max(orders)),
+                        float(np.mean(fixed)), float(np.mean(cycles)))
+
+
+def features(st: GraphStatics, layers, d) -> list:
+    last = [math.log1p(layers[d - k]) if d - k >= 0 else 0.0 for k in range(4)]
+    visited = float(sum(layers[:d + 1]))
+    return last + [math.log1p(visited), st.log_orbit, st.n / 16.0, st.gens / 8.0, float(st.inverse_closed),
+                   st.mean_log_order, st.max_log_order, st.fixed_fraction, st.cycle_fraction, d / 64.0,
+                   visited / st.orbit, math.log1p(st.gens * layers[d])]
+
+
+def training_set(graphs, tables):
+    """(X, T) from complete layer tables: one row per (instance, depth),
+    including the final depth whose next layer is empty."""
+    X, T = [], []
+    for g, layers in zip(graphs, tables):
+        st = graph_statics(g["action"]["generators"], g["start"])
+        for d in range(len(layers)):
+            nxt = layers[d + 1] if d + 1 < len(layers) else 0
+            X.append(features(st, layers, d))
+            T.append([math.log1p(nxt) - math.log1p(layers[d]), 1.0 - nxt / (st.gens * layers[d])])
+    return np.asarray(X, dtype=np.float32), np.asarray(T, dtype=np.float32)
+
+
+# ---------------------------------------------------------------------------
+# The network, on the device.
+
+class PlannerNet:
+    def __init__(self, device: int = 0, seed: int = 0, params=None):
+        import torch
+        self.lib = native.require_device()
+        self.torch = torch
+        self.dev = torch.device("cuda", device)
+        self.count = int(self.lib.mgbfs2_mlp_param_count(INPUTS))
+        if params is None:
+            rng = np.random.default_rng(seed)
+            p = np.zeros(self.count, dtype=np.float32)
+            o = 0
+            for rows, cols in ((64, INPUTS), (64, 64), (2, 64)):
+                p[o:o + rows * cols] = rng.normal(0.0, math.sqrt(2.0 / cols), rows * cols)
+                o += rows * cols + rows
+            params = p
+        self.params = torch.tensor(np.asarray(params, dtype=np.float32), device=self.dev)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.step = 0
+        self.x_mean = np.zeros(INPUTS, dtype=np.float32)
+        self.x_scale = np.ones(INPUTS, dtype=np.float32)
+
+    def _stream(self):
+        return native.stream_handle()
+
+    def _x(self, X):
+        X = (np.asarray(X, dtype=np.float32) - self.x_mean) / self.x_scale
+        return self.torch.tensor(X, device=self.dev).contiguous()
+
+    def loss_and_grad(self, X, T, weights=(1.0, 1.0)):
+        """One fused forward/backward over (X, T); returns (loss, grad) as numpy."""
+        x = self._x(X)
+        t = self.torch.tensor(np.asarray(T, dtype=np.float32), device=self.dev).contiguous()
+        self.grad.zero_()
+        loss = self.torch.zeros(1, dtype=self.torch.float32, device=self.dev)
+        native.check(self.lib.mgbfs2_mlp_loss_grad(INPUTS, self.params.data_ptr(), x.data_ptr(), t.data_ptr(),
+                                                   float(weights[0]), float(weights[1]), x.shape[0],
+                                                   self.grad.data_ptr(), loss.data_ptr(), self._stream()),
+                     "mgbfs2_mlp_loss_grad")
+        return float(loss.item()), self.grad.cpu().numpy()
+
+    def fit(self, X, T, steps=1500, lr=3e-3, weights=(1.0, 1.0), batch=4096, seed=0):
+        """Adam on minibatches; normalisation statistics come from X.  Returns
+        the loss history (every 50 steps)."""
+        X = np.asarray(X, dtype=np.float32)
+        T = np.asarray(T, dtype=np.float32)
+        self.x_mean = X.mean(0)
+        self.x_scale = X.std(0) + 1e-3
+        x_all = self._x(X)
+        t_all = self.torch.tensor(T, device=self.dev).contiguous()
+        rng = np.random.default_rng(seed)
+        history = []
+        loss = self.torch.zeros(1, dtype=self.torch.float32, device=self.dev)
+        for step in range(steps):
+            if len(X) > batch:
+                idx = self.torch.tensor(rng.integers(0, len(X), batch), device=self.dev)
+                xb, tb = x_all[idx].contiguous(), t_all[idx].contiguous()
+            else:
+                xb, tb = x_all, t_all
+            self.grad.zero_()
+            loss.zero_()
+            native.check(self.lib.mgbfs2_mlp_loss_grad(INPUTS, self.params.data_ptr(), xb.data_ptr(), tb.data_ptr(),
+                                                       float(weights[0]), float(weights[1]), xb.shape[0],
+                                                       self.grad.data_ptr(), loss.data_ptr(), self._stream()),
+                         "mgbfs2_mlp_loss_grad")
+            self.step += 1
+            native.check(self.lib.mgbfs2_mlp_adam(self.count, self.params.data_ptr(), self.grad.data_ptr(),
+                                                  self.m.data_ptr(), self.v.data_ptr(), lr, 0.9, 0.999, 1e-8,
+                                                  self.step, self._stream()), "mgbfs2_mlp_adam")
+            if step % 50 == 0 or step == steps - 1:
+                history.append(float(loss.item()))
+        return history
+
+    def predict_fp32(self, X):
+        x = self._x(X)
+        y = self.torch.empty((x.shape[0], 2), dtype=self.torch.float32, device=self.dev)
+        native.check(self.lib.mgbfs2_mlp_forward(INPUTS, self.params.data_ptr(), x.data_ptr(), x.shape[0],
+                                                 y.data_ptr(), self._stream()), "mgbfs2_mlp_forward")
+        return y.cpu().numpy()
+
+    def predict(self, X):
+        """bf16 inference kernel."""
+        x = self._x(X)
+        q = self.torch.empty(self.count, dtype=self.torch.bfloat16, device=self.dev)
+        native.check(self.lib.mgbfs2_mlp_to_bf16(self.count, self.params.data_ptr(), q.data_ptr(), self._stream()),
+                     "mgbfs2_mlp_to_bf16")
+        y = self.torch.empty((x.shape[0], 2), dtype=self.torch.float32, device=self.dev)
+        native.check(self.lib.mgbfs2_mlp_infer_bf16(INPUTS, q.data_ptr(), x.data_ptr(), x.shape[0], y.data_ptr(),
+                                                    self._stream()), "mgbfs2_mlp_infer_bf16")
+        return y.cpu().numpy()
+
+    def to_json(self):
+        return json.dumps({"inputs": INPUTS, "params": self.params.cpu().numpy().tolist(),
+                           "x_mean": self.x_mean.tolist(), "x_scale": self.x_scale.tolist()})
+
+    @classmethod
+    def from_json(cls, text, device=0):
+        d = json.loads(text)
+        net = cls(device, params=np.asarray(d["params"], dtype=np.float32))
+        net.x_mean = np.asarray(d["x_mean"], dtype=np.float32)
+        net.x_scale = np.asarray(d["x_scale"], dtype=np.float32)
+        return net
+
+
+# ---------------------------------------------------------------------------
+# Using the prediction.
+
+def rollout(net: PlannerNet, graphs, max_depth=512):
+    """Predicted layer profiles of all graphs, stepped together (one bf16
+    inference launch per depth)."""
+    stats = [graph_statics(g["action"]["generators"], g["start"]) for g in graphs]
+    layers = [[1.0] for _ in graphs]
+    active = list(range(len(graphs)))
+    for d in range(max_depth):
+        if not active:
+            break
+        X = [features(stats[i], layers[i], d) for i in active]
+        y = net.predict(X)
+        still = []
+        for row, i in enumerate(active):
+            st = stats[i]
+            visited = sum(layers[i])
+            nxt = math.expm1(float(y[row, 0]) + math.log1p(layers[i][d]))
+            nxt = min(nxt, st.orbit - visited, st.gens * layers[i][d])
+            if nxt >= 0.5:
+                layers[i].append(nxt)
+                still.append(i)
+        active = still
+    return layers
+
+
+def predicted_capacities(net: PlannerNet, graphs, margin=1.5, floor=4096):
+    """Per-instance frontier capacity for the batched sweep."""
+    caps = []
+    for g, prof in zip(graphs, rollout(net, graphs)):
+        orbit = math.factorial(len(g["start"]))
+        caps.append(int(min(orbit, max(prof) * margin + floor)))
+    return caps
+
+
+def choose_path(net: PlannerNet, graph: dict) -> dict:
+    """Visited set and dedup mode of a single run from the predicted profile:
+    the exact bitmap when the predicted orbit fills at least 1/128 of the rank
+    domain, else the hash (three layer banks when inverse-closed); bucketed
+    layers when the predicted peak layer reaches the bucketing threshold."""
+    prof = rollout(net, [graph])[0]
+    st = graph_statics(graph["action"]["generators"], graph["start"])
+    total, peak = sum(prof), max(prof)
+    if total >= st.orbit / 128:
+        return {"visited": "bitmap", "dedup": "bucket" if peak * st.gens >= (1 << 22) else "atomic",
+                "predicted_states": total, "predicted_peak": peak}
+    return {"visited": "hash3" if st.inverse_closed else "hash", "dedup": "auto",
+            "predicted_states": total, "predicted_peak": peak}
