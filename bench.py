@@ -178,7 +178,8 @@ def reference_arm(args, rank):
     line = {"metric": "successors/s", "value": value, "unit": "successors/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[name]["desc"], "sample_layers": CPU_SAMPLE_LAYERS},
+            "config": {"workload": WORKLOADS.get(name, WORKLOADS["s13-lrx"])["desc"],
+                       "sample_layers": CPU_SAMPLE_LAYERS},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "successors/s", "cores": runs[0]["cores"], "kind": "port",
                              "sample": runs[0]["sample"]},
@@ -187,13 +188,99 @@ def reference_arm(args, rank):
     return 0
 
 
+def bench_sweep(args, local):
+    """Batched sweep: 512 instances (256 seeds x {directed, inverse-closed}),
+    one device-driven CUDA-graph loop per wave."""
+    import torch
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    torch.cuda.set_device(local)
+    graphs = workloads.sweep(512)
+    with BatchSweep(graphs, local) as sweep:
+        for _ in range(args.warmup):
+            sweep.run()
+        ref = sweep.layer_tables()
+        runs = [sweep.run() for _ in range(args.steps)]
+        assert sweep.layer_tables() == ref
+    dev = sum(r["device_seconds"] for r in runs) / len(runs)
+    succ, states = runs[0]["successors"], runs[0]["states"]
+    line = {"metric": "successors/s", "value": succ / dev, "unit": "successors/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "batched sweep: 512 instances (256 seeds x directed / inverse-closed), n in "
+                                   "{7,8,9,10}, 2-3 seeded random generators, exact per-instance Lehmer bitmaps, "
+                                   "one CUDA-graph WHILE loop per wave",
+                       "instances": len(graphs), "states_per_step": states, "successors_per_step": succ},
+            "settled_states_per_s": states / dev,
+            "wall_ms_per_step": sum(r["seconds"] for r in runs) / len(runs) * 1e3,
+            "waves": runs[0]["waves"], "graph_launches_per_step": runs[0]["graph_launches"],
+            "layer_steps": runs[0]["layer_steps"], "gpu_launches": sum(r["kernel_launches"] for r in runs)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_planner(args, local):
+    """Learned vs plain planner on the batched sweep of 128 S12 instances with
+    2-4 random generators plus inverses.  The network is trained by the
+    library's kernels on layer tables of the 512-instance sweep; the plain run
+    reserves each instance's orbit bound, the learned run its predicted peak
+    (exact rerun on overflow).  Both must produce identical tables."""
+    import math
+    import torch
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    from multigpubfs_b200.planner import PlannerNet, training_set, predicted_capacities, rollout
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    train = workloads.sweep(512)
+    with BatchSweep(train, local) as sw:
+        sw.run()
+        tables = sw.layer_tables()
+    X, T = training_set(train, tables)
+    net = PlannerNet(local, seed=0)
+    hist = net.fit(X, T, steps=2000, lr=3e-3)
+    train_s = time.perf_counter() - t0
+    graphs = [workloads.planner_instance(i) for i in range(args.instances)]
+    t1 = time.perf_counter()
+    caps = predicted_capacities(net, graphs)
+    predict_s = time.perf_counter() - t1
+    out = {}
+    with BatchSweep(graphs, local) as sw:
+        for name, capacities in (("plain", None), ("learned", caps)):
+            st = sw.run(capacities=capacities)
+            st["layer_tables"] = sw.layer_tables()
+            out[name] = st
+    same = out["plain"]["layer_tables"] == out["learned"]["layer_tables"]
+    peaks = [max(t) for t in out["plain"]["layer_tables"]]
+    prof = rollout(net, graphs)
+    err = sorted(abs(math.log(max(p) / max(1.0, q))) for p, q in zip(prof, peaks))
+    line = {"metric": "successors/s", "value": out["learned"]["successors"] / out["learned"]["seconds"],
+            "unit": "successors/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": out["learned"]["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"learned vs plain planner: {args.instances} S12 instances, 2-4 seeded random "
+                                   "generators plus inverses, batched sweep"},
+            "identical_tables": same,
+            "plain": {k: out["plain"][k] for k in ("seconds", "device_seconds", "waves", "redo_instances", "states",
+                                                   "successors")},
+            "learned": {k: out["learned"][k] for k in ("seconds", "device_seconds", "waves", "redo_instances",
+                                                       "states", "successors")},
+            "speedup_wall": out["plain"]["seconds"] / out["learned"]["seconds"],
+            "predictor": {"train_rows": int(len(X)), "loss_first": hist[0], "loss_last": hist[-1],
+                          "train_seconds": train_s, "predict_seconds": predict_s,
+                          "peak_abs_log_error_median": err[len(err) // 2], "peak_abs_log_error_max": err[-1]}}
+    print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["native", "reference"], default="native")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="s13-lrx")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep512", "planner-s12"], default="s13-lrx")
+    ap.add_argument("--instances", type=int, default=128, help="planner-s12: number of S12 instances")
     ap.add_argument("--dedup", default=None)
     ap.add_argument("--visited", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -203,6 +290,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank)
+    if args.workload == "sweep512":
+        return bench_sweep(args, local)
+    if args.workload == "planner-s12":
+        return bench_planner(args, local)
 
     import torch
     import torch.distributed as dist

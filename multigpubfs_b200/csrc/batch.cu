@@ -377,7 +377,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const size_t o_bitmap = off; off = al(off + bitmap_words * 8);
   const size_t o_buf0 = off; off = al(off + seg * 8);
   const size_t o_buf1 = off; off = al(off + seg * 8);
-  int rc = b->arena.ensure(off);
+  // Exact size: waves are planned against the memory budget, so no headroom.
+  int rc = b->arena.ensure(off, true);
   if (rc) return rc;
   char* base = static_cast<char*>(b->arena.ptr);
   BatchCtl ctl{0, 0, 0, max_depth, 0};

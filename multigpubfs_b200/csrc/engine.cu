@@ -383,9 +383,9 @@ void Graph::release() {
 // keeps freed memory reserved (release threshold = max) so that regrowing a
 // buffer, or a new graph handle in the same process, reuses it without device
 // synchronisation.  Growth is geometric (x1.5) so a BFS regrows O(log) times.
-int DeviceBuffer::ensure(size_t want) {
+int DeviceBuffer::ensure(size_t want, bool exact) {
   if (want <= bytes) return MGBFS2_OK;
-  const size_t grown = std::max(want, bytes + bytes / 2);
+  const size_t grown = exact ? want : std::max(want, bytes + bytes / 2);
   free();
   void* p = nullptr;
   cudaError_t e = cudaMallocAsync(&p, grown, stream);

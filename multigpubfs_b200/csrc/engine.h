@@ -18,7 +18,7 @@ struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
   cudaStream_t stream = nullptr;
-  int ensure(size_t want);
+  int ensure(size_t want, bool exact = false);  // exact: no geometric headroom
   void free();
 };
 
