@@ -318,6 +318,14 @@ MGBFS2_API int mgbfs2_mlp_to_bf16(uint32_t count, const float* params, void* par
 MGBFS2_API int mgbfs2_mlp_infer_bf16(uint32_t inputs, const void* params_bf16, const float* x, uint64_t batch,
                                      float* y, void* stream);
 
+/* Order of the group generated by `generators` permutations of {0..n-1}
+ * (row-major, g[i] = image of i; n <= 20), by deterministic Schreier-Sims on
+ * the host.  With distinct labels it is the exact number of states a BFS
+ * settles; the learned planner uses it as the orbit size of its features.  The
+ * reference bounds the state space by the multinomial n!/prod(c!) instead
+ * (crates/mgbfs-runtime/src/generic_memory.rs:82-108). */
+MGBFS2_API int mgbfs2_group_order(const uint32_t* permutations, uint32_t n, uint32_t generators, uint64_t* order);
+
 #ifdef __cplusplus
 }
 #endif

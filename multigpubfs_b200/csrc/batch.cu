@@ -12,10 +12,12 @@
 //
 // Layout: every instance owns a Lehmer bitmap of n!/64 words and a segment of
 // `cap` words in each of the two frontier buffers.  The current frontier is
-// the concatenation of the instances' segments; a block maps its tile of the
-// virtual index space to (instance, local index) through an exclusive prefix
-// of the per-instance counts.  Winners are appended to their instance's
-// segment with one reservation per (warp, instance).  A segment overflow
+// cut into tiles of kBatchTile entries that never straddle two instances; a
+// block maps a tile index to (instance, local tile) through an exclusive
+// prefix of the per-instance tile counts, so the degree, the generator
+// program and the segment are uniform over the block (the rank is unrolled
+// for that degree).  Winners are staged in shared memory and appended to the
+// instance's segment with one reservation per block flush.  A segment overflow
 // stops that instance and marks it; the host reruns it from depth 0 with its
 // plain (orbit-bound) capacity in a later wave, so results never change.
 #include <algorithm>
@@ -39,7 +41,11 @@ namespace mgbfs2 {
 namespace {
 
 constexpr uint32_t kBatchBlock = 256;
+constexpr uint32_t kBatchPpt = 4;                         // frontier entries per thread per tile
+constexpr uint32_t kBatchTile = kBatchBlock * kBatchPpt;  // entries per tile (one instance per tile)
+constexpr uint32_t kBatchOut = 4096;                      // winners staged in shared memory per block
 constexpr uint32_t kMaxBatchGens = 16;
+constexpr uint32_t kMaxBatchTerms = kMaxBatchGens * 15;   // <= n distinct displacements per generator
 enum : uint32_t { INST_ACTIVE = 0, INST_DONE = 1, INST_OVERFLOW = 2, INST_IDLE = 3 };
 
 struct BatchInst {
@@ -50,22 +56,36 @@ struct BatchInst {
 };
 
 struct BatchCtl {
-  unsigned long long total;  // entries in the current frontier (prefix[count])
+  unsigned long long total;  // entries in the current frontier
+  unsigned long long tiles;      // tiles of the current frontier (tile_prefix[count])
+  unsigned long long next_tile;  // work counter of batch_expand, reset by every finalize
   uint32_t parity, depth, max_depth, error;
 };
 
 struct BatchParams {
   BatchInst* inst;
-  uint32_t count, ppt;
+  uint32_t count, pad;
   const Term* terms;
   const uint32_t* tbegin;   // absolute term offsets
   const uint32_t* inverse;  // absolute generator index -> inverse generator index (within the instance)
   unsigned long long* bitmap;
   unsigned long long* buf[2];
-  unsigned long long* prefix;      // count + 1 entries: exclusive prefix of current counts
-  unsigned long long* next_count;  // per instance
-  unsigned long long* layers;      // count x max_depth
+  unsigned long long* tile_prefix;  // count + 1 entries: exclusive prefix of per-instance tile counts
+  unsigned long long* cur_count;    // per instance: entries in the current frontier
+  unsigned long long* next_count;   // per instance: winners appended to the next frontier
+  unsigned long long* layers;       // count x max_depth
   BatchCtl* ctl;
+};
+
+// Per-block state: the instance of the current tile, its generator program,
+// and the staged winners.
+struct BatchSmem {
+  unsigned long long out[kBatchOut];
+  Term terms[kMaxBatchTerms];
+  uint32_t begin[kMaxBatchGens + 1];
+  uint32_t inverse[kMaxBatchGens];
+  unsigned long long bitmap_off, seg_off, seg_cap, count, tile, local_tile, out_base;
+  uint32_t inst, found, n, gens, shift, out_count;
 };
 
 __device__ __forceinline__ uint32_t find_instance(const unsigned long long* prefix, uint32_t count,
@@ -79,73 +99,167 @@ __device__ __forceinline__ uint32_t find_instance(const unsigned long long* pref
   return lo;
 }
 
-__global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
-  const uint32_t parity = p.ctl->parity;
-  const unsigned long long total = p.ctl->total;
-  const unsigned long long* front = p.buf[parity];
-  unsigned long long* next = p.buf[parity ^ 1];
+// Appends the block's staged winners to the current instance's next segment
+// with one reservation.  Positions at or past the segment's capacity are not
+// written; batch_finalize sees the count above capacity and retires the
+// instance as overflowed.  Called by all threads of the block.
+// The pointers a tile needs, passed by value (a reference to the kernel
+// parameter block would copy it to local memory).
+struct TileArgs {
+  const unsigned long long* front;
+  unsigned long long* next;
+  unsigned long long* bitmap;
+  unsigned long long* next_count;
+};
+
+__device__ __forceinline__ void batch_flush(const TileArgs a, BatchSmem& s) {
+  __syncthreads();
+  const uint32_t n = s.out_count;
+  if (threadIdx.x == 0 && n) s.out_base = atomicAdd(&a.next_count[s.inst], static_cast<unsigned long long>(n));
+  __syncthreads();
+  const unsigned long long base = s.out_base, cap = s.seg_cap;
+  unsigned long long* seg = a.next + s.seg_off;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
+    if (base + k < cap) seg[base + k] = s.out[k];
+  __syncthreads();
+  if (threadIdx.x == 0) s.out_count = 0;
+  __syncthreads();
+}
+
+// One tile (kBatchTile consecutive entries of one instance's frontier) with a
+// compile-time degree, so the Lehmer rank is fully unrolled.
+template <int N>
+__device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
   const uint32_t lane = lane_id();
-  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
-  // Uniform trip count per warp: lanes past the end stay in with valid = false.
-  for (unsigned long long base = (blockIdx.x * static_cast<unsigned long long>(blockDim.x)) + (threadIdx.x & ~31u);
-       base < total; base += stride) {
-    const unsigned long long idx = base + lane;
-    const bool valid = idx < total;
-    uint32_t i = 0, n = 0, gens = 0, toff = 0, ioff = 0, shift = 0, skip = 0xffffffffu;
-    unsigned long long w = 0;
-    BatchInst in{};
-    if (valid) {
-      i = find_instance(p.prefix, p.count, idx);
-      in = p.inst[i];
-      n = in.n;
-      gens = in.gens;
-      toff = in.term_off;
-      ioff = in.inv_off;
-      shift = in.gen_shift;
-      w = front[in.seg_off + (idx - p.prefix[i])];
-      const uint32_t tag = shift ? static_cast<uint32_t>(w >> shift) : 0u;
-      if (tag) skip = p.inverse[ioff + tag - 1];
-    }
-    // Generator loop bound: the warp's largest generator count.
-    uint32_t gmax = gens;
+  const unsigned long long count = s.count, base = s.local_tile * kBatchTile;
+  const uint32_t gens = s.gens, shift = s.shift;
+  const unsigned long long* seg = a.front + s.seg_off;
+  unsigned long long* bitmap = a.bitmap + s.bitmap_off;
+  uint64_t par[kBatchPpt];
+  uint32_t skip[kBatchPpt];
+  bool val[kBatchPpt];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) gmax = max(gmax, __shfl_xor_sync(kFullMask, gmax, o));
-    for (uint32_t g = 0; g < gmax; ++g) {
-      const bool live = valid && g < gens && g != skip;
+  for (uint32_t k = 0; k < kBatchPpt; ++k) {
+    const unsigned long long idx = base + k * kBatchBlock + threadIdx.x;
+    val[k] = idx < count;
+    par[k] = val[k] ? seg[idx] : 0ull;
+    const uint32_t tag = shift ? static_cast<uint32_t>(par[k] >> shift) : 0u;
+    skip[k] = tag ? s.inverse[tag - 1] : 0xffffffffu;
+    if (shift) par[k] &= (1ull << shift) - 1ull;
+  }
+  for (uint32_t g = 0; g < gens; ++g) {
+    const uint32_t tb = s.begin[g], te = s.begin[g + 1];
+    const unsigned long long gtag = shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull;
+#pragma unroll
+    for (uint32_t k = 0; k < kBatchPpt; ++k) {
+      const bool live = val[k] && g != skip[k];
       bool won = false;
-      unsigned long long c = 0;
+      uint64_t c = 0;
       if (live) {
-        c = apply_terms(w, p.terms, p.tbegin[toff + g], p.tbegin[toff + g + 1]);
-        const uint64_t r = lehmer_rank4_n(c, n);
+        c = apply_terms(par[k], s.terms, tb, te);
+        const uint64_t r = lehmer_rank4<N>(c);
         const unsigned long long bit = 1ull << (r & 63);
-        won = !(atomicOr(&p.bitmap[in.bitmap_off + (r >> 6)], bit) & bit);
+        won = !(atomicOr(&bitmap[r >> 6], bit) & bit);
       }
-      // One reservation per (warp, instance) among the winners.
-      const unsigned winners = __ballot_sync(kFullMask, won);
-      if (winners) {
-        const unsigned peers = __match_any_sync(kFullMask, won ? i : 0xffffffffu) & winners;
-        if (won) {
-          const int leader = __ffs(peers) - 1;
-          unsigned long long at = 0;
-          if (static_cast<int>(lane) == leader)
-            at = atomicAdd(&p.next_count[i], static_cast<unsigned long long>(__popc(peers)));
-          at = __shfl_sync(peers, at, leader) + __popc(peers & lanemask_lt());
-          if (at < in.seg_cap)
-            next[in.seg_off + at] = c | (shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull);
-        }
+      const unsigned m = __ballot_sync(kFullMask, won);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t at = 0;
+        if (static_cast<int>(lane) == leader) at = atomicAdd(&s.out_count, static_cast<uint32_t>(__popc(m)));
+        at = __shfl_sync(kFullMask, at, leader);
+        if (won) s.out[at + __popc(m & lanemask_lt())] = c | gtag;
       }
+    }
+    if (g + 1 < gens) {
+      __syncthreads();
+      const uint32_t pending = s.out_count;
+      __syncthreads();
+      if (pending + kBatchTile > kBatchOut) batch_flush(a, s);
+    }
+  }
+  batch_flush(a, s);
+}
+
+// Persistent expansion of one layer of every active instance.  The frontier
+// is cut into per-instance tiles; a block takes the next tile from a device
+// counter (so all blocks stay within a window of about one tile each, i.e.
+// on one or two instances' bitmaps, which then stay in L2 even when the
+// wave's bitmaps together do not fit), finds the tile's instance by binary
+// search of the tile prefix, loads that
+// instance's generator program into shared memory when it changes, and
+// stages its winners for one segment reservation per flush.
+__global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
+  __shared__ BatchSmem s;
+  const uint32_t parity = p.ctl->parity;
+  const unsigned long long tiles = p.ctl->tiles;
+  // Select, not index: a runtime index into the parameter block would copy it
+  // to local memory.
+  const TileArgs a{parity ? p.buf[1] : p.buf[0], parity ? p.buf[0] : p.buf[1], p.bitmap, p.next_count};
+  if (threadIdx.x == 0) {
+    s.out_count = 0;
+    s.inst = 0xffffffffu;
+  }
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned long long t = atomicAdd(&p.ctl->next_tile, 1ull);
+      s.tile = t;
+      if (t < tiles) {
+        const uint32_t i = find_instance(p.tile_prefix, p.count, t);
+        s.found = i;
+        s.local_tile = t - p.tile_prefix[i];
+      }
+    }
+    __syncthreads();
+    if (s.tile >= tiles) break;  // block-uniform
+    const uint32_t i = s.found;
+    if (i != s.inst) {  // block-uniform: every thread read the same s.found and s.inst
+      __syncthreads();
+      const BatchInst in = p.inst[i];
+      const uint32_t t0 = p.tbegin[in.term_off], t1 = p.tbegin[in.term_off + in.gens];
+      for (uint32_t k = threadIdx.x; k < t1 - t0; k += blockDim.x) s.terms[k] = p.terms[t0 + k];
+      for (uint32_t k = threadIdx.x; k <= in.gens; k += blockDim.x) s.begin[k] = p.tbegin[in.term_off + k] - t0;
+      for (uint32_t k = threadIdx.x; k < in.gens; k += blockDim.x) s.inverse[k] = p.inverse[in.inv_off + k];
+      if (threadIdx.x == 0) {
+        s.inst = i;
+        s.n = in.n;
+        s.gens = in.gens;
+        s.shift = in.gen_shift;
+        s.bitmap_off = in.bitmap_off;
+        s.seg_off = in.seg_off;
+        s.seg_cap = in.seg_cap;
+        s.count = p.cur_count[i];
+      }
+      __syncthreads();
+    }
+    switch (s.n) {
+      case 2: batch_tile<2>(a, s); break;
+      case 3: batch_tile<3>(a, s); break;
+      case 4: batch_tile<4>(a, s); break;
+      case 5: batch_tile<5>(a, s); break;
+      case 6: batch_tile<6>(a, s); break;
+      case 7: batch_tile<7>(a, s); break;
+      case 8: batch_tile<8>(a, s); break;
+      case 9: batch_tile<9>(a, s); break;
+      case 10: batch_tile<10>(a, s); break;
+      case 11: batch_tile<11>(a, s); break;
+      case 12: batch_tile<12>(a, s); break;
+      case 13: batch_tile<13>(a, s); break;
+      case 14: batch_tile<14>(a, s); break;
+      default: batch_tile<15>(a, s); break;
     }
   }
 }
 
 // One block: record the layer, retire finished or overflowed instances, build
-// the prefix of the new counts, flip the buffers, decide whether to loop.
+// the prefix of the new per-instance tile counts, flip the buffers, decide
+// whether to loop.
 __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphConditionalHandle handle,
                                                        int use_handle) {
   __shared__ unsigned long long warp_sums[32];
-  __shared__ unsigned long long carry;
+  __shared__ unsigned long long carry, entries;
   const uint32_t depth = p.ctl->depth;
-  if (threadIdx.x == 0) carry = 0;
+  if (threadIdx.x == 0) carry = entries = 0;
   __syncthreads();
   for (uint32_t base = 0; base < p.count; base += blockDim.x) {
     const uint32_t i = base + threadIdx.x;
@@ -164,9 +278,11 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
           atomicOr(&p.ctl->error, ERR_FRONTIER_OVERFLOW);
         } else {
           p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth + depth + 1] = produced;
-          c = produced;
+          c = (produced + kBatchTile - 1) / kBatchTile;
+          atomicAdd(&entries, produced);
         }
       }
+      p.cur_count[i] = c ? produced : 0ull;
     }
     // Block-wide exclusive scan of c.
     unsigned long long incl = c;
@@ -188,14 +304,16 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
       if (lane < blockDim.x / 32) warp_sums[lane] = x - v;
     }
     __syncthreads();
-    if (i < p.count) p.prefix[i] = carry + warp_sums[warp] + incl - c;
+    if (i < p.count) p.tile_prefix[i] = carry + warp_sums[warp] + incl - c;
     __syncthreads();
     if (threadIdx.x == blockDim.x - 1) carry += warp_sums[warp] + incl;
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    p.prefix[p.count] = carry;
-    p.ctl->total = carry;
+    p.tile_prefix[p.count] = carry;
+    p.ctl->tiles = carry;
+    p.ctl->next_tile = 0;
+    p.ctl->total = entries;
     p.ctl->parity ^= 1u;
     p.ctl->depth = depth + 1;
     if (use_handle) cudaGraphSetConditional(handle, carry > 0 ? 1u : 0u);
@@ -210,12 +328,15 @@ __global__ void batch_seed(BatchParams p) {
     for (uint32_t e = 0; e < in.n; ++e) start |= static_cast<unsigned long long>(e) << (4 * e);
     p.buf[0][in.seg_off] = start;
     p.bitmap[in.bitmap_off] |= 1ull;
-    p.prefix[i] = i;
+    p.tile_prefix[i] = i;  // one entry, one tile per instance
+    p.cur_count[i] = 1;
     p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth] = 1;
     p.next_count[i] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    p.prefix[p.count] = p.count;
+    p.tile_prefix[p.count] = p.count;
+    p.ctl->tiles = p.count;
+    p.ctl->next_tile = 0;
     p.ctl->total = p.count;
     p.ctl->parity = 0;
     p.ctl->depth = 0;
@@ -363,7 +484,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     h.seg_cap = caps[k];
     seg += caps[k] + 1;  // +1 keeps every segment non-empty
   }
-  // Arena: instance table | terms | tbegin | inverse | prefix | next_count | layers | ctl | bitmaps | buf0 | buf1
+  // Arena: instance table | terms | tbegin | inverse | tile prefix | counts | next counts | layers | ctl |
+  // bitmaps | buf0 | buf1
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   size_t off = 0;
   const size_t o_inst = off; off = al(off + W * sizeof(BatchInst));
@@ -371,6 +493,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const size_t o_tbegin = off; off = al(off + tbegin.size() * 4 + 4);
   const size_t o_inv = off; off = al(off + inverse.size() * 4 + 4);
   const size_t o_prefix = off; off = al(off + (W + 1) * 8);
+  const size_t o_cur = off; off = al(off + W * 8);
   const size_t o_next = off; off = al(off + W * 8);
   const size_t o_layers = off; off = al(off + static_cast<size_t>(W) * max_depth * 8);
   const size_t o_ctl = off; off = al(off + sizeof(BatchCtl));
@@ -381,7 +504,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   int rc = b->arena.ensure(off, true);
   if (rc) return rc;
   char* base = static_cast<char*>(b->arena.ptr);
-  BatchCtl ctl{0, 0, 0, max_depth, 0};
+  BatchCtl ctl{};
+  ctl.max_depth = max_depth;
   MG_CHECK_BATCH(cudaMemcpyAsync(base + o_inst, host.data(), W * sizeof(BatchInst), cudaMemcpyHostToDevice, b->stream));
   if (!terms.empty())
     MG_CHECK_BATCH(cudaMemcpyAsync(base + o_terms, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
@@ -394,14 +518,14 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   BatchParams p{};
   p.inst = reinterpret_cast<BatchInst*>(base + o_inst);
   p.count = W;
-  p.ppt = ppt;
   p.terms = reinterpret_cast<const Term*>(base + o_terms);
   p.tbegin = reinterpret_cast<const uint32_t*>(base + o_tbegin);
   p.inverse = reinterpret_cast<const uint32_t*>(base + o_inv);
   p.bitmap = reinterpret_cast<unsigned long long*>(base + o_bitmap);
   p.buf[0] = reinterpret_cast<unsigned long long*>(base + o_buf0);
   p.buf[1] = reinterpret_cast<unsigned long long*>(base + o_buf1);
-  p.prefix = reinterpret_cast<unsigned long long*>(base + o_prefix);
+  p.tile_prefix = reinterpret_cast<unsigned long long*>(base + o_prefix);
+  p.cur_count = reinterpret_cast<unsigned long long*>(base + o_cur);
   p.next_count = reinterpret_cast<unsigned long long*>(base + o_next);
   p.layers = reinterpret_cast<unsigned long long*>(base + o_layers);
   p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);

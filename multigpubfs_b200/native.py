@@ -146,7 +146,19 @@ _SIGNATURES = {
                                   C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
     "mgbfs2_mlp_to_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mgbfs2_mlp_infer_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "mgbfs2_group_order": (C.c_int, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
 }
+
+
+def group_order(generators) -> int:
+    """Order of the permutation group the generators generate (host
+    Schreier-Sims in libmgbfs2; no device needed)."""
+    gens = [list(g) for g in generators]
+    n = len(gens[0]) if gens else 1
+    flat = (C.c_uint32 * max(1, n * len(gens)))(*[x for g in gens for x in g])
+    out = C.c_uint64()
+    check(load().mgbfs2_group_order(flat, n, len(gens), C.byref(out)), "mgbfs2_group_order")
+    return int(out.value)
 
 
 def exported_symbols():

@@ -4,7 +4,8 @@ layers and the generators, trained and evaluated by libmgbfs2's own kernels
 
 Features of instance i at depth d (16, all O(1)):
     log1p |L_d|, log1p |L_{d-1}|, log1p |L_{d-2}|, log1p |L_{d-3}|,
-    log1p visited, log orbit bound, n/16, g/8, inverse-closed,
+    log1p visited, log orbit (exact group order by Schreier-Sims for distinct
+    labels, else the multinomial bound), n/16, g/8, inverse-closed,
     mean and max log generator order, mean fixed-point fraction,
     mean cycle count / n, d/64, visited/orbit, log1p(g |L_d|)
 Targets: log1p |L_{d+1}| - log1p |L_d| (log growth) and the duplicate ratio
@@ -80,7 +81,11 @@ def graph_statics(generators, start) -> GraphStatics:
     counts = {}
     for v in start:
         counts[v] = counts.get(v, 0) + 1
-    log_orbit = math.lgamma(n + 1) - sum(math.lgamma(c + 1) for c in counts.values())
+    if len(counts) == n and n <= 20:
+        # Distinct labels: the BFS settles exactly |<generators>| states.
+        log_orbit = math.log(native.group_order(generators))
+    else:
+        log_orbit = math.lgamma(n + 1) - sum(math.lgamma(c + 1) for c in counts.values())
     return GraphStatics(n, len(generators), closed, log_orbit, float(np.mean(orders)), float(max(orders)),
                         float(np.mean(fixed)), float(np.mean(cycles)))
 
@@ -221,33 +226,54 @@ def rollout(net: PlannerNet, graphs, max_depth=512):
     """Predicted layer profiles of all graphs, stepped together (one bf16
     inference launch per depth)."""
     stats = [graph_statics(g["action"]["generators"], g["start"]) for g in graphs]
+    # The columns of `features`, built for all active instances at once.
+    static = np.array([[st.log_orbit, st.n / 16.0, st.gens / 8.0, float(st.inverse_closed), st.mean_log_order,
+                        st.max_log_order, st.fixed_fraction, st.cycle_fraction] for st in stats], dtype=np.float64)
+    static = static.reshape(len(graphs), 8)
+    gens = np.array([st.gens for st in stats], dtype=np.float64)
+    orbit = np.exp(static[:, 0])
+    last = np.zeros((len(graphs), 4))  # |L_d|, |L_d-1|, |L_d-2|, |L_d-3| (0 before depth 0)
+    last[:, 0] = 1.0
+    visited = np.ones(len(graphs))
     layers = [[1.0] for _ in graphs]
-    active = list(range(len(graphs)))
+    active = np.arange(len(graphs))
     for d in range(max_depth):
-        if not active:
+        if active.size == 0:
             break
-        X = [features(stats[i], layers[i], d) for i in active]
+        h, v = last[active], visited[active]
+        X = np.column_stack([np.log1p(h), np.log1p(v), static[active], np.full(active.size, d / 64.0),
+                             v / orbit[active], np.log1p(gens[active] * h[:, 0])])
         y = net.predict(X)
-        still = []
-        for row, i in enumerate(active):
-            st = stats[i]
-            visited = sum(layers[i])
-            nxt = math.expm1(float(y[row, 0]) + math.log1p(layers[i][d]))
-            nxt = min(nxt, st.orbit - visited, st.gens * layers[i][d])
-            if nxt >= 0.5:
-                layers[i].append(nxt)
-                still.append(i)
-        active = still
+        nxt = np.expm1(y[:, 0].astype(np.float64) + np.log1p(h[:, 0]))
+        nxt = np.minimum(np.minimum(nxt, orbit[active] - v), gens[active] * h[:, 0])
+        keep = nxt >= 0.5
+        for i, size in zip(active[keep], nxt[keep]):
+            layers[i].append(float(size))
+        last[active[keep]] = np.column_stack([nxt[keep], h[keep, :3]])
+        visited[active[keep]] += nxt[keep]
+        active = active[keep]
     return layers
 
 
 def predicted_capacities(net: PlannerNet, graphs, margin=1.5, floor=4096):
-    """Per-instance frontier capacity for the batched sweep."""
+    """Per-instance frontier capacity for the batched sweep, never above the
+    exact state count |G| (the sweep's instances have distinct labels), which
+    no layer can exceed."""
     caps = []
     for g, prof in zip(graphs, rollout(net, graphs)):
-        orbit = math.factorial(len(g["start"]))
+        orbit = native.group_order(g["action"]["generators"])
         caps.append(int(min(orbit, max(prof) * margin + floor)))
     return caps
+
+
+def calibrate_margin(net: PlannerNet, graphs, tables, quantile=0.97, slack=1.1) -> float:
+    """Capacity margin from complete layer tables the network was not fitted
+    on: the `quantile` of (true peak / predicted peak), at least 1, times
+    `slack`.  A larger margin trades memory for fewer exact reruns."""
+    prof = rollout(net, graphs)
+    ratios = sorted(max(t) / max(1.0, max(p)) for t, p in zip(tables, prof))
+    q = ratios[min(len(ratios) - 1, int(quantile * (len(ratios) - 1) + 0.5))]
+    return max(1.0, q) * slack
 
 
 def choose_path(net: PlannerNet, graph: dict) -> dict:
@@ -257,8 +283,13 @@ def choose_path(net: PlannerNet, graph: dict) -> dict:
     layers when the predicted peak layer reaches the bucketing threshold."""
     prof = rollout(net, [graph])[0]
     st = graph_statics(graph["action"]["generators"], graph["start"])
+    start = graph["start"]
+    counts = {}
+    for v in start:
+        counts[v] = counts.get(v, 0) + 1
+    rank_domain = math.exp(math.lgamma(len(start) + 1) - sum(math.lgamma(c + 1) for c in counts.values()))
     total, peak = sum(prof), max(prof)
-    if total >= st.orbit / 128:
+    if total >= rank_domain / 128:
         return {"visited": "bitmap", "dedup": "bucket" if peak * st.gens >= (1 << 22) else "atomic",
                 "predicted_states": total, "predicted_peak": peak}
     return {"visited": "hash3" if st.inverse_closed else "hash", "dedup": "auto",
