@@ -364,10 +364,13 @@ def main():
     device_s = start.elapsed_time(stop) * 1e-3
     for r in results:
         assert r.complete and r.layer_sizes == expect, "layer table mismatch in a timed run"
-    t = torch.tensor([device_s], dtype=torch.float64, device="cuda")
+    device_max = device_s
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    device_max = float(t.item())
+        # Replicas: every rank must hold the same table; the job time is the slowest rank's.
+        from multigpubfs_b200 import replicas
+        view = replicas.exchange(results[0].layer_sizes, device_s, results[0].successors * args.steps,
+                                 device=torch.device("cuda", local))
+        device_max = view["device_seconds_max"]
     succ = results[0].successors
     states = results[0].states
     kernel_s = sum(r.kernel_seconds for r in results) / len(results)
