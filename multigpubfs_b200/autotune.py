@@ -1,0 +1,162 @@
+"""Pilot-run autotuner: picks the visited-set path of one graph by timing the
+candidate plans on the graph's own first layers, and caches the choice.
+
+Mirrors the reference's tuning layer in what it decides and how (re-designed
+for this engine's plans, not ported):
+
+* size profiles (multigpubfs/size_profiles.py:40-56): graphs below
+  ``PILOT_MIN_STATES`` states are not piloted; they take the fixed default plan;
+* timed trials with a keep-the-default rule (generic_distributed_native.rs:186-266,
+  multigpubfs/autotune.py:276): every candidate expands the same layer prefix,
+  is timed on the device, and replaces the default plan only if it is at
+  least ``MIN_GAIN`` (10 %) faster (autotune.py:263);
+* a profile cache (multigpubfs/profile_cache.py) keyed by graph digest, device
+  name and library build, so a graph is piloted once per machine.
+
+Candidates are the engine's exact paths for the graph (the plain bitmap with
+per-lane or warp-merged atomics, owner-routed bucket layers with one- or
+two-symbol shard prefixes, the open-addressing hash and, for inverse-closed
+graphs, the three-bank hash).  Results never depend on the choice: every path
+is exact and the plan only changes speed.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import time
+from pathlib import Path
+
+from .graph_definition import GraphDefinition
+
+PILOT_MIN_STATES = 1 << 24     # smaller graphs take the default plan
+PILOT_WORK = 1 << 27           # successors expanded by each pilot (a layer prefix)
+MIN_GAIN = 0.10                # a candidate must beat the default by this much
+DEFAULT = {"visited": "auto", "dedup": "auto"}
+
+
+def cache_path() -> Path:
+    env = os.environ.get("MGBFS2_AUTOTUNE_CACHE")
+    if env:
+        return Path(env)
+    return Path(os.environ.get("XDG_CACHE_HOME", Path.home() / ".cache")) / "multigpubfs_b200" / "autotune.json"
+
+
+def _state_bound(graph: GraphDefinition) -> int:
+    start = graph.start
+    counts = {}
+    for v in start:
+        counts[v] = counts.get(v, 0) + 1
+    return math.factorial(len(start)) // math.prod(math.factorial(c) for c in counts.values())
+
+
+def candidate_plans(graph: GraphDefinition) -> list[dict]:
+    """The plans the pilot compares, default first."""
+    out = [dict(DEFAULT)]
+    if graph.action["kind"] == "permutation":
+        n = len(graph.start)
+        distinct = len(set(graph.start)) == n
+        out += [{"visited": "bitmap", "dedup": "atomic"}, {"visited": "bitmap", "dedup": "warp"}]
+        if distinct and 2 <= n <= 16:
+            out.append({"visited": "bitmap", "dedup": "bucket", "shards": 1})       # one-symbol prefix
+            if n * (n - 1) <= 256:
+                out.append({"visited": "bitmap", "dedup": "bucket", "shards": 256})  # two-symbol prefix
+    out.append({"visited": "hash", "dedup": "atomic"})
+    if graph.inverse_closed():
+        out.append({"visited": "hash3", "dedup": "atomic"})
+    return out
+
+
+def cache_key(graph: GraphDefinition, device_name: str, build: str) -> str:
+    return f"{graph.digest()}|{device_name}|{build}"
+
+
+def load_cache(path: Path) -> dict:
+    try:
+        return json.loads(path.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def store_cache(path: Path, cache: dict) -> None:
+    path.parent.mkdir(parents=True, exist_ok=True)
+    tmp = path.with_suffix(".tmp")
+    tmp.write_text(json.dumps(cache, indent=1, sort_keys=True))
+    tmp.replace(path)
+
+
+def pick(trials: list[dict], min_gain: float = MIN_GAIN) -> dict:
+    """Keep-the-default rule over timed trials ({"plan", "seconds"}; the first
+    trial is the default; failed trials have seconds None)."""
+    default = trials[0]
+    ok = [t for t in trials if t["seconds"] is not None]
+    if not ok:
+        return default["plan"]
+    best = min(ok, key=lambda t: t["seconds"])
+    if default["seconds"] is None or best["seconds"] <= default["seconds"] * (1.0 - min_gain):
+        return best["plan"]
+    return default["plan"]
+
+
+def pilot_depth(layer_sizes: list[int], gens: int, work: int = PILOT_WORK) -> int:
+    """Layers a pilot expands: the shortest prefix whose successors reach
+    `work` (all layers if the search is smaller)."""
+    total = 0
+    for d, s in enumerate(layer_sizes):
+        total += s * gens
+        if total >= work:
+            return d + 1
+    return len(layer_sizes)
+
+
+def _run_pilot(graph, plan, device, max_layers, max_seconds):
+    from .engine import NativeGraph
+    from . import native
+    try:
+        with NativeGraph(graph, device) as eng:
+            eng.plan(**plan)
+            eng.run(max_layers=max_layers, max_seconds=max_seconds)   # warm: pool memory, module load
+            r = eng.run(max_layers=max_layers, max_seconds=max_seconds)
+            return r
+    except native.NativeError:
+        return None
+
+
+def choose_profile(graph: GraphDefinition, device: int = 0, *, budget_seconds: float = 60.0,
+                   cache: Path | None = None, use_cache: bool = True) -> dict:
+    """The plan for `graph` on `device`: from the cache, or by pilot runs.
+
+    Returns {"plan": {...}, "source": "size"|"cache"|"pilot", "trials": [...]}."""
+    if _state_bound(graph) < PILOT_MIN_STATES:
+        return {"plan": dict(DEFAULT), "source": "size", "trials": []}
+    import torch
+    from . import native
+    device_name = torch.cuda.get_device_name(device)
+    stamp = Path(native.LIBRARY).with_suffix(".stamp")
+    build = stamp.read_text().strip()[:16] if stamp.exists() else "unbuilt"
+    path = cache or cache_path()
+    key = cache_key(graph, device_name, build)
+    entries = load_cache(path) if use_cache else {}
+    if key in entries:
+        return {"plan": entries[key]["plan"], "source": "cache", "trials": entries[key].get("trials", [])}
+    started = time.perf_counter()
+    plans = candidate_plans(graph)
+    per_trial = max(1.0, budget_seconds / (2 * len(plans)))
+    # The default plan's pilot fixes the layer prefix every candidate expands.
+    first = _run_pilot(graph, plans[0], device, None, per_trial)
+    if first is None:
+        return {"plan": dict(DEFAULT), "source": "pilot", "trials": []}
+    depth = pilot_depth(first.layer_sizes, graph.generator_count)
+    trials = []
+    for plan in plans:
+        if time.perf_counter() - started > budget_seconds:
+            break
+        r = _run_pilot(graph, plan, device, depth, per_trial)
+        ok = r is not None and r.layer_sizes[:depth] == first.layer_sizes[:depth] and len(r.layer_sizes) >= depth
+        trials.append({"plan": plan, "seconds": r.device_seconds if ok else None})
+    choice = pick(trials)
+    if use_cache:
+        entries = load_cache(path)
+        entries[key] = {"plan": choice, "trials": trials, "pilot_layers": depth}
+        store_cache(path, entries)
+    return {"plan": choice, "source": "pilot", "trials": trials, "pilot_layers": depth}

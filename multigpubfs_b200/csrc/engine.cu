@@ -465,11 +465,18 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (visited == MGBFS2_VISITED_BITMAP && !rank_ok) return MGBFS2_UNSUPPORTED;
   if (visited == MGBFS2_VISITED_HASH3 && !inverse_closed) return MGBFS2_INVALID_ARGUMENT;
   uint32_t dedup = r.dedup;
-  if (dedup == MGBFS2_DEDUP_AUTO) dedup = visited == MGBFS2_VISITED_BITMAP ? MGBFS2_DEDUP_WARP : MGBFS2_DEDUP_ATOMIC;
+  if (dedup == MGBFS2_DEDUP_AUTO) {
+    // A bitmap that fits in L2 takes plain atomics; a larger Lehmer bitmap
+    // takes owner-routed layers, whose shard slices do fit.
+    dedup = MGBFS2_DEDUP_ATOMIC;
+    if (visited == MGBFS2_VISITED_BITMAP && lehmer && bitmap_bytes > (64ull << 20) && elements <= 16 &&
+        elements * (elements - 1) <= kMaxShards)
+      dedup = MGBFS2_DEDUP_BUCKET;
+  }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
-  if ((dedup == MGBFS2_DEDUP_SORT || dedup == MGBFS2_DEDUP_BUCKET) && !(visited == MGBFS2_VISITED_BITMAP && lehmer))
-    return MGBFS2_UNSUPPORTED;
-  if (dedup == MGBFS2_DEDUP_SORT) return MGBFS2_UNSUPPORTED;
+  if (dedup == MGBFS2_DEDUP_BUCKET && !(visited == MGBFS2_VISITED_BITMAP && lehmer)) return MGBFS2_UNSUPPORTED;
+  // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
+  if (dedup == MGBFS2_DEDUP_SORT && (!packed || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
   if (dedup == MGBFS2_DEDUP_BUCKET) {
     // Shards = states sharing their first K symbols: N!/(N-K)! shards whose
     // bitmap slices hold (N-K)! bits.  Default: the smallest K (1 or 2) whose
@@ -550,6 +557,28 @@ static ExpandFn pick_lehmer(uint32_t n) {
 #undef MG_CASE
     default:
       return nullptr;
+  }
+}
+
+static ExpandFn pick_sorted(int visit, uint32_t n) {
+  switch (visit) {
+    case V_LEHMER:
+      switch (n) {
+#define MG_CASE(K) \
+  case K:          \
+    return expand_sorted<V_LEHMER, K>;
+        MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
+        MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
+#undef MG_CASE
+        default:
+          return nullptr;
+      }
+    case V_MULTISET:
+      return expand_sorted<V_MULTISET, 0>;
+    case V_HASH:
+      return expand_sorted<V_HASH, 0>;
+    default:
+      return expand_sorted<V_HASH3, 0>;
   }
 }
 
@@ -711,7 +740,8 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   const auto started = Clock::now();
   const int visit = visit_kind();
   const bool warp = plan.dedup == MGBFS2_DEDUP_WARP;
-  ExpandFn fn = pick_expand(visit, warp, elements);
+  const bool sorted = plan.dedup == MGBFS2_DEDUP_SORT;
+  ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements);
   if (!fn) return MGBFS2_UNSUPPORTED;
   // Bucketed layers for large frontiers; small layers use the fused kernel.
   const bool bucketed = plan.dedup == MGBFS2_DEDUP_BUCKET && visit == V_LEHMER;
@@ -850,7 +880,8 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
                                 smem)))
           break;
       } else {
-        const uint64_t tiles = (count + kBlock * p.ppt - 1) / (kBlock * p.ppt);
+        const uint64_t per_tile = sorted ? kSortTile / gens : kBlock * p.ppt;
+        const uint64_t tiles = (count + per_tile - 1) / per_tile;
         const uint32_t grid = grid_for(reinterpret_cast<const void*>(fn), smem, tiles);
         fn<<<grid, kBlock, smem, stream>>>(p);
         ++launches;

@@ -8,6 +8,7 @@
 // every inverse is a positive power).  The learned planner uses it as its
 // orbit size; the reference only bounds the state space by the multinomial
 // n!/prod(c!) (crates/mgbfs-runtime/src/generic_memory.rs:82-108).
+#include <array>
 #include <cstdint>
 #include <vector>
 
@@ -16,29 +17,38 @@
 namespace mgbfs2 {
 namespace {
 
-using Perm = std::vector<uint8_t>;  // p[i] = image of point i
+constexpr uint32_t kMaxPoints = 20;
+// p[i] = image of point i for i < n; entries from n on stay fixed (p[i] = i),
+// so every helper can work on all kMaxPoints entries without knowing n.
+using Perm = std::array<uint8_t, kMaxPoints>;
+
+Perm identity() {
+  Perm r;
+  for (uint32_t i = 0; i < kMaxPoints; ++i) r[i] = static_cast<uint8_t>(i);
+  return r;
+}
 
 Perm compose(const Perm& a, const Perm& b) {  // (a b)(i) = a(b(i))
-  Perm r(b.size());
-  for (size_t i = 0; i < b.size(); ++i) r[i] = a[b[i]];
+  Perm r;
+  for (uint32_t i = 0; i < kMaxPoints; ++i) r[i] = a[b[i]];
   return r;
 }
 
 Perm inverse(const Perm& a) {
-  Perm r(a.size());
-  for (size_t i = 0; i < a.size(); ++i) r[a[i]] = static_cast<uint8_t>(i);
+  Perm r;
+  for (uint32_t i = 0; i < kMaxPoints; ++i) r[a[i]] = static_cast<uint8_t>(i);
   return r;
 }
 
 bool is_identity(const Perm& a) {
-  for (size_t i = 0; i < a.size(); ++i)
+  for (uint32_t i = 0; i < kMaxPoints; ++i)
     if (a[i] != i) return false;
   return true;
 }
 
 uint32_t moved_point(const Perm& a) {
-  for (size_t i = 0; i < a.size(); ++i)
-    if (a[i] != i) return static_cast<uint32_t>(i);
+  for (uint32_t i = 0; i < kMaxPoints; ++i)
+    if (a[i] != i) return i;
   return 0;
 }
 
@@ -71,12 +81,10 @@ struct StabChain {
   // Orbit of base[level] under the level's generators, with transversal.
   void build(size_t level) {
     const auto gens = level_gens(level);
-    u[level].assign(n, Perm());
+    u[level].assign(n, Perm{});
     present[level].assign(n, 0);
-    Perm id(n);
-    for (uint32_t i = 0; i < n; ++i) id[i] = static_cast<uint8_t>(i);
     const uint32_t beta = base[level];
-    u[level][beta] = id;
+    u[level][beta] = identity();
     present[level][beta] = 1;
     std::vector<uint32_t> queue{beta};
     for (size_t q = 0; q < queue.size(); ++q) {
@@ -114,7 +122,7 @@ extern "C" int mgbfs2_group_order(const uint32_t* permutations, uint32_t n, uint
   StabChain c;
   c.n = n;
   for (uint32_t g = 0; g < generators; ++g) {
-    Perm p(n);
+    Perm p = identity();
     std::vector<uint8_t> seen(n, 0);
     for (uint32_t i = 0; i < n; ++i) {
       const uint32_t v = permutations[static_cast<size_t>(g) * n + i];

@@ -9,6 +9,7 @@
 // 27-48, 105-205) for the bitmap, with one global atomicAdd per appended row.
 #pragma once
 #include "device.cuh"
+#include "sort_tiles.cuh"
 
 namespace mgbfs2 {
 
@@ -190,6 +191,74 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
       }
     }
     flush_block(p, out, &out_count, &out_base);
+  }
+}
+
+// Sort-unique layer expansion (dedup = sort).  A tile of parents writes all
+// its children (tagged) into shared memory, a block radix sort on the state
+// bits brings equal children together, unique keeps the first of each run,
+// and only the distinct children are tested against the visited set; the
+// winners are compacted in place and appended with one reservation per tile.
+// Restates, per tile and fused with generation and the claim, the
+// reference's batch strategy of sorting and uniquing candidates before the
+// visited test (cuda/permutation_bitmap_batch.cu:148,
+// cuda/segmented_hash_batch.cu:174).
+template <int V, int N>
+__global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
+  extern __shared__ __align__(16) unsigned char program_smem[];
+  __shared__ SortScratch s;
+  __shared__ uint8_t won_flag[kSortTile];
+  __shared__ unsigned long long out_base;
+  Term* terms = reinterpret_cast<Term*>(program_smem);
+  uint32_t* begin = reinterpret_cast<uint32_t*>(program_smem + p.total_terms * sizeof(Term));
+  const uint32_t* inverse = begin + p.gens + 1;
+  for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) begin[i] = p.term_begin[i];
+  __syncthreads();
+
+  const uint32_t per_tile = kSortTile / p.gens;  // parents per tile
+  const unsigned long long state_mask = p.gen_shift ? (1ull << p.gen_shift) - 1ull : p.key_mask;
+  const uint32_t key_bits = state_mask == ~0ull ? 64u : 64u - __clzll(static_cast<long long>(state_mask));
+  const unsigned long long tiles = (p.count + per_tile - 1) / per_tile;
+  for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const unsigned long long base = t * per_tile;
+    for (uint32_t i = threadIdx.x; i < kSortTile; i += kSortThreads) s.keys[i] = kEmpty;
+    __syncthreads();
+    // Generation: child of local parent j by generator g goes to slot g * per_tile + j.
+    for (uint32_t j = threadIdx.x; j < per_tile; j += kSortThreads) {
+      const unsigned long long idx = base + j;
+      if (idx >= p.count) break;
+      const uint64_t par = p.frontier[idx];
+      const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par >> p.gen_shift) : 0u;
+      const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
+      for (uint32_t g = 0; g < p.gens; ++g) {
+        if (g == skip) continue;
+        const uint64_t c = apply_terms(par, terms, begin[g], begin[g + 1]);
+        s.keys[g * per_tile + j] = c | (p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull);
+      }
+    }
+    __syncthreads();
+    block_radix_sort(s, key_bits);
+    const uint32_t distinct = block_unique(s, state_mask);
+    // Visited claim of the distinct children (coalesced shared-memory reads).
+    for (uint32_t i = threadIdx.x; i < kSortTile; i += kSortThreads) {
+      const bool valid = i < distinct;
+      const unsigned long long key = valid ? s.keys[i] : 0ull;
+      won_flag[i] = claim<V, N, false>(p, key & state_mask, valid) ? 1 : 0;
+    }
+    __syncthreads();
+    const uint32_t winners = block_compact(s, [&](uint32_t i, unsigned long long) { return won_flag[i] != 0; });
+    if (threadIdx.x == 0 && winners)
+      out_base = atomicAdd(&p.control->next_count, static_cast<unsigned long long>(winners));
+    __syncthreads();
+    bool overflow = false;
+    for (uint32_t i = threadIdx.x; i < winners; i += kSortThreads) {
+      const unsigned long long pos = out_base + i;
+      if (pos < p.capacity) p.next[pos] = s.keys[i];
+      else overflow = true;
+    }
+    if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
+    __syncthreads();
   }
 }
 

@@ -105,9 +105,11 @@ __device__ __forceinline__ void block_radix_sort(SortScratch& s, uint32_t key_bi
   }
 }
 
-// After block_radix_sort: compacts the distinct non-padding keys to the front
-// of s.keys and returns their number (identical in every thread).
-__device__ __forceinline__ uint32_t block_unique(SortScratch& s) {
+// Stable in-place compaction of s.keys: keeps the keys i with keep(i, key)
+// at the front and returns their number (identical in every thread).  The
+// predicate may read s.keys: every read happens before the first write.
+template <typename Keep>
+__device__ __forceinline__ uint32_t block_compact(SortScratch& s, Keep keep) {
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = lane_id();
   unsigned long long mine[kSortPerThread];
   uint32_t flags = 0, count = 0;
@@ -115,8 +117,7 @@ __device__ __forceinline__ uint32_t block_unique(SortScratch& s) {
   for (uint32_t k = 0; k < kSortPerThread; ++k) {
     const uint32_t i = tid * kSortPerThread + k;
     mine[k] = s.keys[i];
-    const bool first = mine[k] != kEmpty && (i == 0 || s.keys[i - 1] != mine[k]);
-    if (first) {
+    if (keep(i, mine[k])) {
       flags |= 1u << k;
       ++count;
     }
@@ -141,7 +142,17 @@ __device__ __forceinline__ uint32_t block_unique(SortScratch& s) {
   return s.unique_count;
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_unique_tiles_kernel(const unsigned long long* keys,
+// After block_radix_sort: compacts the distinct non-padding keys to the front
+// of s.keys and returns their number.  Keys are compared on `mask` (bits
+// outside it, such as a parent-edge tag, ride along with the first key of
+// each run).
+__device__ __forceinline__ uint32_t block_unique(SortScratch& s, unsigned long long mask = ~0ull) {
+  return block_compact(s, [&](uint32_t i, unsigned long long key) {
+    return key != kEmpty && (i == 0 || (s.keys[i - 1] & mask) != (key & mask));
+  });
+}
+
+static __global__ void __launch_bounds__(kSortThreads) sort_unique_tiles_kernel(const unsigned long long* keys,
                                                                          unsigned long long count, uint32_t key_bits,
                                                                          unsigned long long* out, uint32_t* counts) {
   __shared__ SortScratch s;

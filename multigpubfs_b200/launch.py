@@ -132,6 +132,20 @@ def run_graph(graph, output, *, device=None, devices=None, capacity=None, max_se
     dev = devices[0] if devices else 0
     digest = graph.digest()
     setup_started = time.perf_counter()
+    tuned = {"enabled": autotune, "source": None}
+    if autotune and visited == "auto" and dedup == "auto" and shards is None:
+        # Only a plan the caller left open is tuned, within min(60, max_seconds // 3)
+        # seconds that come off the run's deadline (multigpubfs/launch.py:277-290).
+        from . import autotune as tuner
+        budget = 60 if max_seconds is None else min(60, max(1, max_seconds // 3))
+        t0 = time.perf_counter()
+        prof = tuner.choose_profile(graph, dev, budget_seconds=budget)
+        if max_seconds is not None:
+            max_seconds = max(1, int(max_seconds - (time.perf_counter() - t0)))
+        tuned = {"enabled": True, "source": prof["source"], "plan": prof["plan"]}
+        visited = prof["plan"].get("visited", visited)
+        dedup = prof["plan"].get("dedup", dedup)
+        shards = prof["plan"].get("shards", shards)
     with NativeGraph(graph, dev) as engine:
         plan = engine.plan(visited=visited, dedup=dedup, capacity=capacity, shards=shards, planner=planner)
         setup_seconds = time.perf_counter() - setup_started
@@ -158,7 +172,7 @@ def run_graph(graph, output, *, device=None, devices=None, capacity=None, max_se
         "successors": result.successors, "successors_per_second": result.successors / bfs,
         "states_per_second": result.states / bfs, "kernel_launches": result.kernel_launches,
         "redo_layers": result.redo_layers, "fatal_bits": result.fatal_names,
-        "memory_backend": memory_backend, "segment_strategy": segment_strategy, "autotune": autotune,
+        "memory_backend": memory_backend, "segment_strategy": segment_strategy, "autotune": tuned,
     }
     output.mkdir(parents=True)
     (output / "states.json").write_bytes(state_bytes)

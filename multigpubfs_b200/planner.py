@@ -21,6 +21,7 @@ buffers from worst-case bounds and timed pilot runs
 """
 from __future__ import annotations
 
+import functools
 import json
 import math
 from dataclasses import dataclass
@@ -65,6 +66,16 @@ class GraphStatics:
         return math.exp(self.log_orbit)
 
 
+@functools.lru_cache(maxsize=4096)
+def _group_order(generators: tuple) -> int:
+    return native.group_order(generators)
+
+
+def group_order(generators) -> int:
+    """|<generators>| (host Schreier-Sims), memoised per generator set."""
+    return _group_order(tuple(tuple(int(x) for x in g) for g in generators))
+
+
 def graph_statics(generators, start) -> GraphStatics:
     n = len(start)
     orders, fixed, cycles = [], [], []
@@ -83,7 +94,7 @@ def graph_statics(generators, start) -> GraphStatics:
         counts[v] = counts.get(v, 0) + 1
     if len(counts) == n and n <= 20:
         # Distinct labels: the BFS settles exactly |<generators>| states.
-        log_orbit = math.log(native.group_order(generators))
+        log_orbit = math.log(group_order(generators))
     else:
         log_orbit = math.lgamma(n + 1) - sum(math.lgamma(c + 1) for c in counts.values())
     return GraphStatics(n, len(generators), closed, log_orbit, float(np.mean(orders)), float(max(orders)),
@@ -261,7 +272,7 @@ def predicted_capacities(net: PlannerNet, graphs, margin=1.5, floor=4096):
     no layer can exceed."""
     caps = []
     for g, prof in zip(graphs, rollout(net, graphs)):
-        orbit = native.group_order(g["action"]["generators"])
+        orbit = group_order(g["action"]["generators"])
         caps.append(int(min(orbit, max(prof) * margin + floor)))
     return caps
 

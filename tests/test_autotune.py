@@ -1,0 +1,56 @@
+"""Autotuner host logic on CPU: candidates, the keep-the-default rule, the
+pilot prefix, the cache and the size profile.  The pilots themselves run in
+tests/test_gpu_autotune.py."""
+import pytest
+
+from multigpubfs_b200 import GraphDefinition, autotune
+from oracle import graph_oracle as G
+
+
+def _lrx(n):
+    return GraphDefinition.permutation(G.lrx_generators(n), list(range(n)))
+
+
+def test_candidates_for_lrx_and_matrix_graphs():
+    plans = autotune.candidate_plans(_lrx(11))
+    assert plans[0] == autotune.DEFAULT
+    assert {"visited": "bitmap", "dedup": "bucket", "shards": 256} in plans
+    assert {"visited": "hash3", "dedup": "atomic"} in plans  # L, R inverse pair and X an involution
+    mat = GraphDefinition.from_dict(G.matrix_graph(2, 2, [([1, 1, 0, 1], 7), ([1, 0, 1, 1], 7)], [1, 0, 0, 1]))
+    kinds = {(p["visited"], p["dedup"]) for p in autotune.candidate_plans(mat)}
+    assert ("bitmap", "atomic") not in kinds and ("hash", "atomic") in kinds
+
+
+def test_keep_the_default_unless_ten_percent_faster():
+    d = {"visited": "auto", "dedup": "auto"}
+    a = {"visited": "bitmap", "dedup": "atomic"}
+    assert autotune.pick([{"plan": d, "seconds": 1.0}, {"plan": a, "seconds": 0.95}]) == d
+    assert autotune.pick([{"plan": d, "seconds": 1.0}, {"plan": a, "seconds": 0.89}]) == a
+    assert autotune.pick([{"plan": d, "seconds": None}, {"plan": a, "seconds": 3.0}]) == a
+    assert autotune.pick([{"plan": d, "seconds": None}, {"plan": a, "seconds": None}]) == d
+
+
+def test_pilot_depth_is_the_shortest_prefix_reaching_the_work():
+    sizes = [1, 3, 9, 27, 81]
+    assert autotune.pilot_depth(sizes, 3, work=3 * 13) == 3
+    assert autotune.pilot_depth(sizes, 3, work=1 << 40) == len(sizes)
+
+
+def test_cache_roundtrip(tmp_path):
+    path = tmp_path / "sub" / "cache.json"
+    assert autotune.load_cache(path) == {}
+    autotune.store_cache(path, {"k": {"plan": {"visited": "hash"}}})
+    assert autotune.load_cache(path)["k"]["plan"] == {"visited": "hash"}
+    key = autotune.cache_key(_lrx(9), "B200", "abc")
+    assert key.startswith(_lrx(9).digest()) and key.endswith("|B200|abc")
+
+
+def test_small_graphs_take_the_size_profile_without_pilots(tmp_path):
+    got = autotune.choose_profile(_lrx(9), 0, cache=tmp_path / "c.json")
+    assert got == {"plan": autotune.DEFAULT, "source": "size", "trials": []}
+    assert not (tmp_path / "c.json").exists()
+
+
+def test_cache_path_override(monkeypatch, tmp_path):
+    monkeypatch.setenv("MGBFS2_AUTOTUNE_CACHE", str(tmp_path / "x.json"))
+    assert autotune.cache_path() == tmp_path / "x.json"

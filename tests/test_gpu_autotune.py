@@ -1,0 +1,45 @@
+"""Autotuner pilots on the device: every candidate expands the same layer
+prefix exactly, the choice is cached, and run_graph with autotune on stays
+exact."""
+import json
+
+import pytest
+
+from oracle import graph_oracle as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _lrx(n):
+    from multigpubfs_b200 import GraphDefinition
+    return GraphDefinition.permutation(G.lrx_generators(n), list(range(n)))
+
+
+def test_pilots_compare_every_candidate_then_cache(tmp_path, lrx_layers):
+    from multigpubfs_b200 import autotune
+    from multigpubfs_b200.engine import NativeGraph
+    g = _lrx(11)
+    cache = tmp_path / "tune.json"
+    got = autotune.choose_profile(g, 0, cache=cache)
+    assert got["source"] == "pilot"
+    assert [t["plan"] for t in got["trials"]] == autotune.candidate_plans(g)
+    assert all(t["seconds"] is not None and t["seconds"] > 0 for t in got["trials"]), got["trials"]
+    assert got["plan"] in autotune.candidate_plans(g)
+    again = autotune.choose_profile(g, 0, cache=cache)
+    assert again["source"] == "cache" and again["plan"] == got["plan"]
+    assert len(json.loads(cache.read_text())) == 1
+    with NativeGraph(g) as e:
+        e.plan(**got["plan"])
+        assert e.run().layer_sizes == lrx_layers[11]
+
+
+def test_run_graph_with_autotune_is_exact(tmp_path, monkeypatch, lrx_layers):
+    from multigpubfs_b200.launch import run_graph
+    monkeypatch.setenv("MGBFS2_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    report = run_graph(_lrx(11), tmp_path / "out", autotune=True)
+    assert report["status"] == "COMPLETE" and report["layer_sizes"] == lrx_layers[11]
+    assert report["autotune"]["source"] == "pilot"
+    report2 = run_graph(_lrx(11), tmp_path / "out2", autotune=True)
+    assert report2["autotune"]["source"] == "cache" and report2["layer_sizes"] == lrx_layers[11]
+    small = run_graph(_lrx(8), tmp_path / "out3", autotune=True)
+    assert small["autotune"]["source"] == "size" and small["layer_sizes"] == lrx_layers[8]

@@ -49,6 +49,11 @@ VARIANTS = {
     # every generator applied, no parent-edge skip
     "bitmap_bucket_noskip": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, parent_skip=False),
     "hash3_noskip": dict(visited="hash3", parent_skip=False),
+    # sort-unique tiles of children before the visited test
+    "bitmap_sort": dict(visited="bitmap", dedup="sort"),
+    "bitmap_sort_noskip": dict(visited="bitmap", dedup="sort", parent_skip=False),
+    "hash_sort": dict(visited="hash", dedup="sort"),
+    "hash3_sort": dict(visited="hash3", dedup="sort"),
 }
 
 
@@ -104,7 +109,8 @@ def test_parent_skip_accounting(lrx_layers):
 
 
 @pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3", "bitmap_bucket",
-                                     "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip"])
+                                     "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip", "bitmap_sort",
+                                     "bitmap_sort_noskip", "hash_sort", "hash3_sort"])
 def test_lrx_small(lrx_layers, variant):
     redo = 0
     for n in range(3, 12):
@@ -155,7 +161,8 @@ def test_random_sweep_instances(closed):
         g = G.sweep_instance(i, closed)
         n = len(g["start"])
         ref, last_ref, _ = P.packed_bfs(g["action"]["generators"], g["start"], sample=1 << 22)
-        for variant in ("auto", "hash", "bitmap_warp") + (("hash3",) if closed else ()):
+        for variant in ("auto", "hash", "bitmap_warp", "bitmap_sort", "hash_sort") + \
+                (("hash3", "hash3_sort") if closed else ()):
             out = run(g, **VARIANTS[variant])
             assert out[1].layer_sizes == ref, (i, variant, n)
             if ref[-1] <= 1000:
