@@ -60,7 +60,7 @@ def coxeter(n):
 
 
 WORKLOADS = {
-    "s13-lrx": dict(n=13, gens=lrx(13), visited="bitmap", dedup="bucket",
+    "s13-lrx": dict(n=13, gens=lrx(13), visited="bitmap", dedup="grouped",
                     desc="S13 LRX full BFS (L, R, X from identity; 6,227,020,800 states), exact Lehmer-rank bitmap"),
     "s13-coxeter": dict(n=13, gens=coxeter(13), visited="bitmap", dedup="bucket",
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),

@@ -58,8 +58,12 @@ typedef struct {
 } mgbfs2_graph_desc;
 
 enum { MGBFS2_VISITED_AUTO = 0, MGBFS2_VISITED_BITMAP = 1, MGBFS2_VISITED_HASH = 2, MGBFS2_VISITED_HASH3 = 3 };
+/* SORT: per-tile radix sort + unique of the children before the visited test.
+ * BUCKET: route successors to rank-range shard buckets, then claim per shard.
+ * GROUPED: claim first, route only the winners into a frontier grouped by its
+ * first N-10 symbols (Lehmer bitmaps of degree 11..13). */
 enum { MGBFS2_DEDUP_AUTO = 0, MGBFS2_DEDUP_ATOMIC = 1, MGBFS2_DEDUP_WARP = 2, MGBFS2_DEDUP_SORT = 3,
-       MGBFS2_DEDUP_BUCKET = 4 };
+       MGBFS2_DEDUP_BUCKET = 4, MGBFS2_DEDUP_GROUPED = 5 };
 enum { MGBFS2_PLANNER_PLAIN = 0, MGBFS2_PLANNER_LEARNED = 1 };
 
 typedef struct {
@@ -71,7 +75,7 @@ typedef struct {
   uint32_t block;          /* threads per block, 0 = tuned */
   uint32_t planner;        /* MGBFS2_PLANNER_* */
   uint32_t bucket_margin;  /* extra entries per shard bucket, 0 = 4096; UINT32_MAX = none */
-  uint64_t bucket_min_work; /* successors per layer from which layers are bucketed, 0 = 2^22 */
+  uint64_t bucket_min_work; /* successors per layer from which layers are bucketed or grouped, 0 = 2^22 */
   uint32_t options;        /* MGBFS2_OPTION_* bits */
   uint32_t reserved;
 } mgbfs2_plan_request;

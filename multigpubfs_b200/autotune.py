@@ -13,11 +13,12 @@ for this engine's plans, not ported):
 * a profile cache (multigpubfs/profile_cache.py) keyed by graph digest, device
   name and library build, so a graph is piloted once per machine.
 
-Candidates are the engine's exact paths for the graph (the plain bitmap with
+Candidates are the engine's exact paths for the graph: the plain bitmap with
 per-lane or warp-merged atomics, owner-routed bucket layers with one- or
-two-symbol shard prefixes, the open-addressing hash and, for inverse-closed
-graphs, the three-bank hash).  Results never depend on the choice: every path
-is exact and the plan only changes speed.
+two-symbol shard prefixes, grouped claim-then-route layers, the
+open-addressing hash and, for inverse-closed graphs, the three-bank hash.
+Results never depend on the choice: every path is exact and the plan only
+changes speed.
 """
 from __future__ import annotations
 
@@ -61,6 +62,7 @@ def candidate_plans(graph: GraphDefinition) -> list[dict]:
             out.append({"visited": "bitmap", "dedup": "bucket", "shards": 1})       # one-symbol prefix
             if n * (n - 1) <= 256:
                 out.append({"visited": "bitmap", "dedup": "bucket", "shards": 256})  # two-symbol prefix
+            out.append({"visited": "bitmap", "dedup": "grouped"})
     out.append({"visited": "hash", "dedup": "atomic"})
     if graph.inverse_closed():
         out.append({"visited": "hash3", "dedup": "atomic"})

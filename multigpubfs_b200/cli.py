@@ -47,7 +47,7 @@ def main(argv=None) -> int:
     ap.add_argument("graph")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--visited", default="auto", choices=["auto", "bitmap", "hash", "hash3"])
-    ap.add_argument("--dedup", default="auto", choices=["auto", "atomic", "warp", "sort", "bucket"])
+    ap.add_argument("--dedup", default="auto", choices=["auto", "atomic", "warp", "sort", "bucket", "grouped"])
     ap.add_argument("--planner", default="plain", choices=["plain", "learned"])
     ap.add_argument("--capacity", type=int, default=None)
     ap.add_argument("--shards", type=int, default=None)

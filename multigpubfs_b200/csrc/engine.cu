@@ -20,6 +20,7 @@
 #include "../../include/mgbfs2.h"
 #include "bucket_kernels.cuh"
 #include "engine.h"
+#include "grouped_kernels.cuh"
 #include "packed_kernels.cuh"
 
 namespace mgbfs2 {
@@ -122,7 +123,7 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
   rc = cuda_status(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   if (rc) { set_message(error, cap, "CUDA_STREAM"); delete g; return rc; }
   for (DeviceBuffer* b : {&g->bitmap, &g->front, &g->next, &g->table, &g->bank[0], &g->bank[1], &g->bank[2],
-                          &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta})
+                          &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta, &g->group_meta})
     b->stream = g->stream;
   retain_pool_memory(dev);
   for (cudaEvent_t* e : {&g->ev_run[0], &g->ev_run[1], &g->ev_kernel[0], &g->ev_kernel[1]}) {
@@ -377,6 +378,12 @@ void Graph::release() {
     cudaFreeHost(host_meta);
     host_meta = nullptr;
   }
+  group_meta.free();
+  if (host_group) {
+    cudaFreeHost(host_group);
+    host_group = nullptr;
+  }
+  front_grouped = false;
 }
 
 // Stream-ordered allocations from the device's default memory pool, which
@@ -429,7 +436,7 @@ uint64_t pool_idle_bytes(int device) {
 int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   mgbfs2_plan_request r{};
   if (req) r = *req;
-  if (r.visited > MGBFS2_VISITED_HASH3 || r.dedup > MGBFS2_DEDUP_BUCKET || r.planner > MGBFS2_PLANNER_LEARNED)
+  if (r.visited > MGBFS2_VISITED_HASH3 || r.dedup > MGBFS2_DEDUP_GROUPED || r.planner > MGBFS2_PLANNER_LEARNED)
     return MGBFS2_INVALID_ARGUMENT;
   MG_CHECK(cudaSetDevice(device));
   size_t free_bytes = 0, total_bytes = 0;
@@ -466,15 +473,28 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (visited == MGBFS2_VISITED_HASH3 && !inverse_closed) return MGBFS2_INVALID_ARGUMENT;
   uint32_t dedup = r.dedup;
   if (dedup == MGBFS2_DEDUP_AUTO) {
-    // A bitmap that fits in L2 takes plain atomics; a larger Lehmer bitmap
-    // takes owner-routed layers, whose shard slices do fit.
+    // A bitmap that fits in L2 takes plain atomics.  A larger Lehmer bitmap
+    // takes grouped layers when every generator fills the child's first K
+    // positions from the parent's first K with at most one exception (then a
+    // parent group's children fall into at most N-K target groups per
+    // generator), else owner-routed layers, whose shard slices fit in L2
+    // whatever the generators.
     dedup = MGBFS2_DEDUP_ATOMIC;
-    if (visited == MGBFS2_VISITED_BITMAP && lehmer && bitmap_bytes > (64ull << 20) && elements <= 16 &&
-        elements * (elements - 1) <= kMaxShards)
-      dedup = MGBFS2_DEDUP_BUCKET;
+    if (visited == MGBFS2_VISITED_BITMAP && lehmer && bitmap_bytes > (64ull << 20) && elements <= 16) {
+      const uint32_t n = elements, K = n > 10 ? std::min<uint32_t>(3, n - 10) : 1;
+      bool local = n <= 13;
+      for (uint32_t k = 0; k < gens && local; ++k) {
+        uint32_t outside = 0;
+        for (uint32_t i = 0; i < K; ++i) outside += perms[static_cast<size_t>(k) * n + i] >= K ? 1 : 0;
+        local = outside <= 1;
+      }
+      if (local) dedup = MGBFS2_DEDUP_GROUPED;
+      else if (n * (n - 1) <= kMaxShards) dedup = MGBFS2_DEDUP_BUCKET;
+    }
   }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
-  if (dedup == MGBFS2_DEDUP_BUCKET && !(visited == MGBFS2_VISITED_BITMAP && lehmer)) return MGBFS2_UNSUPPORTED;
+  if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) && !(visited == MGBFS2_VISITED_BITMAP && lehmer))
+    return MGBFS2_UNSUPPORTED;
   // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
   if (dedup == MGBFS2_DEDUP_SORT && (!packed || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
   if (dedup == MGBFS2_DEDUP_BUCKET) {
@@ -493,6 +513,24 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     bucket_shards = static_cast<uint32_t>(fact[n] / fact[n - K]);
     p.shards = bucket_shards;
     bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
+    bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
+  }
+  if (dedup == MGBFS2_DEDUP_GROUPED) {
+    // Groups = states sharing their first K symbols; K = N - 10 (10!-bit,
+    // 454 KB groups) within 1..3 and at most kMaxGroups groups.
+    const uint32_t n = elements;
+    if (n < 2 || n > 16) return MGBFS2_UNSUPPORTED;
+    uint64_t fact[17] = {1};
+    for (uint32_t i = 1; i <= 16; ++i) fact[i] = fact[i - 1] * i;
+    uint32_t K = n > 10 ? std::min<uint32_t>(3, n - 10) : 1;
+    while (K > 1 && fact[n] / fact[n - K] > kMaxGroups) --K;
+    if (fact[n] / fact[n - K] > kMaxGroups) return MGBFS2_UNSUPPORTED;
+    group_prefix = K;
+    groups = static_cast<uint32_t>(fact[n] / fact[n - K]);
+    plan_group_order();
+    bucket_prefix = K;
+    p.shards = groups;
+    bucket_margin = r.bucket_margin == 0 ? 1024 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
     bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
   }
   p.visited = visited;
@@ -612,6 +650,200 @@ static void pick_bucket(uint32_t n, uint32_t prefix, RouteFn* route, AcceptFn* a
       *route = nullptr;
       *accept = nullptr;
   }
+}
+
+using GroupedFn = void (*)(GroupedParams);
+
+static GroupedFn pick_grouped(uint32_t n, uint32_t prefix) {
+  switch (n) {
+#define MG_CASE(K)                                                                               \
+  case K:                                                                                        \
+    return prefix == 1 ? expand_grouped<K, 1> : (prefix == 2 ? expand_grouped<K, 2> : expand_grouped<K, 3>);
+    MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10) MG_CASE(11) MG_CASE(12)
+    MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
+#undef MG_CASE
+    case 2:
+    case 3:
+      return prefix == 1 ? (n == 2 ? expand_grouped<2, 1> : expand_grouped<3, 1>) : nullptr;
+    default:
+      return nullptr;
+  }
+}
+
+// Visiting order of the groups.  A generator whose child keeps all of its
+// first K symbols among the parent's first K sends a parent group to one
+// target group; otherwise its target groups are fixed by the parent
+// positions it does take from the first K (LRX: L takes positions 1, 2 and R
+// positions 0, 1).  Groups are enumerated lexicographically over their
+// symbols with the positions most of those generators share outermost, so
+// consecutive work items reuse the same target groups while they are in L2.
+void Graph::plan_group_order() {
+  const uint32_t n = elements, K = group_prefix;
+  std::vector<uint32_t> weight(K, 0);
+  for (uint32_t k = 0; k < gens; ++k) {
+    const uint32_t* g = perms.data() + static_cast<size_t>(k) * n;
+    bool inside = true;
+    for (uint32_t i = 0; i < K; ++i) inside = inside && g[i] < K;
+    if (inside) continue;
+    for (uint32_t i = 0; i < K; ++i)
+      if (g[i] < K) ++weight[g[i]];
+  }
+  std::vector<uint32_t> pos(K);
+  for (uint32_t i = 0; i < K; ++i) pos[i] = i;
+  std::stable_sort(pos.begin(), pos.end(), [&](uint32_t a, uint32_t b) { return weight[a] > weight[b]; });
+  group_order.clear();
+  std::vector<uint32_t> sym(K, 0);
+  std::vector<uint8_t> used(n, 0);
+  // Depth-first over positions pos[0], pos[1], ...; at full depth the group is
+  // the mixed-radix number of the Lehmer digits of (sym[0], ..., sym[K-1]).
+  std::vector<uint32_t> next_symbol(K, 0);
+  uint32_t depth = 0;
+  while (true) {
+    if (depth == K) {
+      uint64_t index = 0;
+      for (uint32_t i = 0; i < K; ++i) {
+        uint32_t digit = sym[i];
+        for (uint32_t j = 0; j < i; ++j) digit -= sym[j] < sym[i] ? 1 : 0;
+        index = index * (n - i) + digit;
+      }
+      group_order.push_back(static_cast<uint32_t>(index));
+      --depth;
+      used[sym[pos[depth]]] = 0;
+      continue;
+    }
+    uint32_t& c = next_symbol[depth];
+    while (c < n && used[c]) ++c;
+    if (c == n) {
+      c = 0;
+      if (depth == 0) break;
+      --depth;
+      used[sym[pos[depth]]] = 0;
+      continue;
+    }
+    sym[pos[depth]] = c;
+    used[c] = 1;
+    ++c;
+    ++depth;
+  }
+}
+
+// Meta layout of a grouped layer (R = groups + 1 regions, the spill last), in
+// uint64 words: region_begin[R] | region_count[R] | item_prefix[R + 1] |
+// next_begin[R] | next_cap[R] | next_count[R] | work, then region_order[R] as
+// uint32.
+static size_t group_meta_words(uint32_t groups) { return 6 * static_cast<size_t>(groups + 1) + 2; }
+static size_t group_meta_bytes(uint32_t groups) {
+  return group_meta_words(groups) * sizeof(unsigned long long) + (groups + 1) * sizeof(uint32_t);
+}
+
+// Lays out the next frontier of a grouped layer and uploads the layer's meta.
+// Group regions get the current layer's distribution of `count` scaled by the
+// last growth ratio, plus 25 % and bucket_margin; the spill region gets the exact
+// bound `cap`, so every winner has a place.
+int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total,
+                         size_t smem, uint64_t* items) {
+  const uint32_t G = groups, R = groups + 1;
+  int rc = MGBFS2_OK;
+  const size_t words = group_meta_words(G), bytes = group_meta_bytes(G);
+  if (!host_group && (rc = cuda_status(cudaMallocHost(&host_group, bytes)))) return rc;
+  if ((rc = group_meta.ensure(bytes))) return rc;
+  uint32_t* order = reinterpret_cast<uint32_t*>(host_group + words);
+  unsigned long long* rb = host_group;
+  unsigned long long* rcnt = rb + R;
+  unsigned long long* ip = rcnt + R;
+  unsigned long long* nb = ip + R + 1;
+  unsigned long long* nc = nb + R;
+  unsigned long long* ncount = nc + R;
+  if (front_grouped) {
+    for (uint32_t r = 0; r < R; ++r) {
+      rb[r] = front_begin[r];
+      rcnt[r] = front_count[r];
+    }
+  } else {
+    for (uint32_t r = 0; r < R; ++r) rb[r] = rcnt[r] = 0;
+    rcnt[G] = count;  // a contiguous frontier is all spill
+  }
+  for (uint32_t j = 0; j < G; ++j) order[j] = group_order[j];
+  order[G] = G;  // the spill last
+  uint64_t run = 0;
+  for (uint32_t j = 0; j < R; ++j) {
+    ip[j] = run;
+    run += (rcnt[order[j]] + kGroupChunk - 1) / kGroupChunk;
+  }
+  ip[R] = run;
+  *items = run;
+  const double growth = prev_count ? static_cast<double>(count) / static_cast<double>(prev_count) : gens;
+  const double predicted = std::min(static_cast<double>(cap), growth * static_cast<double>(count));
+  next_begin.assign(R, 0);
+  next_cap.assign(R, 0);
+  uint64_t total = 0;
+  for (uint32_t g = 0; g < G; ++g) {
+    const double frac = front_grouped && count ? static_cast<double>(rcnt[g]) / static_cast<double>(count)
+                                              : 1.0 / static_cast<double>(G);
+    const uint64_t c = static_cast<uint64_t>(frac * predicted * 1.25) + bucket_margin;
+    nb[g] = next_begin[g] = total;
+    nc[g] = next_cap[g] = c;
+    total += c;
+  }
+  nb[G] = next_begin[G] = total;
+  nc[G] = next_cap[G] = cap;
+  total += cap;
+  for (uint32_t r = 0; r < R; ++r) ncount[r] = 0;
+  ncount[R] = 0;  // work counter
+  if ((rc = next.ensure((total + 2) * sizeof(unsigned long long)))) return rc;
+  MG_CHECK(cudaMemcpyAsync(group_meta.ptr, host_group, bytes, cudaMemcpyHostToDevice, stream));
+  GroupedFn f = pick_grouped(elements, group_prefix);
+  if (!f) return MGBFS2_UNSUPPORTED;
+  *fn = reinterpret_cast<void*>(f);
+  *smem_total = sizeof(GroupedSmem) + smem;
+  MG_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(*smem_total)));
+  return MGBFS2_OK;
+}
+
+// After a grouped layer: the per-region counts (read back into host_group)
+// become the layout of the buffer that is about to be the frontier.
+int Graph::grouped_finish() {
+  const uint32_t G = groups, R = groups + 1;
+  const unsigned long long* ncount = host_group + 5 * static_cast<size_t>(R) + 1;
+  front_begin = next_begin;
+  front_count.assign(R, 0);
+  for (uint32_t r = 0; r < R; ++r) front_count[r] = std::min<uint64_t>(ncount[r], next_cap[r]);
+  (void)G;
+  return MGBFS2_OK;
+}
+
+// Copies the grouped `front` into `next` as one contiguous array and swaps.
+int Graph::gather_front(uint64_t count) {
+  if (!front_grouped) return MGBFS2_OK;
+  const uint32_t R = groups + 1;
+  int rc = MGBFS2_OK;
+  if ((rc = group_meta.ensure(group_meta_bytes(groups)))) return rc;
+  unsigned long long* rb = host_group;
+  unsigned long long* rcnt = rb + R;
+  unsigned long long* op = rcnt + R;
+  uint64_t run = 0;
+  for (uint32_t r = 0; r < R; ++r) {
+    rb[r] = front_begin[r];
+    rcnt[r] = front_count[r];
+    op[r] = run;
+    run += front_count[r];
+  }
+  if (run != count) return MGBFS2_STATE;
+  if ((rc = next.ensure((count + 2) * sizeof(unsigned long long)))) return rc;
+  MG_CHECK(cudaMemcpyAsync(group_meta.ptr, host_group, 3 * R * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                           stream));
+  const unsigned long long* meta = static_cast<const unsigned long long*>(group_meta.ptr);
+  gather_regions<<<std::min<uint32_t>(R, 4 * sm_count), kBlock, 0, stream>>>(
+      static_cast<const unsigned long long*>(front.ptr), meta, meta + R, meta + 2 * R, R,
+      static_cast<unsigned long long*>(next.ptr));
+  ++launches;
+  MG_CHECK(cudaGetLastError());
+  // The copy reads host_group at execution time: finish before it is reused.
+  MG_CHECK(cudaStreamSynchronize(stream));
+  std::swap(front, next);
+  front_grouped = false;
+  return MGBFS2_OK;
 }
 
 // Per-shard bucket capacities for `work` routed successors: the previous
@@ -753,6 +985,9 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   }
   shard_history.assign(bucket_shards, 0);
   shard_history_total = 0;
+  const bool grouped_mode = plan.dedup == MGBFS2_DEDUP_GROUPED && visit == V_LEHMER;
+  if (grouped_mode && !pick_grouped(elements, group_prefix)) return MGBFS2_UNSUPPORTED;
+  front_grouped = false;
 
   ExpandParams p{};
   p.terms = static_cast<const Term*>(program.ptr);
@@ -823,7 +1058,17 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     const auto layer_start = Clock::now();
     const uint64_t bound = next_bound(depth, count, visited);
     const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(bound, 1), plan.capacity);
-    if ((rc = next.ensure((cap + 2) * 8))) break;
+    const bool group_layer = grouped_mode && count * gens >= bucket_min_work;
+    if (!group_layer && front_grouped && (rc = gather_front(count))) break;
+    void* group_fn = nullptr;
+    size_t group_smem = 0;
+    uint64_t group_items = 0;
+    if (group_layer) {
+      const uint64_t prev_count = depth ? layer_sizes[depth - 1] : 0;
+      if ((rc = grouped_setup(count, prev_count, cap, &group_fn, &group_smem, smem, &group_items))) break;
+    } else if ((rc = next.ensure((cap + 2) * 8))) {
+      break;
+    }
     p.frontier = static_cast<const unsigned long long*>(front.ptr);
     p.count = count;
     p.next = static_cast<unsigned long long*>(next.ptr);
@@ -879,6 +1124,34 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         if ((rc = bucket_launch(reinterpret_cast<const void*>(route_fn), reinterpret_cast<const void*>(accept_fn), p,
                                 smem)))
           break;
+      } else if (group_layer) {
+        const uint32_t R = groups + 1;
+        unsigned long long* meta = static_cast<unsigned long long*>(group_meta.ptr);
+        GroupedParams gp{};
+        gp.frontier = p.frontier;
+        gp.region_begin = meta;
+        gp.region_count = meta + R;
+        gp.item_prefix = meta + 2 * R;
+        gp.region_order = reinterpret_cast<const uint32_t*>(meta + group_meta_words(groups));
+        gp.regions = R;
+        gp.groups = groups;
+        gp.terms = p.terms;
+        gp.term_begin = p.term_begin;
+        gp.gens = gens;
+        gp.total_terms = p.total_terms;
+        gp.gen_shift = p.gen_shift;
+        gp.ppt = gens <= 4 ? 4 : 2;
+        gp.bitmap = p.bitmap;
+        gp.next = p.next;
+        gp.next_begin = meta + 3 * R + 1;
+        gp.next_cap = meta + 4 * R + 1;
+        gp.next_count = meta + 5 * R + 1;
+        gp.work = meta + 6 * R + 1;
+        gp.control = p.control;
+        reinterpret_cast<GroupedFn>(group_fn)<<<grid_for(group_fn, group_smem, group_items), kBlock, group_smem,
+                                                 stream>>>(gp);
+        ++launches;
+        MG_CHECK(cudaGetLastError());
       } else {
         const uint64_t per_tile = sorted ? kSortTile / gens : kBlock * p.ppt;
         const uint64_t tiles = (count + per_tile - 1) / per_tile;
@@ -892,6 +1165,11 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       if (routed)
         MG_CHECK(cudaMemcpyAsync(host_meta + 2 * kMaxShards, static_cast<unsigned long long*>(shard_meta.ptr) + 2 * kMaxShards,
                                  bucket_shards * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+      if (group_layer) {
+        const size_t off = 5 * static_cast<size_t>(groups + 1) + 1;
+        MG_CHECK(cudaMemcpyAsync(host_group + off, static_cast<unsigned long long*>(group_meta.ptr) + off,
+                                 (groups + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+      }
       MG_CHECK(cudaStreamSynchronize(stream));
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ev_kernel[0], ev_kernel[1]) == cudaSuccess) kernel_seconds += ms * 1e-3;
@@ -926,11 +1204,14 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     const double secs = std::chrono::duration<double>(Clock::now() - layer_start).count();
     layer_sizes.push_back(c.next_count);
     layer_seconds.push_back(secs);
+    if (group_layer) grouped_finish();
     std::swap(front, next);
+    front_grouped = group_layer;
     count = c.next_count;
     visited += count;
     ++depth;
     if (count < 1000) {
+      if (front_grouped && (rc = gather_front(count))) break;
       std::vector<uint64_t> words(count);
       MG_CHECK(cudaMemcpyAsync(words.data(), front.ptr, count * 8, cudaMemcpyDeviceToHost, stream));
       MG_CHECK(cudaStreamSynchronize(stream));
@@ -941,6 +1222,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       break;
     }
   }
+  if (!rc && front_grouped) rc = gather_front(count);  // samples read `front` as one array
   last_count = count;
   st.layers = static_cast<uint32_t>(layer_sizes.size());
   for (uint64_t s : layer_sizes) st.states += s;

@@ -74,6 +74,22 @@ struct Graph {
   int bucket_setup(uint64_t work, bool exact);
   int bucket_launch(const void* route, const void* accept, const ExpandParams& p, size_t smem);
 
+  // Grouped layers (claim, then route the winners): the frontier is kept in
+  // per-group regions (states sharing their first group_prefix symbols) plus a
+  // spill region; `front_grouped` says whether `front` currently has that
+  // layout, described by front_begin / front_count (groups, then the spill).
+  uint32_t group_prefix = 0, groups = 0;
+  DeviceBuffer group_meta;
+  unsigned long long* host_group = nullptr;  // pinned mirror of group_meta
+  bool front_grouped = false;
+  std::vector<uint64_t> front_begin, front_count, next_begin, next_cap;
+  std::vector<uint32_t> group_order;  // visiting order of the groups (work items follow it)
+  void plan_group_order();
+  int grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total, size_t smem,
+                    uint64_t* items);
+  int grouped_finish();   // after the layer: per-region counts of `next` into next_begin/next_cap layout
+  int gather_front(uint64_t count);  // grouped `front` -> contiguous
+
   // Results.
   std::vector<uint64_t> layer_sizes;
   std::vector<double> layer_seconds;

@@ -1,0 +1,225 @@
+// Grouped layers of the Lehmer-bitmap path: claim first, then route only the
+// winners.
+//
+// The frontier is stored grouped by the first K symbols of the state (group =
+// the first K Lehmer digits, so group g owns the bitmap bits
+// [g * (N-K)!, (g + 1) * (N-K)!), 10! bits = 454 KB for K = N - 10).  A layer
+// is ONE kernel:
+//
+//   work items = chunks of the current frontier's groups, claimed from a
+//                device counter in a group visiting order chosen for the
+//                generators, so the resident blocks expand parents of a few
+//                neighbouring groups at a time and the target groups they
+//                share are revisited while still in L2;
+//   per parent = apply each generator, rank the child, atomicOr its bit;
+//   per winner = stage (state, group of the child, rank within the block's
+//                group run) in shared memory; a flush reserves one range per
+//                (block, group) and writes the runs to the next frontier's
+//                group regions.
+//
+// With generators that move only a few leading positions into or out of the
+// first K (LRX, adjacent transpositions), the children of one parent group
+// fall into a few tens of groups, so the bitmap words a block touches stay in
+// L2 although the whole bitmap (778 MB at N = 13) does not.  Compared with
+// route + accept (bucket_kernels.cuh) only the winners are sorted and the
+// 16 B per successor of bucket traffic disappear.
+//
+// Exactness: group regions are sized from the previous layer's distribution;
+// a winner whose group region is full goes to the spill region, whose
+// capacity is the exact bound on the next layer, so no winner is ever lost and
+// no layer is redone.  The spill is expanded after the groups, without
+// locality.  (The reference claims with random atomics from a flat candidate
+// list: cuda/permutation_bitmap.cu:105-205.)
+#pragma once
+#include "packed_kernels.cuh"
+
+namespace mgbfs2 {
+
+constexpr uint32_t kGroupStage = 2048;  // staged winners per block (4 blocks per SM fit)
+constexpr uint32_t kMaxGroups = 1728;   // 13!/10! = 1716 groups at most
+constexpr uint32_t kGroupChunk = 4096;  // parents per work item
+
+constexpr uint64_t factorial_u64(int m) { return m <= 1 ? 1ull : static_cast<uint64_t>(m) * factorial_u64(m - 1); }
+
+struct GroupedParams {
+  const unsigned long long* frontier;
+  // Regions 0..groups-1 are the groups, region `groups` is the spill.
+  const unsigned long long* region_begin;  // regions
+  const unsigned long long* region_count;  // regions
+  const unsigned long long* item_prefix;   // regions + 1: exclusive prefix of work items, in visiting order
+  const uint32_t* region_order;            // regions: the region visited j-th (the spill last)
+  uint32_t regions, groups;
+  const Term* terms;
+  const uint32_t* term_begin;
+  uint32_t gens, total_terms, gen_shift, ppt;
+  unsigned long long* bitmap;
+  unsigned long long* next;
+  const unsigned long long* next_begin;  // regions (spill last)
+  const unsigned long long* next_cap;    // regions (spill last)
+  unsigned long long* next_count;        // regions: winners reserved per region (may pass a group's cap)
+  unsigned long long* work;              // work-item counter, zero at launch
+  Control* control;
+};
+
+struct GroupedSmem {
+  uint32_t item_prefix[kMaxGroups + 2];  // the work-item prefix (regions + 1 entries, visiting order)
+  unsigned long long state[kGroupStage];
+  uint16_t grp[kGroupStage];
+  uint16_t rank[kGroupStage];
+  uint32_t hist[kMaxGroups];   // staged winners per group
+  uint32_t gbase[kMaxGroups];  // reserved position of the block's run in each group (saturated at 2^32 - 1)
+  uint16_t touched[kMaxGroups];  // the groups with staged winners, in first-touch order
+  unsigned long long item;
+  uint32_t count, ntouched;
+};
+
+// Writes the staged winners: one reservation per (block, group); positions
+// past a group's capacity go to the spill region.  All threads call it.
+__device__ __forceinline__ void grouped_flush(const GroupedParams& p, GroupedSmem& sm) {
+  __syncthreads();
+  const uint32_t touched = sm.ntouched;
+  for (uint32_t t = threadIdx.x; t < touched; t += blockDim.x) {
+    const uint32_t g = sm.touched[t];
+    const unsigned long long at = atomicAdd(&p.next_count[g], static_cast<unsigned long long>(sm.hist[g]));
+    // A saturated base only sends the run to the spill region.
+    sm.gbase[g] = at < 0xffffffffull ? static_cast<uint32_t>(at) : 0xffffffffu;
+  }
+  __syncthreads();
+  const uint32_t n = sm.count;
+  bool overflow = false;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t g = sm.grp[i];
+    const unsigned long long pos = static_cast<unsigned long long>(sm.gbase[g]) + sm.rank[i];
+    if (pos < __ldg(&p.next_cap[g])) {
+      p.next[__ldg(&p.next_begin[g]) + pos] = sm.state[i];
+    } else {
+      const unsigned long long sp = atomicAdd(&p.next_count[p.groups], 1ull);
+      if (sp < __ldg(&p.next_cap[p.groups])) p.next[__ldg(&p.next_begin[p.groups]) + sp] = sm.state[i];
+      else overflow = true;
+    }
+  }
+  if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
+  if (threadIdx.x == 0 && n) atomicAdd(&p.control->next_count, static_cast<unsigned long long>(n));
+  __syncthreads();
+  for (uint32_t t = threadIdx.x; t < touched; t += blockDim.x) sm.hist[sm.touched[t]] = 0;
+  if (threadIdx.x == 0) {
+    sm.count = 0;
+    sm.ntouched = 0;
+  }
+  __syncthreads();
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  GroupedSmem& sm = *reinterpret_cast<GroupedSmem*>(dyn_smem);
+  Term* terms = reinterpret_cast<Term*>(dyn_smem + sizeof(GroupedSmem));
+  uint32_t* tbegin = reinterpret_cast<uint32_t*>(dyn_smem + sizeof(GroupedSmem) + p.total_terms * sizeof(Term));
+  for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
+  for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
+  const uint32_t* inverse = tbegin + p.gens + 1;
+  for (uint32_t g = threadIdx.x; g < p.groups; g += blockDim.x) sm.hist[g] = 0;
+  for (uint32_t r = threadIdx.x; r <= p.regions; r += blockDim.x)
+    sm.item_prefix[r] = static_cast<uint32_t>(p.item_prefix[r]);
+  if (threadIdx.x == 0) {
+    sm.count = 0;
+    sm.ntouched = 0;
+  }
+  __syncthreads();
+  constexpr uint64_t kGroupSize = factorial_u64(N - K);  // bits per group
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const uint32_t round = kBlock * p.ppt;
+  const uint32_t items = sm.item_prefix[p.regions];
+  for (;;) {
+    if (tid == 0) sm.item = atomicAdd(p.work, 1ull);
+    __syncthreads();
+    const unsigned long long item = sm.item;
+    if (item >= items) break;
+    uint32_t lo = 0, hi = p.regions;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (sm.item_prefix[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const unsigned long long first = (item - sm.item_prefix[lo]) * kGroupChunk;
+    const uint32_t region = __ldg(&p.region_order[lo]);
+    const unsigned long long avail = p.region_count[region] - first;
+    const uint32_t n = static_cast<uint32_t>(avail < kGroupChunk ? avail : kGroupChunk);
+    const unsigned long long* src = p.frontier + p.region_begin[region] + first;
+    for (uint32_t r0 = 0; r0 < n; r0 += round) {
+      uint64_t par[4];
+      uint32_t skip[4];
+      bool val[4];
+      bool untagged = false;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t i = r0 + k * kBlock + tid;
+        val[k] = k < static_cast<int>(p.ppt) && i < n;
+        par[k] = val[k] ? src[i] : 0ull;
+        const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
+        skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
+        untagged = untagged || (val[k] && !tag);
+      }
+      // Pass j applies to every parent its j-th generator other than the
+      // skipped one, so a round of tagged parents is done after gens - 1
+      // passes with no idle lanes.
+      const uint32_t passes = __syncthreads_or(untagged) ? p.gens : p.gens - 1;
+      for (uint32_t j = 0; j < passes; ++j) {
+        // Room for this pass's winners (at most one per parent).
+        __syncthreads();
+        const uint32_t pending = sm.count;
+        __syncthreads();
+        if (pending + round > kGroupStage) grouped_flush(p, sm);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t g = j + (j >= skip[k] ? 1u : 0u);
+          const bool live = val[k] && g < p.gens;
+          const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
+          bool won = false;
+          uint64_t c = 0, r = 0;
+          if (live) {
+            c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
+            r = lehmer_rank4<N>(c);
+            const unsigned long long bit = 1ull << (r & 63);
+            won = !(atomicOr(&p.bitmap[r >> 6], bit) & bit);
+          }
+          const unsigned m = __ballot_sync(kFullMask, won);
+          if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(&sm.count, static_cast<uint32_t>(__popc(m)));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (won) {
+              const uint32_t grp = static_cast<uint32_t>(r / kGroupSize);
+              const unsigned peers = __match_any_sync(m, grp);
+              const int gl = __ffs(peers) - 1;
+              uint32_t rb = 0;
+              if (static_cast<int>(lane) == gl) {
+                rb = atomicAdd(&sm.hist[grp], static_cast<uint32_t>(__popc(peers)));
+                if (rb == 0) sm.touched[atomicAdd(&sm.ntouched, 1u)] = static_cast<uint16_t>(grp);
+              }
+              rb = __shfl_sync(peers, rb, gl) + __popc(peers & lanemask_lt());
+              const uint32_t slot = base + __popc(m & lanemask_lt());
+              sm.state[slot] = c | gtag;
+              sm.grp[slot] = static_cast<uint16_t>(grp);
+              sm.rank[slot] = static_cast<uint16_t>(rb);
+            }
+          }
+        }
+      }
+    }
+  }
+  grouped_flush(p, sm);
+}
+
+// Copies a grouped frontier into one contiguous array (regions in order).
+static __global__ void gather_regions(const unsigned long long* src, const unsigned long long* begin,
+                                      const unsigned long long* count, const unsigned long long* out_prefix,
+                                      uint32_t regions, unsigned long long* dst) {
+  for (uint32_t r = blockIdx.x; r < regions; r += gridDim.x) {
+    const unsigned long long b = begin[r], c = count[r], o = out_prefix[r];
+    for (unsigned long long i = threadIdx.x; i < c; i += blockDim.x) dst[o + i] = src[b + i];
+  }
+}
+
+}  // namespace mgbfs2

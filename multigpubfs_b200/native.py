@@ -18,7 +18,7 @@ _LIB = None
 DEVICE_STATUS = 5  # MGBFS2_DEVICE_STATUS
 VISITED = {"auto": 0, "bitmap": 1, "hash": 2, "hash3": 3}
 VISITED_NAMES = {v: k for k, v in VISITED.items()}
-DEDUP = {"auto": 0, "atomic": 1, "warp": 2, "sort": 3, "bucket": 4}
+DEDUP = {"auto": 0, "atomic": 1, "warp": 2, "sort": 3, "bucket": 4, "grouped": 5}
 DEDUP_NAMES = {v: k for k, v in DEDUP.items()}
 PLANNER = {"plain": 0, "learned": 1}
 REASONS = {0: "FRONTIER_EXHAUSTED", 1: "DEADLINE", 2: "CANCELLED", 3: "RESOURCE", 4: "PROFILE_LAYER_LIMIT"}

@@ -54,6 +54,11 @@ VARIANTS = {
     "bitmap_sort_noskip": dict(visited="bitmap", dedup="sort", parent_skip=False),
     "hash_sort": dict(visited="hash", dedup="sort"),
     "hash3_sort": dict(visited="hash3", dedup="sort"),
+    # claim, then route the winners into a prefix-grouped frontier, every layer
+    "bitmap_grouped": dict(visited="bitmap", dedup="grouped", bucket_min_work=1),
+    # no group margin: most winners of the first grouped layers go to the spill region
+    "bitmap_grouped_tight": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, bucket_margin=0),
+    "bitmap_grouped_noskip": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, parent_skip=False),
 }
 
 
@@ -110,7 +115,8 @@ def test_parent_skip_accounting(lrx_layers):
 
 @pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3", "bitmap_bucket",
                                      "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip", "bitmap_sort",
-                                     "bitmap_sort_noskip", "hash_sort", "hash3_sort"])
+                                     "bitmap_sort_noskip", "hash_sort", "hash3_sort", "bitmap_grouped",
+                                     "bitmap_grouped_tight", "bitmap_grouped_noskip"])
 def test_lrx_small(lrx_layers, variant):
     redo = 0
     for n in range(3, 12):
@@ -122,9 +128,11 @@ def test_lrx_small(lrx_layers, variant):
         assert redo > 0  # the exact redo path ran and changed nothing
 
 
-@pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic", "bitmap_bucket_default"])
+@pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic", "bitmap_bucket_default", "bitmap_grouped_default"])
 def test_lrx13_full_table(lrx13, variant):
-    plan = VARIANTS.get(variant, dict(visited="bitmap", dedup="bucket"))
+    defaults = {"bitmap_bucket_default": dict(visited="bitmap", dedup="bucket"),
+                "bitmap_grouped_default": dict(visited="bitmap", dedup="grouped")}
+    plan = VARIANTS.get(variant) or defaults[variant]
     out = run(G.permutation_graph(G.lrx_generators(13), list(range(13))), **plan)
     info, r, last, prev = out
     assert info["visited"] == "bitmap"
@@ -134,9 +142,9 @@ def test_lrx13_full_table(lrx13, variant):
     assert sorted(last[0]) == list(range(13))
 
 
-@pytest.mark.parametrize("n", [12, 13])
-def test_coxeter_bucketed(n):
-    out = run(G.permutation_graph(G.coxeter_generators(n), list(range(n))), visited="bitmap", dedup="bucket")
+@pytest.mark.parametrize("n,dedup", [(12, "bucket"), (13, "bucket"), (12, "grouped"), (13, "grouped")])
+def test_coxeter_bucketed(n, dedup):
+    out = run(G.permutation_graph(G.coxeter_generators(n), list(range(n))), visited="bitmap", dedup=dedup)
     assert out[1].layer_sizes == G.coxeter_layers(n)
     # The deepest Coxeter layer is the single longest element (the reversal).
     assert out[2] == [list(range(n))[::-1]]
@@ -161,7 +169,7 @@ def test_random_sweep_instances(closed):
         g = G.sweep_instance(i, closed)
         n = len(g["start"])
         ref, last_ref, _ = P.packed_bfs(g["action"]["generators"], g["start"], sample=1 << 22)
-        for variant in ("auto", "hash", "bitmap_warp", "bitmap_sort", "hash_sort") + \
+        for variant in ("auto", "hash", "bitmap_warp", "bitmap_sort", "hash_sort", "bitmap_grouped_tight") + \
                 (("hash3", "hash3_sort") if closed else ()):
             out = run(g, **VARIANTS[variant])
             assert out[1].layer_sizes == ref, (i, variant, n)
