@@ -62,7 +62,7 @@ def coxeter(n):
 WORKLOADS = {
     "s13-lrx": dict(n=13, gens=lrx(13), visited="bitmap", dedup="grouped",
                     desc="S13 LRX full BFS (L, R, X from identity; 6,227,020,800 states), exact Lehmer-rank bitmap"),
-    "s13-coxeter": dict(n=13, gens=coxeter(13), visited="bitmap", dedup="bucket",
+    "s13-coxeter": dict(n=13, gens=coxeter(13), visited="bitmap", dedup="grouped",
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash3", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash, 3 layer banks"),
@@ -407,9 +407,11 @@ def main():
         prof = ROOT / "profiles" / f"traffic_{args.workload}.json"
         if prof.exists():
             try:
-                traffic = json.loads(prof.read_text()).get("dram_bytes_per_bfs")
+                traffic = json.loads(prof.read_text()).get(plan["dedup"], {}).get("dram_bytes_per_bfs")
             except Exception:
                 traffic = None
+        kernel_names = {"grouped": "expand_grouped (grouped layers; small layers expand_packed)",
+                        "bucket": "route_lehmer + accept_lehmer (bucketed layers; small layers expand_packed)"}
         line = {
             "metric": "successors/s",
             "value": world * succ * args.steps / device_max,
@@ -435,7 +437,8 @@ def main():
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "b_alg_bytes": b_alg, "kernel": "expand_packed (layer expansion)"},
+                         "b_alg_bytes": b_alg,
+                         "kernel": kernel_names.get(plan["dedup"], "expand_packed (fused layer expansion)")},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
