@@ -229,4 +229,23 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return mask;
 }
 
+// L2 eviction priority for the bitmap words a layer keeps hitting: an
+// evict-last access policy (PTX createpolicy) attached to the atomicOr, so the
+// streaming frontier traffic is evicted before the hot bitmap lines.
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+  unsigned long long policy;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
+  return policy;
+}
+
+__device__ __forceinline__ unsigned long long atomic_or_hinted(unsigned long long* address, unsigned long long bits,
+                                                               unsigned long long policy) {
+  unsigned long long old;
+  asm volatile("atom.global.or.L2::cache_hint.b64 %0, [%1], %2, %3;"
+               : "=l"(old)
+               : "l"(address), "l"(bits), "l"(policy)
+               : "memory");
+  return old;
+}
+
 }  // namespace mgbfs2

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
             c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
             r = lehmer_rank4<N>(c);
             const unsigned long long bit = 1ull << (r & 63);
-            won = !(atomicOr(&p.bitmap[r >> 6], bit) & bit);
+            won = !(atomic_or_hinted(&p.bitmap[r >> 6], bit, l2_policy_evict_last()) & bit);
           }
           const unsigned m = __ballot_sync(kFullMask, won);
           if (m) {
