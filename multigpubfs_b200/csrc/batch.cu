@@ -51,6 +51,7 @@ enum : uint32_t { INST_ACTIVE = 0, INST_DONE = 1, INST_OVERFLOW = 2, INST_IDLE =
 struct BatchInst {
   uint32_t n, gens, term_off, inv_off;  // term_off: first of gens + 1 offsets in tbegin
   uint32_t gen_shift, status;           // parent-edge tag position (0 = none)
+  uint32_t sel_off, bytes;              // byte-permute selectors (6 per generator) when bytes != 0
   unsigned long long bitmap_off;        // first bitmap word
   unsigned long long seg_off, seg_cap;  // frontier segment (same in both buffers)
 };
@@ -68,6 +69,7 @@ struct BatchParams {
   const Term* terms;
   const uint32_t* tbegin;   // absolute term offsets
   const uint32_t* inverse;  // absolute generator index -> inverse generator index (within the instance)
+  const uint32_t* sel;      // byte-permute selectors, 6 per generator of a byte-path instance
   unsigned long long* bitmap;
   unsigned long long* buf[2];
   unsigned long long* tile_prefix;  // count + 1 entries: exclusive prefix of per-instance tile counts
@@ -82,10 +84,11 @@ struct BatchParams {
 struct BatchSmem {
   unsigned long long out[kBatchOut];
   Term terms[kMaxBatchTerms];
+  uint32_t sel[kMaxBatchGens * 6];
   uint32_t begin[kMaxBatchGens + 1];
   uint32_t inverse[kMaxBatchGens];
   unsigned long long bitmap_off, seg_off, seg_cap, count, tile, local_tile, out_base;
-  uint32_t inst, found, n, gens, shift, out_count;
+  uint32_t inst, found, n, gens, shift, out_count, bytes;
 };
 
 __device__ __forceinline__ uint32_t find_instance(const unsigned long long* prefix, uint32_t count,
@@ -126,10 +129,112 @@ __device__ __forceinline__ void batch_flush(const TileArgs a, BatchSmem& s) {
   __syncthreads();
 }
 
+// Byte-lane form of a packed state of at most 12 symbols: symbol i in byte
+// i % 4 of register i / 4 (nibble -> byte spreading, 4 ops per register).
+__device__ __forceinline__ void spread_bytes(uint64_t w, uint32_t (&b)[3]) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const uint32_t v = static_cast<uint32_t>(w >> (16 * j)) & 0xffffu;
+    const uint32_t y = (v | (v << 8)) & 0x00ff00ffu;
+    b[j] = (y | (y << 4)) & 0x0f0f0f0fu;
+  }
+}
+
+// Inverse of spread_bytes for byte values below 16.
+__device__ __forceinline__ uint64_t pack_bytes(const uint32_t (&b)[3]) {
+  uint64_t w = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const uint32_t y = (b[j] | (b[j] >> 4)) & 0x00ff00ffu;
+    w |= static_cast<uint64_t>((y | (y >> 8)) & 0xffffu) << (16 * j);
+  }
+  return w;
+}
+
+// Lehmer rank of N <= 12 distinct byte-lane symbols.
+template <int N>
+__device__ __forceinline__ uint32_t lehmer_rank_bytes(const uint32_t (&b)[3]) {
+  uint32_t used = 0, rank = 0;
+#pragma unroll
+  for (int i = 0; i < N - 1; ++i) {
+    const uint32_t s = (b[i >> 2] >> (8 * (i & 3))) & 0xffu;
+    rank = rank * static_cast<uint32_t>(N - i) + (s - __popc(used & ((1u << s) - 1u)));
+    used |= 1u << s;
+  }
+  return rank;
+}
+
+// Tile of a byte-path instance (N <= 12, generators with many displacement
+// groups): every parent is spread to byte lanes once, and each child is two
+// byte permutes per output register (selectors precomputed on the host)
+// instead of one shift-mask-or per displacement group; only winners are
+// packed back to nibbles.
+template <int N>
+__device__ __forceinline__ void batch_tile_bytes(const TileArgs a, BatchSmem& s) {
+  const uint32_t lane = lane_id();
+  const unsigned long long count = s.count, base = s.local_tile * kBatchTile;
+  const uint32_t gens = s.gens, shift = s.shift;
+  const unsigned long long* seg = a.front + s.seg_off;
+  unsigned int* bitmap = reinterpret_cast<unsigned int*>(a.bitmap + s.bitmap_off);
+  uint32_t eb[kBatchPpt][3];
+  uint32_t skip[kBatchPpt];
+  bool val[kBatchPpt];
+#pragma unroll
+  for (uint32_t k = 0; k < kBatchPpt; ++k) {
+    const unsigned long long idx = base + k * kBatchBlock + threadIdx.x;
+    val[k] = idx < count;
+    uint64_t w = val[k] ? seg[idx] : 0ull;
+    const uint32_t tag = shift ? static_cast<uint32_t>(w >> shift) : 0u;
+    skip[k] = tag ? s.inverse[tag - 1] : 0xffffffffu;
+    if (shift) w &= (1ull << shift) - 1ull;
+    spread_bytes(w, eb[k]);
+  }
+  for (uint32_t g = 0; g < gens; ++g) {
+    const uint32_t* sel = s.sel + 6 * g;
+    const uint32_t s0 = sel[0], s1 = sel[1], s2 = sel[2], s3 = sel[3], s4 = sel[4], s5 = sel[5];
+    const unsigned long long gtag = shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull;
+#pragma unroll
+    for (uint32_t k = 0; k < kBatchPpt; ++k) {
+      const bool live = val[k] && g != skip[k];
+      bool won = false;
+      uint32_t cb[3];
+      cb[0] = __byte_perm(__byte_perm(eb[k][0], eb[k][1], s0), eb[k][2], s1);
+      cb[1] = __byte_perm(__byte_perm(eb[k][0], eb[k][1], s2), eb[k][2], s3);
+      cb[2] = __byte_perm(__byte_perm(eb[k][0], eb[k][1], s4), eb[k][2], s5);
+      if (live) {
+        const uint32_t r = lehmer_rank_bytes<N>(cb);
+        const uint32_t bit = 1u << (r & 31);
+        won = !(atomicOr(&bitmap[r >> 5], bit) & bit);
+      }
+      const unsigned m = __ballot_sync(kFullMask, won);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t at = 0;
+        if (static_cast<int>(lane) == leader) at = atomicAdd(&s.out_count, static_cast<uint32_t>(__popc(m)));
+        at = __shfl_sync(kFullMask, at, leader);
+        if (won) s.out[at + __popc(m & lanemask_lt())] = pack_bytes(cb) | gtag;
+      }
+    }
+    if (g + 1 < gens) {
+      __syncthreads();
+      const uint32_t pending = s.out_count;
+      __syncthreads();
+      if (pending + kBatchTile > kBatchOut) batch_flush(a, s);
+    }
+  }
+  batch_flush(a, s);
+}
+
 // One tile (kBatchTile consecutive entries of one instance's frontier) with a
 // compile-time degree, so the Lehmer rank is fully unrolled.
 template <int N>
 __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
+  if constexpr (N <= 12) {
+    if (s.bytes) {
+      batch_tile_bytes<N>(a, s);
+      return;
+    }
+  }
   const uint32_t lane = lane_id();
   const unsigned long long count = s.count, base = s.local_tile * kBatchTile;
   const uint32_t gens = s.gens, shift = s.shift;
@@ -220,11 +325,14 @@ __global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
       for (uint32_t k = threadIdx.x; k < t1 - t0; k += blockDim.x) s.terms[k] = p.terms[t0 + k];
       for (uint32_t k = threadIdx.x; k <= in.gens; k += blockDim.x) s.begin[k] = p.tbegin[in.term_off + k] - t0;
       for (uint32_t k = threadIdx.x; k < in.gens; k += blockDim.x) s.inverse[k] = p.inverse[in.inv_off + k];
+      if (in.bytes)
+        for (uint32_t k = threadIdx.x; k < 6 * in.gens; k += blockDim.x) s.sel[k] = p.sel[in.sel_off + k];
       if (threadIdx.x == 0) {
         s.inst = i;
         s.n = in.n;
         s.gens = in.gens;
         s.shift = in.gen_shift;
+        s.bytes = in.bytes;
         s.bitmap_off = in.bitmap_off;
         s.seg_off = in.seg_off;
         s.seg_cap = in.seg_cap;
@@ -359,6 +467,7 @@ struct Batch {
     std::vector<Term> terms;
     std::vector<uint32_t> begin;   // gens + 1 relative offsets
     std::vector<uint32_t> inverse; // gens entries
+    std::vector<uint32_t> sel;     // byte-permute selectors (6 per generator); empty = displacement terms
     bool inverse_closed = false;
     uint64_t orbit = 0;            // n!
     std::vector<uint64_t> layers;
@@ -413,6 +522,26 @@ static int validate_instance(const mgbfs2_graph_desc& d, Batch::Instance* out, s
     }
     in.begin.push_back(static_cast<uint32_t>(in.terms.size()));
   }
+  // Byte path for degree <= 12 when the generators average more than three
+  // displacement groups: child register j (symbols 4j..4j+3) is
+  // perm(perm(parent0, parent1, s1), parent2, s2) over the byte lanes, with
+  // source symbol g[q] (or a zero lane past the degree) for every output symbol q.
+  if (n <= 12 && in.terms.size() > 3ull * in.gens) {
+    for (uint32_t k = 0; k < in.gens; ++k) {
+      const uint32_t* g = d.permutations + static_cast<size_t>(k) * n;
+      for (uint32_t j = 0; j < 3; ++j) {
+        uint32_t s1 = 0, s2 = 0;
+        for (uint32_t t = 0; t < 4; ++t) {
+          const uint32_t q = 4 * j + t;
+          const uint32_t src = q < n ? g[q] : (n < 12 ? n : 0);
+          s1 |= (src < 8 ? src : 0u) << (4 * t);
+          s2 |= (src < 8 ? t : 4 + (src - 8)) << (4 * t);
+        }
+        in.sel.push_back(s1);
+        in.sel.push_back(s2);
+      }
+    }
+  }
   in.inverse_closed = true;
   in.inverse.assign(in.gens, 0xffffffffu);
   for (uint32_t k = 0; k < in.gens; ++k) {
@@ -464,7 +593,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const uint32_t W = static_cast<uint32_t>(ids.size());
   std::vector<BatchInst> host(W);
   std::vector<Term> terms;
-  std::vector<uint32_t> tbegin, inverse;
+  std::vector<uint32_t> tbegin, inverse, sels;
   uint64_t bitmap_words = 0, seg = 0;
   for (uint32_t k = 0; k < W; ++k) {
     const auto& in = b->inst[ids[k]];
@@ -477,6 +606,9 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     h.inv_off = static_cast<uint32_t>(inverse.size());
     inverse.insert(inverse.end(), in.inverse.begin(), in.inverse.end());
     h.gen_shift = in.inverse_closed ? 4 * in.n : 0;
+    h.bytes = in.sel.empty() ? 0u : 1u;
+    h.sel_off = static_cast<uint32_t>(sels.size());
+    sels.insert(sels.end(), in.sel.begin(), in.sel.end());
     h.status = INST_ACTIVE;
     h.bitmap_off = bitmap_words;
     bitmap_words += (in.orbit + 63) / 64;
@@ -492,6 +624,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const size_t o_terms = off; off = al(off + terms.size() * sizeof(Term) + 16);
   const size_t o_tbegin = off; off = al(off + tbegin.size() * 4 + 4);
   const size_t o_inv = off; off = al(off + inverse.size() * 4 + 4);
+  const size_t o_sel = off; off = al(off + sels.size() * 4 + 4);
   const size_t o_prefix = off; off = al(off + (W + 1) * 8);
   const size_t o_cur = off; off = al(off + W * 8);
   const size_t o_next = off; off = al(off + W * 8);
@@ -512,6 +645,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   MG_CHECK_BATCH(cudaMemcpyAsync(base + o_tbegin, tbegin.data(), tbegin.size() * 4, cudaMemcpyHostToDevice, b->stream));
   if (!inverse.empty())
     MG_CHECK_BATCH(cudaMemcpyAsync(base + o_inv, inverse.data(), inverse.size() * 4, cudaMemcpyHostToDevice, b->stream));
+  if (!sels.empty())
+    MG_CHECK_BATCH(cudaMemcpyAsync(base + o_sel, sels.data(), sels.size() * 4, cudaMemcpyHostToDevice, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(base + o_ctl, &ctl, sizeof(ctl), cudaMemcpyHostToDevice, b->stream));
   MG_CHECK_BATCH(cudaMemsetAsync(base + o_layers, 0, static_cast<size_t>(W) * max_depth * 8, b->stream));
   MG_CHECK_BATCH(cudaMemsetAsync(base + o_bitmap, 0, bitmap_words * 8, b->stream));
@@ -521,6 +656,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   p.terms = reinterpret_cast<const Term*>(base + o_terms);
   p.tbegin = reinterpret_cast<const uint32_t*>(base + o_tbegin);
   p.inverse = reinterpret_cast<const uint32_t*>(base + o_inv);
+  p.sel = reinterpret_cast<const uint32_t*>(base + o_sel);
   p.bitmap = reinterpret_cast<unsigned long long*>(base + o_bitmap);
   p.buf[0] = reinterpret_cast<unsigned long long*>(base + o_buf0);
   p.buf[1] = reinterpret_cast<unsigned long long*>(base + o_buf1);

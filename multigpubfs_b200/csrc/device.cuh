@@ -86,6 +86,26 @@ __device__ __forceinline__ uint64_t lehmer_rank4(uint64_t w) {
   return lo;
 }
 
+// lehmer_rank4<N> split at digit K: *group = the first K digits in mixed radix
+// N, N-1, ..., N-K+1 and *inner = the Horner value of the remaining digits, so
+// rank = group * (N-K)! + inner.  Needs (N-K)! < 2^32, i.e. N - K <= 12.
+template <int N, int K>
+__device__ __forceinline__ void lehmer_split4(uint64_t w, uint32_t* group, uint32_t* inner) {
+  static_assert(N - K <= 12, "in-group rank must fit 32 bits");
+  const uint32_t lo_word = static_cast<uint32_t>(w), hi_word = static_cast<uint32_t>(w >> 32);
+  uint32_t used = 0, head = 0, tail = 0;
+#pragma unroll
+  for (int i = 0; i < N - 1; ++i) {
+    const uint32_t s = (i < 8 ? (lo_word >> (4 * i)) : (hi_word >> (4 * (i - 8)))) & 15u;
+    const uint32_t c = s - __popc(used & ((1u << s) - 1u));
+    used |= 1u << s;
+    if (i < K) head = head * static_cast<uint32_t>(N - i) + c;
+    else tail = tail * static_cast<uint32_t>(N - i) + c;
+  }
+  *group = head;
+  *inner = tail;
+}
+
 // Inverse of lehmer_rank4<N>: factorial-base digits (mixed radix, least
 // significant first, all divisors compile-time constants), then the c_i-th
 // unused symbol of a sorted nibble list for every position.
@@ -236,6 +256,16 @@ __device__ __forceinline__ unsigned long long l2_policy_evict_last() {
   unsigned long long policy;
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
   return policy;
+}
+
+__device__ __forceinline__ unsigned int atomic_or_hinted32(unsigned int* address, unsigned int bits,
+                                                           unsigned long long policy) {
+  unsigned int old;
+  asm volatile("atom.global.or.L2::cache_hint.b32 %0, [%1], %2, %3;"
+               : "=r"(old)
+               : "l"(address), "r"(bits), "l"(policy)
+               : "memory");
+  return old;
 }
 
 __device__ __forceinline__ unsigned long long atomic_or_hinted(unsigned long long* address, unsigned long long bits,

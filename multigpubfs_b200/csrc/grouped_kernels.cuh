@@ -127,6 +127,8 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   }
   __syncthreads();
   constexpr uint64_t kGroupSize = factorial_u64(N - K);  // bits per group
+  constexpr bool kSplitRank = N - K >= 8 && N - K <= 12;  // 32-bit in-group rank, word-aligned groups
+  constexpr uint64_t kGroupWords32 = kGroupSize / 32;
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const uint32_t round = kBlock * p.ppt;
   const uint32_t items = sm.item_prefix[p.regions];
@@ -176,12 +178,26 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
           const bool live = val[k] && g < p.gens;
           const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
           bool won = false;
-          uint64_t c = 0, r = 0;
+          uint64_t c = 0;
+          uint32_t grp = 0;
           if (live) {
             c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
-            r = lehmer_rank4<N>(c);
-            const unsigned long long bit = 1ull << (r & 63);
-            won = !(atomic_or_hinted(&p.bitmap[r >> 6], bit, l2_policy_evict_last()) & bit);
+            if constexpr (kSplitRank) {
+              // Group = the first K Lehmer digits, and the rank inside the group
+              // in 32 bits; (N-K)! is a multiple of 32, so group regions start
+              // on 32-bit words and the claim is a 32-bit atomicOr.
+              uint32_t inner = 0;
+              lehmer_split4<N, K>(c, &grp, &inner);
+              const uint32_t bit = 1u << (inner & 31);
+              unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
+                                   (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
+              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+            } else {
+              const uint64_t r = lehmer_rank4<N>(c);
+              const unsigned long long bit = 1ull << (r & 63);
+              won = !(atomic_or_hinted(&p.bitmap[r >> 6], bit, l2_policy_evict_last()) & bit);
+              grp = static_cast<uint32_t>(r / kGroupSize);
+            }
           }
           const unsigned m = __ballot_sync(kFullMask, won);
           if (m) {
@@ -190,7 +206,6 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
             if (static_cast<int>(lane) == leader) base = atomicAdd(&sm.count, static_cast<uint32_t>(__popc(m)));
             base = __shfl_sync(kFullMask, base, leader);
             if (won) {
-              const uint32_t grp = static_cast<uint32_t>(r / kGroupSize);
               const unsigned peers = __match_any_sync(m, grp);
               const int gl = __ffs(peers) - 1;
               uint32_t rb = 0;
