@@ -232,7 +232,7 @@ def bench_planner(args, local):
     import torch
     from multigpubfs_b200 import workloads
     from multigpubfs_b200.batch import BatchSweep
-    from multigpubfs_b200.planner import (PlannerNet, calibrate_margin, predicted_capacities, rollout,
+    from multigpubfs_b200.planner import (PlannerNet, calibrate_margin, predicted_capacities, rollout_device,
                                           training_set)
     torch.cuda.set_device(local)
     t0 = time.perf_counter()
@@ -274,8 +274,8 @@ def bench_planner(args, local):
         same = out["plain"]["layer_tables"] == out["learned"]["layer_tables"]
         same_all &= same
         peaks = [max(t) for t in out["plain"]["layer_tables"]]
-        prof = rollout(net, graphs)
-        logr = sorted(math.log(q / max(1.0, max(p))) for p, q in zip(prof, peaks))
+        peaks_pred, _, _ = rollout_device(net, graphs)
+        logr = sorted(math.log(q / max(1.0, p)) for p, q in zip(peaks_pred, peaks))
         learned_wall = out["learned"]["seconds"] + predict_s
         report[name] = {
             "workload": desc, "instances": len(graphs), "memory_budget_bytes": budget, "identical_tables": same,

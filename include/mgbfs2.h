@@ -322,6 +322,18 @@ MGBFS2_API int mgbfs2_mlp_to_bf16(uint32_t count, const float* params, void* par
 MGBFS2_API int mgbfs2_mlp_infer_bf16(uint32_t inputs, const void* params_bf16, const float* x, uint64_t batch,
                                      float* y, void* stream);
 
+/* Device rollout of the planner network (16 inputs, bf16 parameters as made by
+ * mgbfs2_mlp_to_bf16), one thread per instance: from |L_0| = 1, predicts
+ * layer after layer from the last four (features normalised by x_mean and
+ * x_scale, 16 floats each) until the prediction drops below one half or
+ * max_depth layers, and writes each instance's predicted peak layer, total and
+ * depth.  statics: count x 8 floats (log orbit, n/16, g/8, inverse-closed, mean
+ * and max log generator order, fixed-point fraction, cycle fraction); gens:
+ * count floats.  All device pointers.  No reference counterpart. */
+MGBFS2_API int mgbfs2_mlp_rollout_bf16(const void* params_bf16, const float* x_mean, const float* x_scale,
+                                       const float* statics, const float* gens, uint32_t count, uint32_t max_depth,
+                                       double* peak, double* total, uint32_t* depth, void* stream);
+
 /* Order of the group generated by `generators` permutations of {0..n-1}
  * (row-major, g[i] = image of i; n <= 20), by deterministic Schreier-Sims on
  * the host.  With distinct labels it is the exact number of states a BFS

@@ -138,6 +138,55 @@ extern "C" int mgbfs2_group_order(const uint32_t* permutations, uint32_t n, uint
   }
   for (const Perm& s : c.strong)
     if (c.fixes_prefix(s, c.base.size())) c.add_level(moved_point(s));
+  // Fast exact exit.  The product of the orbit lengths of any partial chain
+  // built from group elements is a lower bound on |G|; n! (n!/2 when every
+  // generator is even) is an upper bound.  Sifting a random walk over the
+  // generators into the chain usually lifts the lower bound to the upper one
+  // within a few dozen steps when G is the symmetric or alternating group (as
+  // for random generators); equality proves the order.  Otherwise the
+  // deterministic completion below finishes the chain.
+  {
+    uint64_t upper = 1;
+    for (uint32_t k = 2; k <= n; ++k) upper *= k;
+    bool all_even = true;
+    for (const Perm& s : c.strong) {
+      uint32_t cycles = 0;
+      std::array<uint8_t, kMaxPoints> seen{};
+      for (uint32_t x = 0; x < n; ++x) {
+        if (seen[x]) continue;
+        ++cycles;
+        for (uint32_t y = x; !seen[y]; y = s[y]) seen[y] = 1;
+      }
+      if ((n - cycles) & 1u) all_even = false;
+    }
+    if (all_even) upper /= 2;
+    const size_t gens0 = c.strong.size();
+    Perm walk = identity();
+    uint64_t state = 0x9e3779b97f4a7c15ull;
+    for (uint32_t step = 0; step < 64 * n; ++step) {
+      state ^= state << 13;
+      state ^= state >> 7;
+      state ^= state << 17;
+      walk = compose(walk, c.strong[state % gens0]);
+      Perm h = walk;
+      const size_t j = c.sift(h, 0);
+      if (is_identity(h)) continue;
+      c.strong.push_back(h);
+      if (j == c.base.size()) c.add_level(moved_point(h));
+      for (size_t l = 0; l <= j && l < c.base.size(); ++l) c.fresh[l] = 0;
+      uint64_t lower = 1;
+      for (size_t l = 0; l < c.base.size(); ++l) {
+        if (!c.fresh[l]) c.build(l);
+        uint64_t orbit = 0;
+        for (uint32_t q = 0; q < n; ++q) orbit += c.present[l][q];
+        lower *= orbit;
+      }
+      if (lower == upper) {
+        *order = upper;
+        return MGBFS2_OK;
+      }
+    }
+  }
   // Level i is complete when every Schreier generator of its orbit sifts to
   // the identity through the levels below it.
   long i = static_cast<long>(c.base.size()) - 1;

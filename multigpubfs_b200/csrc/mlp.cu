@@ -179,6 +179,74 @@ __global__ void __launch_bounds__(kMlpBlock) mlp_infer_bf16_kernel(uint32_t in, 
   }
 }
 
+// Whole-profile rollout on the device, one thread per instance: the 16
+// planner features of depth d are formed from the last four predicted layers
+// (bookkeeping in fp64), run through the same bf16 network as
+// mlp_infer_bf16_kernel (bf16 inputs and hidden activations, fp32
+// accumulation), and the predicted next layer
+//     |L_{d+1}| = min(expm1(y0 + log1p |L_d|), orbit - visited, g |L_d|)
+// is appended until it drops below one half.  statics[8 m + k] holds
+// log orbit, n/16, g/8, inverse-closed, mean and max log generator order,
+// fixed-point fraction and cycle fraction; gens[m] the generator counts.
+constexpr uint32_t kRolloutInputs = 16;
+
+__global__ void __launch_bounds__(kMlpBlock) mlp_rollout_kernel(const __nv_bfloat16* params, const float* x_mean,
+                                                                const float* x_scale, const float* statics,
+                                                                const float* gens, uint32_t count, uint32_t max_depth,
+                                                                double* peak, double* total, uint32_t* depth) {
+  extern __shared__ __nv_bfloat16 Q[];
+  const Offsets o = offsets(kRolloutInputs);
+  for (uint32_t i = threadIdx.x; i < o.total; i += blockDim.x) Q[i] = params[i];
+  __syncthreads();
+  const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= count) return;
+  const float* st = statics + 8ull * m;
+  const double g = gens[m], log_orbit = st[0], orbit = exp(log_orbit);
+  double last[4] = {1.0, 0.0, 0.0, 0.0}, visited = 1.0, best = 1.0, sum = 1.0;
+  uint32_t d = 0;
+  for (; d < max_depth; ++d) {
+    float x[kRolloutInputs];
+    for (int k = 0; k < 4; ++k) x[k] = static_cast<float>(log1p(last[k]));
+    x[4] = static_cast<float>(log1p(visited));
+    for (int k = 0; k < 8; ++k) x[5 + k] = st[k];
+    x[13] = static_cast<float>(d) / 64.0f;
+    x[14] = static_cast<float>(visited / orbit);
+    x[15] = static_cast<float>(log1p(g * last[0]));
+    __nv_bfloat16 xs[kRolloutInputs], h1[kHidden];
+    for (uint32_t i = 0; i < kRolloutInputs; ++i) xs[i] = __float2bfloat16((x[i] - x_mean[i]) / x_scale[i]);
+    for (uint32_t k = 0; k < kHidden; ++k) {
+      float a = __bfloat162float(Q[o.b1 + k]);
+      for (uint32_t i = 0; i < kRolloutInputs; ++i)
+        a = fmaf(__bfloat162float(Q[o.w1 + k * kRolloutInputs + i]), __bfloat162float(xs[i]), a);
+      h1[k] = __float2bfloat16(fmaxf(a, 0.f));
+    }
+    float y0 = __bfloat162float(Q[o.b3]);
+    for (uint32_t j = 0; j < kHidden; ++j) {
+      float a = __bfloat162float(Q[o.b2 + j]);
+      const __nv_bfloat162* row = reinterpret_cast<const __nv_bfloat162*>(Q + o.w2 + j * kHidden);
+      for (uint32_t k = 0; k < kHidden; k += 2) {
+        const float2 w = __bfloat1622float2(row[k / 2]);
+        a = fmaf(w.x, __bfloat162float(h1[k]), a);
+        a = fmaf(w.y, __bfloat162float(h1[k + 1]), a);
+      }
+      y0 = fmaf(__bfloat162float(Q[o.w3 + j]), __bfloat162float(__float2bfloat16(fmaxf(a, 0.f))), y0);
+    }
+    double nxt = expm1(static_cast<double>(y0) + log1p(last[0]));
+    nxt = fmin(nxt, fmin(orbit - visited, g * last[0]));
+    if (!(nxt >= 0.5)) break;
+    last[3] = last[2];
+    last[2] = last[1];
+    last[1] = last[0];
+    last[0] = nxt;
+    visited += nxt;
+    sum += nxt;
+    best = fmax(best, nxt);
+  }
+  peak[m] = best;
+  total[m] = sum;
+  depth[m] = d + 1;
+}
+
 uint32_t mlp_grid(unsigned long long batch) {
   return static_cast<uint32_t>(std::max<unsigned long long>(1, std::min<unsigned long long>((batch + kMlpBlock - 1) / kMlpBlock, 148ull * 4)));
 }
@@ -237,6 +305,19 @@ int mgbfs2_mlp_infer_bf16(uint32_t inputs, const void* params_bf16, const float*
   const size_t smem = offsets(inputs).total * sizeof(__nv_bfloat16);
   mlp_infer_bf16_kernel<<<mlp_grid(batch), kMlpBlock, smem, static_cast<cudaStream_t>(stream)>>>(
       inputs, static_cast<const __nv_bfloat16*>(params_bf16), x, batch, y);
+  return cuda_status(cudaGetLastError());
+}
+
+int mgbfs2_mlp_rollout_bf16(const void* params_bf16, const float* x_mean, const float* x_scale, const float* statics,
+                            const float* gens, uint32_t count, uint32_t max_depth, double* peak, double* total,
+                            uint32_t* depth, void* stream) {
+  if (!params_bf16 || !x_mean || !x_scale || (count && (!statics || !gens || !peak || !total || !depth)))
+    return MGBFS2_INVALID_ARGUMENT;
+  if (!count) return MGBFS2_OK;
+  const size_t smem = offsets(kRolloutInputs).total * sizeof(__nv_bfloat16);
+  mlp_rollout_kernel<<<(count + kMlpBlock - 1) / kMlpBlock, kMlpBlock, smem, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const __nv_bfloat16*>(params_bf16), x_mean, x_scale, statics, gens, count, max_depth, peak, total,
+      depth);
   return cuda_status(cudaGetLastError());
 }
 

@@ -146,6 +146,8 @@ _SIGNATURES = {
                                   C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
     "mgbfs2_mlp_to_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mgbfs2_mlp_infer_bf16": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "mgbfs2_mlp_rollout_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                          C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mgbfs2_group_order": (C.c_int, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
 }
 

@@ -88,7 +88,13 @@ def graph_statics(generators, start) -> GraphStatics:
         fixed.append(sum(1 for length in c if length == 1) / n)
         cycles.append(len(c) / n)
     gens = {tuple(g) for g in generators}
-    closed = all(tuple(np.argsort(g).tolist()) in gens for g in generators)
+
+    def inverse(g):
+        inv = [0] * len(g)
+        for i, x in enumerate(g):
+            inv[x] = i
+        return tuple(inv)
+    closed = all(inverse(g) in gens for g in generators)
     counts = {}
     for v in start:
         counts[v] = counts.get(v, 0) + 1
@@ -97,8 +103,8 @@ def graph_statics(generators, start) -> GraphStatics:
         log_orbit = math.log(group_order(generators))
     else:
         log_orbit = math.lgamma(n + 1) - sum(math.lgamma(c + 1) for c in counts.values())
-    return GraphStatics(n, len(generators), closed, log_orbit, float(np.mean(orders)), float(max(orders)),
-                        float(np.mean(fixed)), float(np.mean(cycles)))
+    k = len(generators)
+    return GraphStatics(n, k, closed, log_orbit, sum(orders) / k, max(orders), sum(fixed) / k, sum(cycles) / k)
 
 
 def features(st: GraphStatics, layers, d) -> list:
@@ -266,23 +272,48 @@ def rollout(net: PlannerNet, graphs, max_depth=512):
     return layers
 
 
+def rollout_device(net: PlannerNet, graphs, max_depth=512):
+    """(peak, total, depth) of every graph's predicted profile, from one
+    launch of the device rollout kernel (mgbfs2_mlp_rollout_bf16): the same
+    features and bf16 network as `rollout`, with the depth loop on the GPU, so
+    predicting a whole sweep costs one launch instead of one per depth."""
+    t = net.torch
+    stats = [graph_statics(g["action"]["generators"], g["start"]) for g in graphs]
+    m = len(stats)
+    static = t.tensor([[st.log_orbit, st.n / 16.0, st.gens / 8.0, float(st.inverse_closed), st.mean_log_order,
+                        st.max_log_order, st.fixed_fraction, st.cycle_fraction] for st in stats],
+                      dtype=t.float32, device=net.dev).reshape(m, 8).contiguous()
+    gens = t.tensor([float(st.gens) for st in stats], dtype=t.float32, device=net.dev)
+    mean = t.tensor(net.x_mean, dtype=t.float32, device=net.dev)
+    scale = t.tensor(net.x_scale, dtype=t.float32, device=net.dev)
+    q = t.empty(net.count, dtype=t.bfloat16, device=net.dev)
+    native.check(net.lib.mgbfs2_mlp_to_bf16(net.count, net.params.data_ptr(), q.data_ptr(), net._stream()),
+                 "mgbfs2_mlp_to_bf16")
+    peak = t.empty(m, dtype=t.float64, device=net.dev)
+    total = t.empty(m, dtype=t.float64, device=net.dev)
+    depth = t.empty(m, dtype=t.int32, device=net.dev)
+    native.check(net.lib.mgbfs2_mlp_rollout_bf16(q.data_ptr(), mean.data_ptr(), scale.data_ptr(), static.data_ptr(),
+                                                 gens.data_ptr(), m, max_depth, peak.data_ptr(), total.data_ptr(),
+                                                 depth.data_ptr(), net._stream()), "mgbfs2_mlp_rollout_bf16")
+    return peak.cpu().numpy(), total.cpu().numpy(), depth.cpu().numpy()
+
+
 def predicted_capacities(net: PlannerNet, graphs, margin=1.5, floor=4096):
-    """Per-instance frontier capacity for the batched sweep, never above the
-    exact state count |G| (the sweep's instances have distinct labels), which
-    no layer can exceed."""
-    caps = []
-    for g, prof in zip(graphs, rollout(net, graphs)):
-        orbit = group_order(g["action"]["generators"])
-        caps.append(int(min(orbit, max(prof) * margin + floor)))
-    return caps
+    """Per-instance frontier capacity for the batched sweep (predicted peak x
+    margin + floor, from the device rollout), never above the exact state count
+    |G| (the sweep's instances have distinct labels), which no layer can
+    exceed."""
+    peaks, _, _ = rollout_device(net, graphs)
+    return [int(min(group_order(g["action"]["generators"]), peak * margin + floor))
+            for g, peak in zip(graphs, peaks)]
 
 
 def calibrate_margin(net: PlannerNet, graphs, tables, quantile=0.97, slack=1.1) -> float:
     """Capacity margin from complete layer tables the network was not fitted
     on: the `quantile` of (true peak / predicted peak), at least 1, times
     `slack`.  A larger margin trades memory for fewer exact reruns."""
-    prof = rollout(net, graphs)
-    ratios = sorted(max(t) / max(1.0, max(p)) for t, p in zip(tables, prof))
+    peaks, _, _ = rollout_device(net, graphs)
+    ratios = sorted(max(t) / max(1.0, p) for t, p in zip(tables, peaks))
     q = ratios[min(len(ratios) - 1, int(quantile * (len(ratios) - 1) + 0.5))]
     return max(1.0, q) * slack
 

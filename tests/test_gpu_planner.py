@@ -58,6 +58,15 @@ def test_training_reduces_loss_and_predicts_layers():
     prof = rollout(net, graphs)
     ratios = [max(p) / max(t) for p, t in zip(prof, tables)]
     assert np.median([abs(math.log(r)) for r in ratios]) < math.log(4)
+    # The one-launch device rollout follows the host-stepped rollout (same
+    # features, same bf16 kernel arithmetic; the orbit reaches the device as
+    # fp32, so the last layer's clamp may differ by rounding).
+    from multigpubfs_b200.planner import rollout_device
+    peak, total, depth = rollout_device(net, graphs)
+    for p, pk, tt, dp in zip(prof, peak, total, depth):
+        assert abs(pk - max(p)) <= 1e-3 * max(p)
+        assert abs(tt - sum(p)) <= 1e-3 * sum(p)
+        assert abs(int(dp) - len(p)) <= 1
 
 
 def test_learned_capacities_never_change_results():
