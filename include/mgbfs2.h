@@ -84,6 +84,11 @@ typedef struct {
  * that produced it and skip that generator's inverse (the edge back to the
  * previous layer) without a visited test; this option turns that off. */
 #define MGBFS2_OPTION_NO_PARENT_SKIP 1u
+/* Plans whose frontier buffers and visited set are sized up front (the fused
+ * bitmap or all-visited hash layers, no limits or callback) run the whole BFS
+ * as ONE CUDA graph whose WHILE node repeats {expand layer, finalize} on the
+ * device; this option keeps the host-driven layer loop instead. */
+#define MGBFS2_OPTION_HOST_LOOP 2u
 
 typedef struct {
   uint32_t visited, dedup;

@@ -123,7 +123,8 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
   rc = cuda_status(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
   if (rc) { set_message(error, cap, "CUDA_STREAM"); delete g; return rc; }
   for (DeviceBuffer* b : {&g->bitmap, &g->front, &g->next, &g->table, &g->bank[0], &g->bank[1], &g->bank[2],
-                          &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta, &g->group_meta})
+                          &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta, &g->group_meta,
+                          &g->loop_buf})
     b->stream = g->stream;
   retain_pool_memory(dev);
   for (cudaEvent_t* e : {&g->ev_run[0], &g->ev_run[1], &g->ev_kernel[0], &g->ev_kernel[1]}) {
@@ -379,6 +380,7 @@ void Graph::release() {
     host_meta = nullptr;
   }
   group_meta.free();
+  loop_buf.free();
   if (host_group) {
     cudaFreeHost(host_group);
     host_group = nullptr;
@@ -536,6 +538,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   p.visited = visited;
   p.dedup = dedup;
   parent_skip = packed && gen_shift && !(r.options & MGBFS2_OPTION_NO_PARENT_SKIP);
+  host_loop_only = (r.options & MGBFS2_OPTION_HOST_LOOP) != 0;
   p.parent_skip = parent_skip;
   p.bucket_prefix = bucket_prefix;
   p.history_layers = visited == MGBFS2_VISITED_HASH3 ? 3 : 1;
@@ -957,6 +960,125 @@ uint64_t Graph::next_bound(uint32_t depth, uint64_t count, uint64_t visited) con
   return b;
 }
 
+// Graph mode: the layer loop as ONE CUDA graph.  A conditional WHILE node
+// repeats {expand the frontier, loop_finalize}; loop_finalize records the new
+// layer's size and a globaltimer stamp, swaps the buffers and clears the loop
+// condition when the frontier is exhausted, on a device error, or when the
+// layer table is full (then the host loop takes over from the device state).
+// Frontier buffers (`front`, `next`) already hold `cap` states each.
+int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64_t cap, mgbfs2_status* st,
+                           double* kernel_seconds, uint64_t* count, uint64_t* visited, uint32_t* depth,
+                           bool* paused) {
+  constexpr uint32_t kEntries = 4096;
+  const size_t head = (sizeof(LoopState) + 255) / 256 * 256;
+  int rc = loop_buf.ensure(head + 2 * kEntries * sizeof(unsigned long long));
+  if (rc) return rc;
+  char* base = static_cast<char*>(loop_buf.ptr);
+  LoopState* ls = reinterpret_cast<LoopState*>(base);
+  unsigned long long* layers = reinterpret_cast<unsigned long long*>(base + head);
+  unsigned long long* stamps = layers + kEntries;
+  LoopState h{};
+  h.count = 1;
+  h.visited = 1;
+  h.capacity = cap;
+  h.buf[0] = static_cast<unsigned long long*>(front.ptr);
+  h.buf[1] = static_cast<unsigned long long*>(next.ptr);
+  h.max_entries = kEntries;
+  MG_CHECK(cudaMemcpyAsync(ls, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
+  ExpandParams p = *pp;
+  p.loop = ls;
+  p.capacity = cap;
+  const uint32_t grid = grid_for(fn, smem, UINT32_MAX);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  };
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  cudaGraphConditionalHandle handle{};
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(cap_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    reinterpret_cast<void (*)(ExpandParams)>(const_cast<void*>(fn))<<<grid, kBlock, smem, cap_stream>>>(p);
+    loop_finalize<<<1, 1, 0, cap_stream>>>(ls, p.control, layers, stamps, handle);
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamEndCapture(cap_stream, &body);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_kernel[0], stream);
+  if (e == cudaSuccess) {
+    loop_start<<<1, 1, 0, stream>>>(stamps);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_kernel[1], stream);
+  LoopState out{};
+  std::vector<unsigned long long> sizes(kEntries), times(kEntries);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&out, ls, sizeof(out), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host_control, control_buf.ptr, sizeof(Control), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sizes.data(), layers, kEntries * 8, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(times.data(), stamps, kEntries * 8, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  cleanup();
+  if (e != cudaSuccess) return cuda_status(e);
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ev_kernel[0], ev_kernel[1]) == cudaSuccess) *kernel_seconds += ms * 1e-3;
+  // Layers 1..out.depth were recorded; layers 0..out.depth were expanded
+  // unless the table filled up (then layer out.depth is still to expand).
+  const uint32_t D = out.depth;
+  const uint32_t expanded = out.stop == 3 ? D : D + 1;
+  for (uint32_t d = 1; d <= D; ++d) {
+    layer_sizes.push_back(sizes[d]);
+    layer_seconds.push_back(static_cast<double>(times[d] - times[d - 1]) * 1e-9);
+  }
+  for (uint32_t d = 0; d < expanded; ++d) {
+    const uint64_t c = d ? sizes[d] : 1;
+    st->successors += c * gens;
+    st->visited_tests += c * gens - (parent_skip && d > 0 ? c : 0);
+  }
+  launches += 1 + 2 * expanded;
+  if (out.parity) std::swap(front, next);
+  *count = D ? sizes[D] : 1;
+  *visited = out.visited;
+  *depth = D;
+  *paused = out.stop == 3;
+  if (out.stop == 2) {
+    st->reason = MGBFS2_REASON_RESOURCE;
+    st->fatal = host_control->error ? host_control->error : ERR_FRONTIER_OVERFLOW;
+    return MGBFS2_OK;
+  }
+  if (out.stop == 1) st->complete = 1;
+  // The deepest layer sits in `front`; the layer before it is intact in `next`
+  // (the last expansion appended nothing, or the loop paused before it).
+  if (D >= 2 && sizes[D - 1] < 1000) {
+    std::vector<uint64_t> words(sizes[D - 1]);
+    MG_CHECK(cudaMemcpyAsync(words.data(), next.ptr, words.size() * 8, cudaMemcpyDeviceToHost, stream));
+    MG_CHECK(cudaStreamSynchronize(stream));
+    keep_small(D - 1, std::move(words));
+  }
+  if (D >= 1 && sizes[D] < 1000) {
+    std::vector<uint64_t> words(sizes[D]);
+    MG_CHECK(cudaMemcpyAsync(words.data(), front.ptr, words.size() * 8, cudaMemcpyDeviceToHost, stream));
+    MG_CHECK(cudaStreamSynchronize(stream));
+    keep_small(D, std::move(words));
+  }
+  return MGBFS2_OK;
+}
+
 int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status) {
   if (!planned) return MGBFS2_STATE;
   MG_CHECK(cudaSetDevice(device));
@@ -1024,6 +1146,19 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     if ((rc = bank[0].ensure(bank_slots[0] * 8))) return rc;
     MG_CHECK(cudaMemsetAsync(bank[0].ptr, 0xff, bank_slots[0] * 8, stream));
   }
+  // Graph mode: the fused bitmap or all-visited hash layers with buffers sized
+  // up front (frontier capacity for every layer, hash table for every state),
+  // no limits and no callback.
+  const bool limited = limits && (limits->max_seconds > 0 || limits->max_layers || limits->cancel);
+  const uint64_t loop_cap = std::max<uint64_t>(1, plan.capacity);
+  bool device_loop = !host_loop_only && !bucketed && !grouped_mode && !sorted && !limited && !cb &&
+                     (visit == V_LEHMER || visit == V_MULTISET || visit == V_HASH) &&
+                     2 * (loop_cap + 2) * 8 <= (16ull << 30);
+  if (device_loop && visit == V_HASH) device_loop = state_bound && plan.table_slots >= 2 * state_bound;
+  if (device_loop) {
+    if ((rc = front.ensure((loop_cap + 2) * 8))) return rc;
+    if ((rc = next.ensure((loop_cap + 2) * 8))) return rc;
+  }
   if ((rc = front.ensure(16))) return rc;
   MG_CHECK(cudaMemcpyAsync(front.ptr, &start_word, 8, cudaMemcpyHostToDevice, stream));
   {
@@ -1047,7 +1182,21 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   }
   uint64_t peak = plan.device_bytes;
   st.reason = MGBFS2_REASON_FRONTIER_EXHAUSTED;
-  for (;;) {
+  bool finished = false;
+  if (device_loop) {
+    if (visit == V_HASH) {
+      p.table = static_cast<unsigned long long*>(table.ptr);
+      p.table_mask = table_slots - 1;
+      p.tag = 0;
+    }
+    p.probe_limit = 1u << 20;
+    bool paused = false;
+    rc = run_device_loop(reinterpret_cast<const void*>(fn), &p, smem, loop_cap, &st, &kernel_seconds, &count,
+                         &visited, &depth, &paused);
+    finished = rc != MGBFS2_OK || !paused;
+    peak = std::max<uint64_t>(peak, bitmap.bytes + front.bytes + next.bytes + table.bytes);
+  }
+  for (; !finished;) {
     const double elapsed = std::chrono::duration<double>(Clock::now() - started).count();
     if (limits && limits->cancel && *limits->cancel) { st.reason = MGBFS2_REASON_CANCELLED; break; }
     if (limits && limits->max_seconds > 0 && elapsed >= limits->max_seconds) { st.reason = MGBFS2_REASON_DEADLINE; break; }

@@ -90,6 +90,13 @@ struct Graph {
   int grouped_finish();   // after the layer: per-region counts of `next` into next_begin/next_cap layout
   int gather_front(uint64_t count);  // grouped `front` -> contiguous
 
+  // Graph mode of the fused path: one CUDA graph whose WHILE node repeats
+  // {expand, loop_finalize} with the layer loop state on the device.
+  DeviceBuffer loop_buf;
+  bool host_loop_only = false;  // plan option MGBFS2_OPTION_HOST_LOOP
+  int run_device_loop(const void* fn, ExpandParams* p, size_t smem, uint64_t cap, mgbfs2_status* st,
+                      double* kernel_seconds, uint64_t* count, uint64_t* visited, uint32_t* depth, bool* paused);
+
   // Results.
   std::vector<uint64_t> layer_sizes;
   std::vector<double> layer_seconds;

@@ -18,6 +18,15 @@ enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3 };
 constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
 constexpr uint32_t kBlock = 256;
 
+// Device-resident layer loop (graph mode): the frontier size, which of the
+// two buffers holds it, and the loop's stop reason live on the device, so one
+// CUDA graph with a WHILE node runs a whole BFS without host round trips.
+struct LoopState {
+  unsigned long long count, visited, capacity;
+  unsigned long long* buf[2];
+  uint32_t parity, depth, max_entries, stop;  // stop: 0 running, 1 exhausted, 2 error, 3 table full of layers
+};
+
 struct ExpandParams {
   const unsigned long long* frontier;
   unsigned long long count;
@@ -41,6 +50,7 @@ struct ExpandParams {
   unsigned long long look0_mask;
   const unsigned long long* look1;
   unsigned long long look1_mask;
+  LoopState* loop;  // graph mode: count and buffers from here instead of frontier/count/next
 };
 
 // Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the
@@ -102,8 +112,8 @@ __device__ __forceinline__ bool claim(const ExpandParams& p, uint64_t c, bool va
 
 // Append the block's shared-memory winners to the next frontier with one
 // global reservation.  Called by all threads of the block.
-__device__ __forceinline__ void flush_block(const ExpandParams& p, unsigned long long* out, uint32_t* out_count,
-                                            unsigned long long* out_base) {
+__device__ __forceinline__ void flush_block(const ExpandParams& p, unsigned long long* next, unsigned long long* out,
+                                            uint32_t* out_count, unsigned long long* out_base) {
   __syncthreads();
   const uint32_t n = *out_count;
   if (threadIdx.x == 0 && n) *out_base = atomicAdd(&p.control->next_count, static_cast<unsigned long long>(n));
@@ -112,7 +122,7 @@ __device__ __forceinline__ void flush_block(const ExpandParams& p, unsigned long
   bool overflow = false;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
     const unsigned long long pos = base + i;
-    if (pos < p.capacity) p.next[pos] = out[i];
+    if (pos < p.capacity) next[pos] = out[i];
     else overflow = true;
   }
   if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
@@ -135,9 +145,18 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
   if (threadIdx.x == 0) out_count = 0;
   __syncthreads();
 
+  unsigned long long count = p.count;
+  const unsigned long long* frontier = p.frontier;
+  unsigned long long* next = p.next;
+  if (p.loop) {
+    count = p.loop->count;
+    const uint32_t parity = p.loop->parity;
+    frontier = p.loop->buf[parity];
+    next = p.loop->buf[parity ^ 1u];
+  }
   const uint32_t lane = lane_id();
   const uint32_t tile = blockDim.x * p.ppt;
-  const unsigned long long tiles = (p.count + tile - 1) / tile;
+  const unsigned long long tiles = (count + tile - 1) / tile;
   for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
     const unsigned long long base = t * tile;
     uint64_t par[4];
@@ -148,13 +167,13 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
       val[2 * j] = val[2 * j + 1] = false;
       if (2 * j < static_cast<int>(p.ppt)) {
         const unsigned long long i0 = base + 2ull * (j * blockDim.x + threadIdx.x);
-        if (i0 + 1 < p.count) {
-          const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p.frontier + i0);
+        if (i0 + 1 < count) {
+          const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(frontier + i0);
           par[2 * j] = v.x;
           par[2 * j + 1] = v.y;
           val[2 * j] = val[2 * j + 1] = true;
-        } else if (i0 < p.count) {
-          par[2 * j] = p.frontier[i0];
+        } else if (i0 < count) {
+          par[2 * j] = frontier[i0];
           val[2 * j] = true;
         }
       }
@@ -187,10 +206,10 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
         __syncthreads();
         const uint32_t pending = out_count;
         __syncthreads();
-        if (pending + tile > kOutCap) flush_block(p, out, &out_count, &out_base);
+        if (pending + tile > kOutCap) flush_block(p, next, out, &out_count, &out_base);
       }
     }
-    flush_block(p, out, &out_count, &out_base);
+    flush_block(p, next, out, &out_count, &out_base);
   }
 }
 
@@ -260,6 +279,41 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
     if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
     __syncthreads();
   }
+}
+
+// Graph mode, after each expansion: record the new layer, stop on an empty
+// layer, a device error or a full layer table, else make the new layer the
+// frontier; the WHILE node repeats while `stop` is 0.  layers/stamps hold
+// max_entries sizes and globaltimer readings (stamp d = end of layer d).
+static __global__ void loop_finalize(LoopState* s, Control* c, unsigned long long* layers, unsigned long long* stamps,
+                                     cudaGraphConditionalHandle handle) {
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  const unsigned long long produced = c->next_count;
+  uint32_t stop = 0;
+  if (c->error || produced > s->capacity) {
+    stop = 2;
+  } else if (produced == 0) {
+    stop = 1;
+  } else {
+    const uint32_t d = s->depth + 1;
+    layers[d] = produced;
+    stamps[d] = now;
+    s->count = produced;
+    s->visited += produced;
+    s->parity ^= 1u;
+    s->depth = d;
+    c->next_count = 0;
+    if (d + 1 >= s->max_entries) stop = 3;
+  }
+  s->stop = stop;
+  cudaGraphSetConditional(handle, stop ? 0u : 1u);
+}
+
+static __global__ void loop_start(unsigned long long* stamps) {
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  stamps[0] = now;
 }
 
 // Marks the start state visited (and, for the hash paths, inserts it).

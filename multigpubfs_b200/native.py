@@ -54,6 +54,7 @@ class PlanRequest(C.Structure):
 
 
 OPTION_NO_PARENT_SKIP = 1
+OPTION_HOST_LOOP = 2
 
 
 class PlanInfo(C.Structure):

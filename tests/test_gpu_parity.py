@@ -59,6 +59,9 @@ VARIANTS = {
     # no group margin: most winners of the first grouped layers go to the spill region
     "bitmap_grouped_tight": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, bucket_margin=0),
     "bitmap_grouped_noskip": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, parent_skip=False),
+    # host-driven layer loop instead of the one-graph device loop
+    "bitmap_atomic_hostloop": dict(visited="bitmap", dedup="atomic", host_loop=True),
+    "hash_hostloop": dict(visited="hash", host_loop=True),
 }
 
 
@@ -98,6 +101,23 @@ def test_golden_cases(exact_cases, variant):
         assert r.successors == sum(sizes) * len(case["graph"]["action"]["generators"])
         ran += 1
     assert ran >= 8
+
+
+@pytest.mark.parametrize("plan", [dict(visited="bitmap", dedup="atomic"), dict(visited="hash")])
+def test_device_loop_matches_host_loop(lrx_layers, plan):
+    """The one-graph device loop and the host loop give the same table, edge
+    counts and samples; the device loop launches two kernels per layer (expand,
+    finalize) plus the seed and the start stamp, the host loop one per layer."""
+    g = G.permutation_graph(G.lrx_generators(10), list(range(10)))
+    info, dev, last_d, prev_d = run(g, **plan)
+    info_h, host, last_h, prev_h = run(g, **plan, host_loop=True)
+    assert dev.layer_sizes == host.layer_sizes == lrx_layers[10]
+    assert dev.successors == host.successors and dev.visited_tests == host.visited_tests
+    assert last_d == last_h and prev_d == prev_h
+    layers = len(lrx_layers[10])
+    assert host.kernel_launches == 1 + layers
+    assert dev.kernel_launches == 2 + 2 * layers
+    assert len(dev.layer_seconds) == layers - 1 and all(t >= 0 for t in dev.layer_seconds)
 
 
 def test_parent_skip_accounting(lrx_layers):
