@@ -64,8 +64,8 @@ WORKLOADS = {
                     desc="S13 LRX full BFS (L, R, X from identity; 6,227,020,800 states), exact Lehmer-rank bitmap"),
     "s13-coxeter": dict(n=13, gens=coxeter(13), visited="bitmap", dedup="grouped",
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
-    "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash3", dedup="atomic",
-                         desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash, 3 layer banks"),
+    "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
+                         desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
 }
 
 
