@@ -89,6 +89,10 @@ typedef struct {
  * as ONE CUDA graph whose WHILE node repeats {expand layer, finalize} on the
  * device; this option keeps the host-driven layer loop instead. */
 #define MGBFS2_OPTION_HOST_LOOP 2u
+/* Grouped layers over adjacent-transposition generators derive each child's
+ * rank from its parent's Lehmer digits (two digits change); this option makes
+ * them rank every child from scratch instead. */
+#define MGBFS2_OPTION_FULL_RANK 4u
 
 typedef struct {
   uint32_t visited, dedup;

@@ -106,6 +106,28 @@ __device__ __forceinline__ void lehmer_split4(uint64_t w, uint32_t* group, uint3
   *inner = tail;
 }
 
+// lehmer_split4<N, K> that also returns every Lehmer digit, 4 bits each
+// (digit i in bits [4i, 4i+4); the last digit is always 0 and left out).
+template <int N, int K>
+__device__ __forceinline__ void lehmer_digits_split4(uint64_t w, uint64_t* digits, uint32_t* group, uint32_t* inner) {
+  static_assert(N - K <= 12, "in-group rank must fit 32 bits");
+  const uint32_t lo_word = static_cast<uint32_t>(w), hi_word = static_cast<uint32_t>(w >> 32);
+  uint32_t used = 0, head = 0, tail = 0, dlo = 0, dhi = 0;
+#pragma unroll
+  for (int i = 0; i < N - 1; ++i) {
+    const uint32_t s = (i < 8 ? (lo_word >> (4 * i)) : (hi_word >> (4 * (i - 8)))) & 15u;
+    const uint32_t c = s - __popc(used & ((1u << s) - 1u));
+    used |= 1u << s;
+    if (i < 8) dlo |= c << (4 * i);
+    else dhi |= c << (4 * (i - 8));
+    if (i < K) head = head * static_cast<uint32_t>(N - i) + c;
+    else tail = tail * static_cast<uint32_t>(N - i) + c;
+  }
+  *digits = (static_cast<uint64_t>(dhi) << 32) | dlo;
+  *group = head;
+  *inner = tail;
+}
+
 // Inverse of lehmer_rank4<N>: factorial-base digits (mixed radix, least
 // significant first, all divisors compile-time constants), then the c_i-th
 // unused symbol of a sorted nibble list for every position.

@@ -124,7 +124,7 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
   if (rc) { set_message(error, cap, "CUDA_STREAM"); delete g; return rc; }
   for (DeviceBuffer* b : {&g->bitmap, &g->front, &g->next, &g->table, &g->bank[0], &g->bank[1], &g->bank[2],
                           &g->program, &g->control_buf, &g->scratch, &g->buckets, &g->shard_meta, &g->group_meta,
-                          &g->loop_buf})
+                          &g->loop_buf, &g->transp_buf})
     b->stream = g->stream;
   retain_pool_memory(dev);
   for (cudaEvent_t* e : {&g->ev_run[0], &g->ev_run[1], &g->ev_kernel[0], &g->ev_kernel[1]}) {
@@ -381,6 +381,7 @@ void Graph::release() {
   }
   group_meta.free();
   loop_buf.free();
+  transp_buf.free();
   if (host_group) {
     cudaFreeHost(host_group);
     host_group = nullptr;
@@ -530,6 +531,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     group_prefix = K;
     groups = static_cast<uint32_t>(fact[n] / fact[n - K]);
     plan_group_order();
+    if (int rc = plan_transpositions(!(r.options & MGBFS2_OPTION_FULL_RANK))) return rc;
     bucket_prefix = K;
     p.shards = groups;
     bucket_margin = r.bucket_margin == 0 ? 1024 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
@@ -661,13 +663,30 @@ static GroupedFn pick_grouped(uint32_t n, uint32_t prefix) {
   switch (n) {
 #define MG_CASE(K)                                                                               \
   case K:                                                                                        \
-    return prefix == 1 ? expand_grouped<K, 1> : (prefix == 2 ? expand_grouped<K, 2> : expand_grouped<K, 3>);
+    return prefix == 1 ? expand_grouped<K, 1, false>                                             \
+                       : (prefix == 2 ? expand_grouped<K, 2, false> : expand_grouped<K, 3, false>);
     MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10) MG_CASE(11) MG_CASE(12)
     MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
 #undef MG_CASE
     case 2:
     case 3:
-      return prefix == 1 ? (n == 2 ? expand_grouped<2, 1> : expand_grouped<3, 1>) : nullptr;
+      return prefix == 1 ? (n == 2 ? expand_grouped<2, 1, false> : expand_grouped<3, 1, false>) : nullptr;
+    default:
+      return nullptr;
+  }
+}
+
+// The incremental-rank instantiations: adjacent-transposition generators and a
+// 32-bit in-group rank (8 <= N - K <= 12).
+static GroupedFn pick_grouped_transp(uint32_t n, uint32_t prefix) {
+  switch (n * 4 + prefix) {
+#define MG_CASE(N, K) \
+  case N * 4 + K:     \
+    return expand_grouped<N, K, true>;
+    MG_CASE(9, 1) MG_CASE(10, 1) MG_CASE(11, 1) MG_CASE(12, 1) MG_CASE(13, 1)
+    MG_CASE(10, 2) MG_CASE(11, 2) MG_CASE(12, 2) MG_CASE(13, 2) MG_CASE(14, 2)
+    MG_CASE(11, 3) MG_CASE(12, 3) MG_CASE(13, 3) MG_CASE(14, 3) MG_CASE(15, 3)
+#undef MG_CASE
     default:
       return nullptr;
   }
@@ -728,6 +747,48 @@ void Graph::plan_group_order() {
     ++c;
     ++depth;
   }
+}
+
+// Adjacent-transposition generators (g swaps positions t-1 and t): the
+// incremental-rank form of the grouped layers needs, per generator, t and the
+// weights of Lehmer digits t-1 and t in the group number (the first K digits,
+// mixed radix N, N-1, ...) and in the in-group rank (the other digits,
+// weight (N-1-j)!).
+int Graph::plan_transpositions(bool allowed) {
+  const uint32_t n = elements, K = group_prefix;
+  group_transp = false;
+  if (!allowed || gens > kMaxTranspGens || !pick_grouped_transp(n, K)) return MGBFS2_OK;
+  std::vector<uint32_t> info;
+  auto wg = [&](uint32_t j) {
+    if (j >= K) return 0u;
+    uint32_t w = 1;
+    for (uint32_t k = j + 1; k < K; ++k) w *= n - k;
+    return w;
+  };
+  auto wi = [&](uint32_t j) {
+    if (j < K) return 0u;
+    uint32_t w = 1;
+    for (uint32_t k = 2; k <= n - 1 - j; ++k) w *= k;
+    return w;
+  };
+  for (uint32_t k = 0; k < gens; ++k) {
+    const uint32_t* g = perms.data() + static_cast<size_t>(k) * n;
+    uint32_t moved = 0, t = 0;
+    for (uint32_t i = 0; i < n; ++i)
+      if (g[i] != i) {
+        ++moved;
+        t = i;  // the larger moved position
+      }
+    if (moved != 2 || t == 0 || g[t] != t - 1 || g[t - 1] != t) return MGBFS2_OK;
+    info.insert(info.end(), {t, wg(t - 1), wg(t), wi(t - 1), wi(t)});
+  }
+  int rc = transp_buf.ensure(info.size() * sizeof(uint32_t));
+  if (rc) return rc;
+  MG_CHECK(cudaMemcpyAsync(transp_buf.ptr, info.data(), info.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           stream));
+  MG_CHECK(cudaStreamSynchronize(stream));
+  group_transp = true;
+  return MGBFS2_OK;
 }
 
 // Meta layout of a grouped layer (R = groups + 1 regions, the spill last), in
@@ -795,7 +856,7 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   ncount[R] = 0;  // work counter
   if ((rc = next.ensure((total + 2) * sizeof(unsigned long long)))) return rc;
   MG_CHECK(cudaMemcpyAsync(group_meta.ptr, host_group, bytes, cudaMemcpyHostToDevice, stream));
-  GroupedFn f = pick_grouped(elements, group_prefix);
+  GroupedFn f = group_transp ? pick_grouped_transp(elements, group_prefix) : pick_grouped(elements, group_prefix);
   if (!f) return MGBFS2_UNSUPPORTED;
   *fn = reinterpret_cast<void*>(f);
   *smem_total = sizeof(GroupedSmem) + smem;
@@ -1297,6 +1358,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         gp.next_count = meta + 5 * R + 1;
         gp.work = meta + 6 * R + 1;
         gp.control = p.control;
+        gp.transp = static_cast<const uint32_t*>(transp_buf.ptr);
         reinterpret_cast<GroupedFn>(group_fn)<<<grid_for(group_fn, group_smem, group_items), kBlock, group_smem,
                                                  stream>>>(gp);
         ++launches;

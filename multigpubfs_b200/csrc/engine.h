@@ -84,6 +84,9 @@ struct Graph {
   bool front_grouped = false;
   std::vector<uint64_t> front_begin, front_count, next_begin, next_cap;
   std::vector<uint32_t> group_order;  // visiting order of the groups (work items follow it)
+  bool group_transp = false;          // every generator swaps two adjacent positions: incremental ranks
+  DeviceBuffer transp_buf;            // per generator: t, wg(t-1), wg(t), wi(t-1), wi(t)
+  int plan_transpositions(bool allowed);
   void plan_group_order();
   int grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total, size_t smem,
                     uint64_t* items);

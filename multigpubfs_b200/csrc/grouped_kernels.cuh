@@ -38,6 +38,7 @@ namespace mgbfs2 {
 constexpr uint32_t kGroupStage = 2048;  // staged winners per block (4 blocks per SM fit)
 constexpr uint32_t kMaxGroups = 1728;   // 13!/10! = 1716 groups at most
 constexpr uint32_t kGroupChunk = 4096;  // parents per work item
+constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
 
 constexpr uint64_t factorial_u64(int m) { return m <= 1 ? 1ull : static_cast<uint64_t>(m) * factorial_u64(m - 1); }
 
@@ -59,6 +60,10 @@ struct GroupedParams {
   unsigned long long* next_count;        // regions: winners reserved per region (may pass a group's cap)
   unsigned long long* work;              // work-item counter, zero at launch
   Control* control;
+  // Incremental-rank path (every generator swaps positions t-1 and t): per
+  // generator t and the weights of digits t-1 and t in the group part and in
+  // the in-group rank (0 where the position lies in the other part).
+  const uint32_t* transp;                // gens x 5: t, wg(t-1), wg(t), wi(t-1), wi(t)
 };
 
 struct GroupedSmem {
@@ -69,6 +74,7 @@ struct GroupedSmem {
   uint32_t hist[kMaxGroups];   // staged winners per group
   uint32_t gbase[kMaxGroups];  // reserved position of the block's run in each group (saturated at 2^32 - 1)
   uint16_t touched[kMaxGroups];  // the groups with staged winners, in first-touch order
+  uint32_t transp[kMaxTranspGens * 5];
   unsigned long long item;
   uint32_t count, ntouched;
 };
@@ -109,7 +115,7 @@ __device__ __forceinline__ void grouped_flush(const GroupedParams& p, GroupedSme
   __syncthreads();
 }
 
-template <int N, int K>
+template <int N, int K, bool TRANSP>
 __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   GroupedSmem& sm = *reinterpret_cast<GroupedSmem*>(dyn_smem);
@@ -121,6 +127,8 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   for (uint32_t g = threadIdx.x; g < p.groups; g += blockDim.x) sm.hist[g] = 0;
   for (uint32_t r = threadIdx.x; r <= p.regions; r += blockDim.x)
     sm.item_prefix[r] = static_cast<uint32_t>(p.item_prefix[r]);
+  if constexpr (TRANSP)
+    for (uint32_t i = threadIdx.x; i < 5 * p.gens; i += blockDim.x) sm.transp[i] = p.transp[i];
   if (threadIdx.x == 0) {
     sm.count = 0;
     sm.ntouched = 0;
@@ -128,6 +136,7 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   __syncthreads();
   constexpr uint64_t kGroupSize = factorial_u64(N - K);  // bits per group
   constexpr bool kSplitRank = N - K >= 8 && N - K <= 12;  // 32-bit in-group rank, word-aligned groups
+  static_assert(!TRANSP || kSplitRank, "the incremental-rank path needs the split rank");
   constexpr uint64_t kGroupWords32 = kGroupSize / 32;
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const uint32_t round = kBlock * p.ppt;
@@ -153,6 +162,9 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
       uint32_t skip[4];
       bool val[4];
       bool untagged = false;
+      // Incremental-rank path: the parent's digits and split rank, once per parent.
+      uint64_t pdig[4];
+      uint32_t pgrp[4], pinner[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const uint32_t i = r0 + k * kBlock + tid;
@@ -161,6 +173,11 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
         const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
         skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
         untagged = untagged || (val[k] && !tag);
+        if constexpr (TRANSP) {
+          pdig[k] = 0;
+          pgrp[k] = pinner[k] = 0;
+          if (val[k]) lehmer_digits_split4<N, K>(par[k], &pdig[k], &pgrp[k], &pinner[k]);
+        }
       }
       // Pass j applies to every parent its j-th generator other than the
       // skipped one, so a round of tagged parents is done after gens - 1
@@ -180,7 +197,33 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
           bool won = false;
           uint64_t c = 0;
           uint32_t grp = 0;
-          if (live) {
+          if (live && TRANSP) {
+            // Swapping positions t-1 and t changes only those two Lehmer
+            // digits: with a, b the two symbols and c1, c2 their digits,
+            // the new digits are c2 + [a < b] and c1 - [b < a].
+            const uint32_t* ti = sm.transp + 5 * g;
+            const uint32_t t = ti[0];
+            const uint32_t a = static_cast<uint32_t>(par[k] >> (4 * (t - 1))) & 15u;
+            const uint32_t b = static_cast<uint32_t>(par[k] >> (4 * t)) & 15u;
+            const unsigned long long x = static_cast<unsigned long long>(a ^ b);
+            c = (par[k] ^ (x << (4 * (t - 1))) ^ (x << (4 * t))) & ((1ull << (4 * N)) - 1ull);
+            const int c1 = static_cast<int>((pdig[k] >> (4 * (t - 1))) & 15u);
+            const int c2 = static_cast<int>((pdig[k] >> (4 * t)) & 15u);
+            const int lt = a < b ? 1 : 0;
+            const int d1 = c2 + lt - c1, d2 = c1 - (1 - lt) - c2;
+            grp = static_cast<uint32_t>(static_cast<int>(pgrp[k]) + d1 * static_cast<int>(ti[1]) +
+                                        d2 * static_cast<int>(ti[2]));
+            const uint32_t inner = static_cast<uint32_t>(static_cast<int>(pinner[k]) + d1 * static_cast<int>(ti[3]) +
+                                                         d2 * static_cast<int>(ti[4]));
+            if (grp < p.groups && inner < kGroupSize) {
+              const uint32_t bit = 1u << (inner & 31);
+              unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
+                                   (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
+              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+            } else {
+              raise_error(&p.control->error, ERR_RANK_RANGE);
+            }
+          } else if (live) {
             c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
             if constexpr (kSplitRank) {
               // Group = the first K Lehmer digits, and the rank inside the group

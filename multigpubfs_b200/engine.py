@@ -91,9 +91,11 @@ class NativeGraph:
         self.close()
 
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
-             planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True, host_loop=False) -> dict:
+             planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True, host_loop=False,
+             full_rank=False) -> dict:
         req = native.PlanRequest()
-        req.options = (0 if parent_skip else native.OPTION_NO_PARENT_SKIP) | (native.OPTION_HOST_LOOP if host_loop else 0)
+        req.options = ((0 if parent_skip else native.OPTION_NO_PARENT_SKIP) |
+                       (native.OPTION_HOST_LOOP if host_loop else 0) | (native.OPTION_FULL_RANK if full_rank else 0))
         req.bucket_margin = 0 if bucket_margin is None else (0xFFFFFFFF if bucket_margin == 0 else bucket_margin)
         req.bucket_min_work = bucket_min_work or 0
         req.visited = native.VISITED[visited]

@@ -55,6 +55,7 @@ class PlanRequest(C.Structure):
 
 OPTION_NO_PARENT_SKIP = 1
 OPTION_HOST_LOOP = 2
+OPTION_FULL_RANK = 4
 
 
 class PlanInfo(C.Structure):

@@ -170,6 +170,18 @@ def test_coxeter_bucketed(n, dedup):
     assert out[2] == [list(range(n))[::-1]]
 
 
+@pytest.mark.parametrize("n", [9, 10, 11])
+@pytest.mark.parametrize("full_rank", [False, True])
+def test_coxeter_grouped_incremental_rank(n, full_rank):
+    """Adjacent transpositions: grouped layers derive each child's rank from
+    its parent's Lehmer digits (or rank from scratch with full_rank); both give
+    the Mahonian layer table, from the first layer on."""
+    g = G.permutation_graph(G.coxeter_generators(n), list(range(n)))
+    out = run(g, visited="bitmap", dedup="grouped", bucket_min_work=1, full_rank=full_rank)
+    assert out[1].layer_sizes == G.coxeter_layers(n)
+    assert out[2] == [list(range(n))[::-1]]
+
+
 def test_lrx12_three_bank_hash():
     sizes_ref, _, _ = P.packed_bfs(G.lrx_generators(10), list(range(10)))
     out = run(G.permutation_graph(G.lrx_generators(10), list(range(10))), visited="hash3")
