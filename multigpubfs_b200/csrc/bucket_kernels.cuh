@@ -54,6 +54,10 @@ struct RouteParams {
   const unsigned long long* shard_cap;     // per shard
   unsigned long long* shard_count;         // per shard, exact
   Control* control;
+  // Hash routing (route_lehmer<0, 0>): shard = the region of the key's home
+  // slot, (mix64(key) & table_mask) >> region_shift.
+  unsigned long long table_mask, key_mask;
+  uint32_t region_shift, pad1;
 };
 
 struct AcceptParams {
@@ -66,7 +70,16 @@ struct AcceptParams {
   unsigned long long capacity;
   unsigned long long* work;                // device work-item counter, zero at launch
   Control* control;
+  // accept_hash: the all-visited table.
+  unsigned long long* table;
+  unsigned long long table_mask, key_mask;
+  uint32_t probe_limit, pad1;
 };
+
+// Shard of a successor: its rank range for the Lehmer bitmap, or (N = 0) the
+// table region of its home slot for the hash.
+template <int N, int K>
+__device__ __forceinline__ uint32_t route_shard(const RouteParams& p, uint64_t c);
 
 // Dynamic shared memory of route_lehmer (after the generator program).
 struct RouteSmem {
@@ -90,6 +103,15 @@ __device__ __forceinline__ uint32_t prefix_shard(uint64_t w) {
     used |= 1u << s;
   }
   return shard;
+}
+
+template <int N, int K>
+__device__ __forceinline__ uint32_t route_shard(const RouteParams& p, uint64_t c) {
+  if constexpr (N == 0) {
+    return static_cast<uint32_t>((mix64(c & p.key_mask) & p.table_mask) >> p.region_shift);
+  } else {
+    return prefix_shard<N, K>(c);
+  }
 }
 
 template <int N, int K>
@@ -151,7 +173,7 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
           if (k >= static_cast<int>(p.ppt)) break;
           if (val[k] && g != skip[k]) {
             const uint64_t c = apply_terms(par[k], terms, tb, te);
-            const uint32_t s = prefix_shard<N, K>(c);
+            const uint32_t s = route_shard<N, K>(p, c);
             const uint32_t slot = live * kBlock + tid;
             sm.state[slot] = c | gtag;
             sm.tag[slot] = s | (atomicAdd(&sm.hist[warp][s], 1u) << 8);
@@ -332,6 +354,97 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const bool won = !(old[k] & (1ull << (r[k] & 63)));
+        const unsigned m = __ballot_sync(kFullMask, won);
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          uint32_t wb = 0;
+          if (static_cast<int>(lane) == leader) wb = atomicAdd(&win_count, static_cast<uint32_t>(__popc(m)));
+          wb = __shfl_sync(kFullMask, wb, leader);
+          if (won) win[wb + __popc(m & lanemask_lt())] = w[k];
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t nw = win_count;
+    if (tid == 0 && nw) win_base = atomicAdd(&p.control->next_count, static_cast<unsigned long long>(nw));
+    __syncthreads();
+    bool overflow = false;
+    for (uint32_t i = tid; i < nw; i += kBlock) {
+      const unsigned long long at = win_base + i;
+      if (at < p.capacity) p.next[at] = win[i];
+      else overflow = true;
+    }
+    if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
+    __syncthreads();
+    if (tid == 0) win_count = 0;
+  }
+}
+
+// Accept for hash-routed layers: items are chunks of one table region, claimed
+// region-major from a device counter, so the resident blocks insert into one or
+// two L2-sized regions.  The home slots of eight keys per thread are read
+// before any result is used; a key found there is done, the others insert
+// (CAS, probing on).  Winners are appended like accept_lehmer's.
+static __global__ void __launch_bounds__(kBlock) accept_hash(AcceptParams p) {
+  __shared__ unsigned long long win[kAcceptChunk];
+  __shared__ unsigned long long item_prefix[kMaxShards + 1];
+  __shared__ unsigned long long item_s;
+  __shared__ uint32_t win_count;
+  __shared__ unsigned long long win_base;
+  if (*reinterpret_cast<volatile unsigned int*>(&p.control->error) & ERR_BUCKET_OVERFLOW) return;
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint32_t s = 0; s < p.shards; ++s) {
+      item_prefix[s] = run;
+      run += (p.shard_count[s] + kAcceptChunk - 1) / kAcceptChunk;
+    }
+    item_prefix[p.shards] = run;
+    win_count = 0;
+  }
+  __syncthreads();
+  const uint32_t tid = threadIdx.x, lane = lane_id();
+  const unsigned long long items = item_prefix[p.shards];
+  for (;;) {
+    if (tid == 0) item_s = atomicAdd(p.work, 1ull);
+    __syncthreads();
+    const unsigned long long item = item_s;
+    if (item >= items) break;
+    uint32_t lo = 0, hi = p.shards;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (item_prefix[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const uint32_t s = lo;
+    const unsigned long long first = (item - item_prefix[s]) * kAcceptChunk;
+    const uint32_t n = static_cast<uint32_t>(min(static_cast<unsigned long long>(kAcceptChunk), p.shard_count[s] - first));
+    const unsigned long long* src = p.buckets + p.shard_begin[s] + first;
+    for (uint32_t round = 0; round < n; round += 8 * kBlock) {
+      unsigned long long w[8], prev[8];
+      uint64_t slot[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = round + k * kBlock + tid;
+        w[k] = i < n ? src[i] : 0ull;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = round + k * kBlock + tid;
+        const uint64_t key = w[k] & p.key_mask;
+        slot[k] = mix64(key) & p.table_mask;
+        prev[k] = i < n ? *reinterpret_cast<volatile unsigned long long*>(&p.table[slot[k]]) : key;
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t i = round + k * kBlock + tid;
+        const uint64_t key = w[k] & p.key_mask;
+        bool won = false;
+        if (i < n && (prev[k] & p.key_mask) != key) {
+          // Empty or another key in the home slot: insert (CAS and probe on).
+          const int rc = hash_insert(p.table, p.table_mask, key, p.key_mask, 0, p.probe_limit);
+          if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+          won = rc == 1;
+        }
         const unsigned m = __ballot_sync(kFullMask, won);
         if (m) {
           const int leader = __ffs(m) - 1;

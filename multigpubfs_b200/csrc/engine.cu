@@ -496,11 +496,13 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     }
   }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
-  if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) && !(visited == MGBFS2_VISITED_BITMAP && lehmer))
+  const bool hash_routed = dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_HASH && packed;
+  if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) && !(visited == MGBFS2_VISITED_BITMAP && lehmer) &&
+      !hash_routed)
     return MGBFS2_UNSUPPORTED;
   // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
   if (dedup == MGBFS2_DEDUP_SORT && (!packed || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
-  if (dedup == MGBFS2_DEDUP_BUCKET) {
+  if (dedup == MGBFS2_DEDUP_BUCKET && !hash_routed) {
     // Shards = states sharing their first K symbols: N!/(N-K)! shards whose
     // bitmap slices hold (N-K)! bits.  Default: the smallest K (1 or 2) whose
     // slice is at most 8 MiB, so the slices the resident accept blocks work
@@ -559,6 +561,17 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (visited == MGBFS2_VISITED_HASH) {
     const uint64_t want = state_bound ? state_bound : cap;
     p.table_slots = std::max<uint64_t>(1024, next_pow2(2 * std::min(want, cap)));
+  }
+  if (hash_routed) {
+    // Hash-routed layers: shard = table region of a key's home slot, regions
+    // of about 16 MB (L2-sized), a power of two between 1 and kMaxShards.
+    uint32_t regions = 1;
+    while (regions < kMaxShards && p.table_slots * 8 / (2ull * regions) >= (16ull << 20)) regions *= 2;
+    bucket_prefix = 0;
+    bucket_shards = regions;
+    p.shards = regions;
+    bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
+    bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
   }
   p.device_bytes = fixed + (visited == MGBFS2_VISITED_HASH ? p.table_slots * 8 : 0);
   if (!packed) {
@@ -968,6 +981,15 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   rp.shard_cap = meta + kMaxShards;
   rp.shard_count = meta + 2 * kMaxShards;
   rp.control = p.control;
+  if (visit_kind() == V_HASH) {
+    uint32_t shift = 0;
+    while ((1ull << shift) < table_slots) ++shift;
+    uint32_t rbits = 0;
+    while ((1u << rbits) < bucket_shards) ++rbits;
+    rp.table_mask = table_slots - 1;
+    rp.key_mask = key_mask;
+    rp.region_shift = shift - rbits;
+  }
   const uint64_t tiles = (p.count + kBlock * rp.ppt - 1) / (kBlock * rp.ppt);
   const size_t route_smem = sizeof(RouteSmem) + smem;
   MG_CHECK(cudaFuncSetAttribute(route_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(route_smem)));
@@ -985,6 +1007,10 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   ap.next = p.next;
   ap.capacity = p.capacity;
   ap.control = p.control;
+  ap.table = p.table;
+  ap.table_mask = p.table_mask;
+  ap.key_mask = key_mask;
+  ap.probe_limit = p.probe_limit;
   reinterpret_cast<AcceptFn>(const_cast<void*>(accept_fn))<<<grid_for(accept_fn, 0, UINT32_MAX), kBlock, 0, stream>>>(ap);
   ++launches;
   MG_CHECK(cudaGetLastError());
@@ -1159,11 +1185,16 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements);
   if (!fn) return MGBFS2_UNSUPPORTED;
   // Bucketed layers for large frontiers; small layers use the fused kernel.
-  const bool bucketed = plan.dedup == MGBFS2_DEDUP_BUCKET && visit == V_LEHMER;
+  const bool bucketed = plan.dedup == MGBFS2_DEDUP_BUCKET && (visit == V_LEHMER || visit == V_HASH);
   RouteFn route_fn = nullptr;
   AcceptFn accept_fn = nullptr;
   if (bucketed) {
-    pick_bucket(elements, bucket_prefix, &route_fn, &accept_fn);
+    if (visit == V_HASH) {
+      route_fn = route_lehmer<0, 0>;
+      accept_fn = accept_hash;
+    } else {
+      pick_bucket(elements, bucket_prefix, &route_fn, &accept_fn);
+    }
     if (!route_fn) return MGBFS2_UNSUPPORTED;
   }
   shard_history.assign(bucket_shards, 0);

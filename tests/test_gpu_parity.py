@@ -59,6 +59,9 @@ VARIANTS = {
     # no group margin: most winners of the first grouped layers go to the spill region
     "bitmap_grouped_tight": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, bucket_margin=0),
     "bitmap_grouped_noskip": dict(visited="bitmap", dedup="grouped", bucket_min_work=1, parent_skip=False),
+    # hash with every layer routed to table regions, then inserted per region
+    "hash_bucket": dict(visited="hash", dedup="bucket", bucket_min_work=1),
+    "hash_bucket_tight": dict(visited="hash", dedup="bucket", bucket_min_work=1, bucket_margin=0),
     # host-driven layer loop instead of the one-graph device loop
     "bitmap_atomic_hostloop": dict(visited="bitmap", dedup="atomic", host_loop=True),
     "hash_hostloop": dict(visited="hash", host_loop=True),
@@ -136,7 +139,8 @@ def test_parent_skip_accounting(lrx_layers):
 @pytest.mark.parametrize("variant", ["auto", "bitmap_atomic", "bitmap_warp", "hash", "hash3", "bitmap_bucket",
                                      "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip", "bitmap_sort",
                                      "bitmap_sort_noskip", "hash_sort", "hash3_sort", "bitmap_grouped",
-                                     "bitmap_grouped_tight", "bitmap_grouped_noskip"])
+                                     "bitmap_grouped_tight", "bitmap_grouped_noskip", "hash_bucket",
+                                     "hash_bucket_tight"])
 def test_lrx_small(lrx_layers, variant):
     redo = 0
     for n in range(3, 12):
@@ -144,7 +148,7 @@ def test_lrx_small(lrx_layers, variant):
         assert out is not None
         assert out[1].layer_sizes == lrx_layers[n], (n, variant)
         redo += out[1].redo_layers
-    if variant == "bitmap_bucket_tight":
+    if variant in ("bitmap_bucket_tight", "hash_bucket_tight"):
         assert redo > 0  # the exact redo path ran and changed nothing
 
 
@@ -201,7 +205,8 @@ def test_random_sweep_instances(closed):
         g = G.sweep_instance(i, closed)
         n = len(g["start"])
         ref, last_ref, _ = P.packed_bfs(g["action"]["generators"], g["start"], sample=1 << 22)
-        for variant in ("auto", "hash", "bitmap_warp", "bitmap_sort", "hash_sort", "bitmap_grouped_tight") + \
+        for variant in ("auto", "hash", "bitmap_warp", "bitmap_sort", "hash_sort", "bitmap_grouped_tight",
+                        "hash_bucket") + \
                 (("hash3", "hash3_sort") if closed else ()):
             out = run(g, **VARIANTS[variant])
             assert out[1].layer_sizes == ref, (i, variant, n)
