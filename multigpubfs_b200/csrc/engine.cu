@@ -132,7 +132,11 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
     if (rc) { set_message(error, cap, "CUDA_EVENT"); delete g; return rc; }
   }
   cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) g->sm_count = prop.multiProcessorCount;
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+    g->sm_count = prop.multiProcessorCount;
+    g->smem_per_sm = static_cast<int>(prop.sharedMemPerMultiprocessor);
+    g->smem_reserved = static_cast<int>(prop.reservedSharedMemPerBlock);
+  }
   g->analyse();
   *out = g;
   return MGBFS2_OK;
@@ -818,7 +822,7 @@ static size_t group_meta_bytes(uint32_t groups) {
 // last growth ratio, plus 25 % and bucket_margin; the spill region gets the exact
 // bound `cap`, so every winner has a place.
 int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total,
-                         size_t smem, uint64_t* items) {
+                         size_t smem, uint64_t* items, uint32_t* grid) {
   const uint32_t G = groups, R = groups + 1;
   int rc = MGBFS2_OK;
   const size_t words = group_meta_words(G), bytes = group_meta_bytes(G);
@@ -872,9 +876,14 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   GroupedFn f = group_transp ? pick_grouped_transp(elements, group_prefix) : pick_grouped(elements, group_prefix);
   if (!f) return MGBFS2_UNSUPPORTED;
   *fn = reinterpret_cast<void*>(f);
-  *smem_total = sizeof(GroupedSmem) + smem;
+  *smem_total = sizeof(GroupedSmem) + smem + (group_transp ? 5 * sizeof(uint32_t) * gens : 0);
   MG_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(*smem_total)));
+  // Five blocks per SM in the 196 KB configuration measured fastest on S13
+  // LRX (60 KB left as L1); the transposition kernel's registers allow four,
+  // which take the 164 KB configuration.
+  const int blocks = set_carveout(reinterpret_cast<const void*>(f), *smem_total, kGroupBlocksPerSM);
+  *grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(blocks) * sm_count, *items)));
   return MGBFS2_OK;
 }
 
@@ -1022,9 +1031,47 @@ int Graph::visit_kind() const {
   return plan.visited == MGBFS2_VISITED_HASH ? V_HASH : V_HASH3;
 }
 
+int Graph::set_carveout(const void* fn, size_t smem, int want) {
+  // Left to itself the runtime may pick the largest shared-memory
+  // configuration for occupancy, which leaves about 28 KB of L1; the grouped
+  // layers ran about 1.5x slower there, as the L1 also stages the loads and
+  // atomics in flight.
+  int by_regs = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by_regs, fn, kBlock, 0) != cudaSuccess || by_regs < 1) {
+    cudaGetLastError();
+    by_regs = 1;
+  }
+  cudaFuncAttributes attr{};
+  if (cudaFuncGetAttributes(&attr, fn) != cudaSuccess) {
+    cudaGetLastError();
+    attr.sharedSizeBytes = 0;
+  }
+  const size_t per_block = attr.sharedSizeBytes + smem + static_cast<size_t>(smem_reserved);
+  int blocks = std::min(want, by_regs);
+  blocks = std::max(1, std::min<int>(blocks, static_cast<int>(static_cast<size_t>(smem_per_sm) / per_block)));
+  // Shared-memory configurations of compute capability 9.0 and 10.0, in KB;
+  // the runtime rounds a preference up to the next one, so the floor of the
+  // chosen configuration's share selects exactly it.
+  static constexpr int kConfigKB[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+  const size_t need = static_cast<size_t>(blocks) * per_block;
+  int config = smem_per_sm;
+  for (int kb : kConfigKB)
+    if (static_cast<size_t>(kb) * 1024 >= need) {
+      config = std::min(kb * 1024, smem_per_sm);
+      break;
+    }
+  const int pct = static_cast<int>((100ll * config) / smem_per_sm);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct) != cudaSuccess) cudaGetLastError();
+  carveout_blocks[fn] = blocks;
+  return blocks;
+}
+
 uint32_t Graph::grid_for(const void* fn, size_t smem, uint64_t work_blocks) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem) != cudaSuccess || per_sm < 1) {
+  const auto known = carveout_blocks.find(fn);
+  if (known != carveout_blocks.end()) {
+    per_sm = known->second;
+  } else if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem) != cudaSuccess || per_sm < 1) {
     cudaGetLastError();
     per_sm = 1;
   }
@@ -1213,6 +1260,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   p.key_mask = key_mask;
   p.ppt = gens <= 4 ? 4 : 2;
   const size_t smem = terms.size() * sizeof(Term) + term_begin.size() * sizeof(uint32_t);
+  if (!sorted) set_carveout(reinterpret_cast<const void*>(fn), smem, kPackedBlocksPerSM);
   if (visit == V_MULTISET) {
     p.ms.n = elements;
     p.ms.bits = bits;
@@ -1303,10 +1351,11 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     if (!group_layer && front_grouped && (rc = gather_front(count))) break;
     void* group_fn = nullptr;
     size_t group_smem = 0;
+    uint32_t group_grid = 1;
     uint64_t group_items = 0;
     if (group_layer) {
       const uint64_t prev_count = depth ? layer_sizes[depth - 1] : 0;
-      if ((rc = grouped_setup(count, prev_count, cap, &group_fn, &group_smem, smem, &group_items))) break;
+      if ((rc = grouped_setup(count, prev_count, cap, &group_fn, &group_smem, smem, &group_items, &group_grid))) break;
     } else if ((rc = next.ensure((cap + 2) * 8))) {
       break;
     }
@@ -1390,7 +1439,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         gp.work = meta + 6 * R + 1;
         gp.control = p.control;
         gp.transp = static_cast<const uint32_t*>(transp_buf.ptr);
-        reinterpret_cast<GroupedFn>(group_fn)<<<grid_for(group_fn, group_smem, group_items), kBlock, group_smem,
+        reinterpret_cast<GroupedFn>(group_fn)<<<group_grid, kBlock, group_smem,
                                                  stream>>>(gp);
         ++launches;
         MG_CHECK(cudaGetLastError());

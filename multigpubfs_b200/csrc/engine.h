@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <vector>
 
 #include "../../include/mgbfs2.h"
@@ -58,6 +59,7 @@ struct Graph {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_run[2] = {nullptr, nullptr}, ev_kernel[2] = {nullptr, nullptr};
   int sm_count = 148;
+  int smem_per_sm = 233472, smem_reserved = 1024;  // shared memory per SM, and reserved per block
   DeviceBuffer bitmap, front, next, table, bank[3], program, control_buf, scratch;
   uint64_t table_slots = 0, bank_slots[3] = {0, 0, 0};
   Control* host_control = nullptr;
@@ -89,7 +91,11 @@ struct Graph {
   int plan_transpositions(bool allowed);
   void plan_group_order();
   int grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total, size_t smem,
-                    uint64_t* items);
+                    uint64_t* items, uint32_t* grid);
+  // Sets fn's shared-memory carveout to the smallest configuration holding
+  // `want` resident blocks (fewer where registers allow fewer); returns them.
+  int set_carveout(const void* fn, size_t smem, int want);
+  std::map<const void*, int> carveout_blocks;  // resident blocks per SM of kernels given a carveout
   int grouped_finish();   // after the layer: per-region counts of `next` into next_begin/next_cap layout
   int gather_front(uint64_t count);  // grouped `front` -> contiguous
 

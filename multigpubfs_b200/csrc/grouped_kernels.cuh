@@ -35,10 +35,12 @@
 
 namespace mgbfs2 {
 
-constexpr uint32_t kGroupStage = 2048;  // staged winners per block (4 blocks per SM fit)
+constexpr uint32_t kGroupStage = 1024;  // staged winners per block (one pass of 256 x 4 parents)
+constexpr int kGroupBlocksPerSM = 5;    // resident blocks the shared-memory carveout is sized for
 constexpr uint32_t kMaxGroups = 1728;   // 13!/10! = 1716 groups at most
 constexpr uint32_t kGroupChunk = 4096;  // parents per work item
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
+static_assert(kGroupStage >= kBlock * 4, "a pass stages up to kBlock * ppt winners, ppt <= 4");
 
 constexpr uint64_t factorial_u64(int m) { return m <= 1 ? 1ull : static_cast<uint64_t>(m) * factorial_u64(m - 1); }
 
@@ -67,16 +69,16 @@ struct GroupedParams {
 };
 
 struct GroupedSmem {
-  uint32_t item_prefix[kMaxGroups + 2];  // the work-item prefix (regions + 1 entries, visiting order)
   unsigned long long state[kGroupStage];
   uint16_t grp[kGroupStage];
   uint16_t rank[kGroupStage];
-  uint32_t hist[kMaxGroups];   // staged winners per group
-  uint32_t gbase[kMaxGroups];  // reserved position of the block's run in each group (saturated at 2^32 - 1)
+  // Per group: staged winners, then (after the reservation) how many of them fit.
+  uint32_t hist[kMaxGroups];
+  // Per group: index in `next` of the block's reserved run.
+  unsigned long long gdst[kMaxGroups];
   uint16_t touched[kMaxGroups];  // the groups with staged winners, in first-touch order
-  uint32_t transp[kMaxTranspGens * 5];
-  unsigned long long item;
-  uint32_t count, ntouched;
+  unsigned long long item, src;  // the claimed work item and its first parent's index
+  uint32_t count, ntouched, n;
 };
 
 // Writes the staged winners: one reservation per (block, group); positions
@@ -86,19 +88,24 @@ __device__ __forceinline__ void grouped_flush(const GroupedParams& p, GroupedSme
   const uint32_t touched = sm.ntouched;
   for (uint32_t t = threadIdx.x; t < touched; t += blockDim.x) {
     const uint32_t g = sm.touched[t];
-    const unsigned long long at = atomicAdd(&p.next_count[g], static_cast<unsigned long long>(sm.hist[g]));
-    // A saturated base only sends the run to the spill region.
-    sm.gbase[g] = at < 0xffffffffull ? static_cast<uint32_t>(at) : 0xffffffffu;
+    const uint32_t staged = sm.hist[g];
+    const unsigned long long at = atomicAdd(&p.next_count[g], static_cast<unsigned long long>(staged));
+    const unsigned long long cap = __ldg(&p.next_cap[g]);
+    const unsigned long long room = at < cap ? cap - at : 0ull;
+    sm.hist[g] = room < staged ? static_cast<uint32_t>(room) : staged;
+    sm.gdst[g] = __ldg(&p.next_begin[g]) + at;
   }
   __syncthreads();
+  // The destinations come from shared memory: no per-winner reads of the
+  // region tables, which would otherwise compete for L1 with the claims.
   const uint32_t n = sm.count;
   bool overflow = false;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t g = sm.grp[i];
-    const unsigned long long pos = static_cast<unsigned long long>(sm.gbase[g]) + sm.rank[i];
-    if (pos < __ldg(&p.next_cap[g])) {
-      p.next[__ldg(&p.next_begin[g]) + pos] = sm.state[i];
+    const uint32_t g = sm.grp[i], r = sm.rank[i];
+    if (r < sm.hist[g]) {
+      p.next[sm.gdst[g] + r] = sm.state[i];
     } else {
+      // Past the group's capacity: the spill region.
       const unsigned long long sp = atomicAdd(&p.next_count[p.groups], 1ull);
       if (sp < __ldg(&p.next_cap[p.groups])) p.next[__ldg(&p.next_begin[p.groups]) + sp] = sm.state[i];
       else overflow = true;
@@ -124,11 +131,12 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   for (uint32_t i = threadIdx.x; i < p.total_terms; i += blockDim.x) terms[i] = p.terms[i];
   for (uint32_t i = threadIdx.x; i <= 2 * p.gens; i += blockDim.x) tbegin[i] = p.term_begin[i];
   const uint32_t* inverse = tbegin + p.gens + 1;
+  // The transposition table sits after the term offsets in the dynamic tail, sized only for TRANSP
+  // launches, so the plain kernel's footprint does not grow.
+  uint32_t* transp = tbegin + 2 * p.gens + 1;
   for (uint32_t g = threadIdx.x; g < p.groups; g += blockDim.x) sm.hist[g] = 0;
-  for (uint32_t r = threadIdx.x; r <= p.regions; r += blockDim.x)
-    sm.item_prefix[r] = static_cast<uint32_t>(p.item_prefix[r]);
   if constexpr (TRANSP)
-    for (uint32_t i = threadIdx.x; i < 5 * p.gens; i += blockDim.x) sm.transp[i] = p.transp[i];
+    for (uint32_t i = threadIdx.x; i < 5 * p.gens; i += blockDim.x) transp[i] = p.transp[i];
   if (threadIdx.x == 0) {
     sm.count = 0;
     sm.ntouched = 0;
@@ -140,23 +148,32 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   constexpr uint64_t kGroupWords32 = kGroupSize / 32;
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const uint32_t round = kBlock * p.ppt;
-  const uint32_t items = sm.item_prefix[p.regions];
+  const unsigned long long items = __ldg(&p.item_prefix[p.regions]);
   for (;;) {
-    if (tid == 0) sm.item = atomicAdd(p.work, 1ull);
-    __syncthreads();
-    const unsigned long long item = sm.item;
-    if (item >= items) break;
-    uint32_t lo = 0, hi = p.regions;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (sm.item_prefix[mid] <= item) lo = mid;
-      else hi = mid;
+    if (tid == 0) {
+      // Claim a work item and locate it: a binary search over the region
+      // prefix (in visiting order), once per 4096 parents.
+      const unsigned long long item = atomicAdd(p.work, 1ull);
+      sm.item = item;
+      if (item < items) {
+        uint32_t lo = 0, hi = p.regions;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (__ldg(&p.item_prefix[mid]) <= item) lo = mid;
+          else hi = mid;
+        }
+        const unsigned long long first = (item - __ldg(&p.item_prefix[lo])) * kGroupChunk;
+        const uint32_t region = __ldg(&p.region_order[lo]);
+        const unsigned long long avail = __ldg(&p.region_count[region]) - first;
+        sm.n = static_cast<uint32_t>(avail < kGroupChunk ? avail : kGroupChunk);
+        sm.src = __ldg(&p.region_begin[region]) + first;
+      }
     }
-    const unsigned long long first = (item - sm.item_prefix[lo]) * kGroupChunk;
-    const uint32_t region = __ldg(&p.region_order[lo]);
-    const unsigned long long avail = p.region_count[region] - first;
-    const uint32_t n = static_cast<uint32_t>(avail < kGroupChunk ? avail : kGroupChunk);
-    const unsigned long long* src = p.frontier + p.region_begin[region] + first;
+    __syncthreads();
+    if (sm.item >= items) break;
+    const uint32_t n = sm.n;
+    const unsigned long long* src = p.frontier + sm.src;
+    __syncthreads();  // every thread has the item before thread 0 claims the next
     for (uint32_t r0 = 0; r0 < n; r0 += round) {
       uint64_t par[4];
       uint32_t skip[4];
@@ -201,7 +218,7 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
             // Swapping positions t-1 and t changes only those two Lehmer
             // digits: with a, b the two symbols and c1, c2 their digits,
             // the new digits are c2 + [a < b] and c1 - [b < a].
-            const uint32_t* ti = sm.transp + 5 * g;
+            const uint32_t* ti = transp + 5 * g;
             const uint32_t t = ti[0];
             const uint32_t a = static_cast<uint32_t>(par[k] >> (4 * (t - 1))) & 15u;
             const uint32_t b = static_cast<uint32_t>(par[k] >> (4 * t)) & 15u;

@@ -17,6 +17,7 @@ enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3 };
 
 constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
 constexpr uint32_t kBlock = 256;
+constexpr int kPackedBlocksPerSM = 4;  // resident expand_packed blocks: the 164 KB configuration, 92 KB left as L1
 
 // Device-resident layer loop (graph mode): the frontier size, which of the
 // two buffers holds it, and the loop's stop reason live on the device, so one
