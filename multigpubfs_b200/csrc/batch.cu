@@ -41,6 +41,7 @@ namespace mgbfs2 {
 namespace {
 
 constexpr uint32_t kBatchBlock = 256;
+constexpr int kBatchBlocksPerSM = 4;   // default resident batch_expand blocks per SM
 constexpr uint32_t kBatchPpt = 4;                         // frontier entries per thread per tile
 constexpr uint32_t kBatchTile = kBatchBlock * kBatchPpt;  // entries per tile (one instance per tile)
 constexpr uint32_t kBatchOut = 4096;                      // winners staged in shared memory per block
@@ -667,10 +668,11 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);
   batch_seed<<<std::max<uint32_t>(1, (W + 255) / 256), 256, 0, b->stream>>>(p);
   ++st->kernel_launches;
-  int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(batch_expand), kBatchBlock, 0);
-  // `ppt` here is the tuned blocks-per-SM of batch_expand (0 = occupancy limit).
-  const uint32_t grid = static_cast<uint32_t>((ppt ? static_cast<int>(ppt) : std::max(1, per_sm)) * b->sm_count);
+  // `ppt` here is the tuned blocks-per-SM of batch_expand (0 = the default);
+  // the carveout is sized for that many and the rest left as L1.
+  const int per_sm = size_carveout(reinterpret_cast<const void*>(batch_expand), 0,
+                                   ppt ? static_cast<int>(ppt) : kBatchBlocksPerSM, kBatchBlock);
+  const uint32_t grid = static_cast<uint32_t>(per_sm * b->sm_count);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

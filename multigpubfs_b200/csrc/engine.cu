@@ -132,11 +132,7 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
     if (rc) { set_message(error, cap, "CUDA_EVENT"); delete g; return rc; }
   }
   cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
-    g->sm_count = prop.multiProcessorCount;
-    g->smem_per_sm = static_cast<int>(prop.sharedMemPerMultiprocessor);
-    g->smem_reserved = static_cast<int>(prop.reservedSharedMemPerBlock);
-  }
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) g->sm_count = prop.multiProcessorCount;
   g->analyse();
   *out = g;
   return MGBFS2_OK;
@@ -1031,13 +1027,21 @@ int Graph::visit_kind() const {
   return plan.visited == MGBFS2_VISITED_HASH ? V_HASH : V_HASH3;
 }
 
-int Graph::set_carveout(const void* fn, size_t smem, int want) {
+int size_carveout(const void* fn, size_t smem, int want, int threads) {
   // Left to itself the runtime may pick the largest shared-memory
-  // configuration for occupancy, which leaves about 28 KB of L1; the grouped
-  // layers ran about 1.5x slower there, as the L1 also stages the loads and
+  // configuration for occupancy, which leaves about 28 KB of L1; the layer
+  // kernels ran up to 1.5x slower there, as the L1 also stages the loads and
   // atomics in flight.
+  int device = 0, smem_per_sm = 233472, reserved = 1024;
+  if (cudaGetDevice(&device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess) {
+    cudaGetLastError();
+    smem_per_sm = 233472;
+    reserved = 1024;
+  }
   int by_regs = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by_regs, fn, kBlock, 0) != cudaSuccess || by_regs < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by_regs, fn, threads, 0) != cudaSuccess || by_regs < 1) {
     cudaGetLastError();
     by_regs = 1;
   }
@@ -1046,7 +1050,7 @@ int Graph::set_carveout(const void* fn, size_t smem, int want) {
     cudaGetLastError();
     attr.sharedSizeBytes = 0;
   }
-  const size_t per_block = attr.sharedSizeBytes + smem + static_cast<size_t>(smem_reserved);
+  const size_t per_block = attr.sharedSizeBytes + smem + static_cast<size_t>(reserved);
   int blocks = std::min(want, by_regs);
   blocks = std::max(1, std::min<int>(blocks, static_cast<int>(static_cast<size_t>(smem_per_sm) / per_block)));
   // Shared-memory configurations of compute capability 9.0 and 10.0, in KB;
@@ -1062,6 +1066,11 @@ int Graph::set_carveout(const void* fn, size_t smem, int want) {
     }
   const int pct = static_cast<int>((100ll * config) / smem_per_sm);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct) != cudaSuccess) cudaGetLastError();
+  return blocks;
+}
+
+int Graph::set_carveout(const void* fn, size_t smem, int want) {
+  const int blocks = size_carveout(fn, smem, want, kBlock);
   carveout_blocks[fn] = blocks;
   return blocks;
 }

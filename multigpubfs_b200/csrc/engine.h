@@ -13,6 +13,12 @@ namespace mgbfs2 {
 
 int cuda_status(cudaError_t e);
 
+// Sets fn's shared-memory carveout on the current device to the smallest
+// configuration that holds `want` resident blocks of `threads` threads (fewer
+// where registers or shared memory allow fewer), leaving the rest as L1.
+// smem is the dynamic shared memory per block; returns the resident blocks.
+int size_carveout(const void* fn, size_t smem, int want, int threads);
+
 // A device allocation that only grows, ordered on its owner's stream.  No
 // destructor: owners call free().
 struct DeviceBuffer {
@@ -59,7 +65,6 @@ struct Graph {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_run[2] = {nullptr, nullptr}, ev_kernel[2] = {nullptr, nullptr};
   int sm_count = 148;
-  int smem_per_sm = 233472, smem_reserved = 1024;  // shared memory per SM, and reserved per block
   DeviceBuffer bitmap, front, next, table, bank[3], program, control_buf, scratch;
   uint64_t table_slots = 0, bank_slots[3] = {0, 0, 0};
   Control* host_control = nullptr;
