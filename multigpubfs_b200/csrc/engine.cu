@@ -875,9 +875,8 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   *smem_total = sizeof(GroupedSmem) + smem + (group_transp ? 5 * sizeof(uint32_t) * gens : 0);
   MG_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(f), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(*smem_total)));
-  // Five blocks per SM in the 196 KB configuration measured fastest on S13
-  // LRX (60 KB left as L1); the transposition kernel's registers allow four,
-  // which take the 164 KB configuration.
+  // Eight blocks per SM (the 164 KB configuration, 92 KB left as L1) for the
+  // plain kernel; the transposition kernel's registers allow five.
   const int blocks = set_carveout(reinterpret_cast<const void*>(f), *smem_total, kGroupBlocksPerSM);
   *grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(blocks) * sm_count, *items)));
   return MGBFS2_OK;

@@ -36,7 +36,7 @@
 namespace mgbfs2 {
 
 constexpr uint32_t kGroupStage = 1024;  // staged winners per block (one pass of 256 x 4 parents)
-constexpr int kGroupBlocksPerSM = 5;    // resident blocks the shared-memory carveout is sized for
+constexpr int kGroupBlocksPerSM = 8;    // resident blocks the shared-memory carveout is sized for
 constexpr uint32_t kMaxGroups = 1728;   // 13!/10! = 1716 groups at most
 constexpr uint32_t kGroupChunk = 4096;  // parents per work item
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
@@ -68,44 +68,72 @@ struct GroupedParams {
   const uint32_t* transp;                // gens x 5: t, wg(t-1), wg(t), wi(t-1), wi(t)
 };
 
+// The groups a block stages winners for live in a small open-addressing
+// table: a work item's children reach a few dozen groups (LRX: X keeps the
+// group, L and R reach ten each), so 256 slots replace per-group arrays of
+// all 1,716 groups and leave room for eight blocks per SM.  A winner whose
+// group finds no slot (a full table) is staged with kNoSlot and written to
+// the spill region.
+constexpr uint32_t kGroupSlots = 256;
+constexpr uint32_t kEmptySlot = 0xffffffffu;
+constexpr uint16_t kNoSlot = 0xffff;
+static_assert(kGroupSlots == 256, "group_slot hashes to the top 8 bits");
+
 struct GroupedSmem {
   unsigned long long state[kGroupStage];
-  uint16_t grp[kGroupStage];
-  uint16_t rank[kGroupStage];
-  // Per group: staged winners, then (after the reservation) how many of them fit.
-  uint32_t hist[kMaxGroups];
-  // Per group: index in `next` of the block's reserved run.
-  unsigned long long gdst[kMaxGroups];
-  uint16_t touched[kMaxGroups];  // the groups with staged winners, in first-touch order
-  unsigned long long item, src;  // the claimed work item and its first parent's index
-  uint32_t count, ntouched, n;
+  unsigned long long sdst[kGroupSlots];  // per slot: index in `next` of the block's reserved run
+  uint32_t skey[kGroupSlots];            // per slot: the group, or kEmptySlot
+  uint32_t scnt[kGroupSlots];            // per slot: staged winners, then (after the reservation) how many fit
+  uint16_t rank[kGroupStage];            // per winner: its position in its slot's run
+  uint16_t slot[kGroupStage];            // per winner: its slot, or kNoSlot
+  uint16_t used[kGroupSlots];            // the occupied slots, in first-use order
+  unsigned long long item, src;          // the claimed work item and its first parent's index
+  uint32_t count, nused, n;
 };
 
+// The slot of group g, claimed if new; -1 when the table has none free.
+// Bounded: at most kGroupSlots probes.
+__device__ __forceinline__ int group_slot(GroupedSmem& sm, uint32_t g) {
+  uint32_t h = (g * 0x9E3779B1u) >> 24;
+  for (uint32_t probe = 0; probe < kGroupSlots; ++probe, h = (h + 1) & (kGroupSlots - 1)) {
+    const uint32_t k = *reinterpret_cast<volatile uint32_t*>(&sm.skey[h]);
+    if (k == g) return static_cast<int>(h);
+    if (k == kEmptySlot) {
+      const uint32_t prev = atomicCAS(&sm.skey[h], kEmptySlot, g);
+      if (prev == kEmptySlot) {
+        sm.used[atomicAdd(&sm.nused, 1u)] = static_cast<uint16_t>(h);
+        return static_cast<int>(h);
+      }
+      if (prev == g) return static_cast<int>(h);
+    }
+  }
+  return -1;
+}
+
 // Writes the staged winners: one reservation per (block, group); positions
-// past a group's capacity go to the spill region.  All threads call it.
+// past a group's capacity, and winners without a slot, go to the spill
+// region.  All threads call it.
 __device__ __forceinline__ void grouped_flush(const GroupedParams& p, GroupedSmem& sm) {
   __syncthreads();
-  const uint32_t touched = sm.ntouched;
-  for (uint32_t t = threadIdx.x; t < touched; t += blockDim.x) {
-    const uint32_t g = sm.touched[t];
-    const uint32_t staged = sm.hist[g];
+  const uint32_t used = sm.nused;
+  for (uint32_t t = threadIdx.x; t < used; t += blockDim.x) {
+    const uint32_t s = sm.used[t];
+    const uint32_t g = sm.skey[s];
+    const uint32_t staged = sm.scnt[s];
     const unsigned long long at = atomicAdd(&p.next_count[g], static_cast<unsigned long long>(staged));
     const unsigned long long cap = __ldg(&p.next_cap[g]);
     const unsigned long long room = at < cap ? cap - at : 0ull;
-    sm.hist[g] = room < staged ? static_cast<uint32_t>(room) : staged;
-    sm.gdst[g] = __ldg(&p.next_begin[g]) + at;
+    sm.scnt[s] = room < staged ? static_cast<uint32_t>(room) : staged;
+    sm.sdst[s] = __ldg(&p.next_begin[g]) + at;
   }
   __syncthreads();
-  // The destinations come from shared memory: no per-winner reads of the
-  // region tables, which would otherwise compete for L1 with the claims.
   const uint32_t n = sm.count;
   bool overflow = false;
   for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const uint32_t g = sm.grp[i], r = sm.rank[i];
-    if (r < sm.hist[g]) {
-      p.next[sm.gdst[g] + r] = sm.state[i];
+    const uint32_t s = sm.slot[i], r = sm.rank[i];
+    if (s != kNoSlot && r < sm.scnt[s]) {
+      p.next[sm.sdst[s] + r] = sm.state[i];
     } else {
-      // Past the group's capacity: the spill region.
       const unsigned long long sp = atomicAdd(&p.next_count[p.groups], 1ull);
       if (sp < __ldg(&p.next_cap[p.groups])) p.next[__ldg(&p.next_begin[p.groups]) + sp] = sm.state[i];
       else overflow = true;
@@ -114,16 +142,22 @@ __device__ __forceinline__ void grouped_flush(const GroupedParams& p, GroupedSme
   if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
   if (threadIdx.x == 0 && n) atomicAdd(&p.control->next_count, static_cast<unsigned long long>(n));
   __syncthreads();
-  for (uint32_t t = threadIdx.x; t < touched; t += blockDim.x) sm.hist[sm.touched[t]] = 0;
+  for (uint32_t t = threadIdx.x; t < used; t += blockDim.x) {
+    const uint32_t s = sm.used[t];
+    sm.skey[s] = kEmptySlot;
+    sm.scnt[s] = 0;
+  }
   if (threadIdx.x == 0) {
     sm.count = 0;
-    sm.ntouched = 0;
+    sm.nused = 0;
   }
   __syncthreads();
 }
 
+// Eight blocks per SM for the plain kernel (32 registers, no spills); the
+// incremental-rank kernel spills at 32 registers and runs five.
 template <int N, int K, bool TRANSP>
-__global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
+__global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand_grouped(GroupedParams p) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   GroupedSmem& sm = *reinterpret_cast<GroupedSmem*>(dyn_smem);
   Term* terms = reinterpret_cast<Term*>(dyn_smem + sizeof(GroupedSmem));
@@ -134,12 +168,15 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
   // The transposition table sits after the term offsets in the dynamic tail, sized only for TRANSP
   // launches, so the plain kernel's footprint does not grow.
   uint32_t* transp = tbegin + 2 * p.gens + 1;
-  for (uint32_t g = threadIdx.x; g < p.groups; g += blockDim.x) sm.hist[g] = 0;
+  for (uint32_t t = threadIdx.x; t < kGroupSlots; t += blockDim.x) {
+    sm.skey[t] = kEmptySlot;
+    sm.scnt[t] = 0;
+  }
   if constexpr (TRANSP)
     for (uint32_t i = threadIdx.x; i < 5 * p.gens; i += blockDim.x) transp[i] = p.transp[i];
   if (threadIdx.x == 0) {
     sm.count = 0;
-    sm.ntouched = 0;
+    sm.nused = 0;
   }
   __syncthreads();
   constexpr uint64_t kGroupSize = factorial_u64(N - K);  // bits per group
@@ -202,10 +239,11 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
       const uint32_t passes = __syncthreads_or(untagged) ? p.gens : p.gens - 1;
       for (uint32_t j = 0; j < passes; ++j) {
         // Room for this pass's winners (at most one per parent).
+        // Also flush a half-full slot table, which keeps probes short.
         __syncthreads();
-        const uint32_t pending = sm.count;
+        const uint32_t pending = sm.count, slots_used = sm.nused;
         __syncthreads();
-        if (pending + round > kGroupStage) grouped_flush(p, sm);
+        if (pending + round > kGroupStage || slots_used > kGroupSlots / 2) grouped_flush(p, sm);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const uint32_t g = j + (j >= skip[k] ? 1u : 0u);
@@ -268,16 +306,18 @@ __global__ void __launch_bounds__(kBlock) expand_grouped(GroupedParams p) {
             if (won) {
               const unsigned peers = __match_any_sync(m, grp);
               const int gl = __ffs(peers) - 1;
-              uint32_t rb = 0;
+              uint32_t packed = 0;  // slot | first rank << 16 (ranks stay below kGroupStage)
               if (static_cast<int>(lane) == gl) {
-                rb = atomicAdd(&sm.hist[grp], static_cast<uint32_t>(__popc(peers)));
-                if (rb == 0) sm.touched[atomicAdd(&sm.ntouched, 1u)] = static_cast<uint16_t>(grp);
+                const int gs = group_slot(sm, grp);
+                packed = gs < 0 ? kNoSlot
+                                : (static_cast<uint32_t>(gs) |
+                                   atomicAdd(&sm.scnt[gs], static_cast<uint32_t>(__popc(peers))) << 16);
               }
-              rb = __shfl_sync(peers, rb, gl) + __popc(peers & lanemask_lt());
-              const uint32_t slot = base + __popc(m & lanemask_lt());
-              sm.state[slot] = c | gtag;
-              sm.grp[slot] = static_cast<uint16_t>(grp);
-              sm.rank[slot] = static_cast<uint16_t>(rb);
+              packed = __shfl_sync(peers, packed, gl);
+              const uint32_t at = base + __popc(m & lanemask_lt());
+              sm.state[at] = c | gtag;
+              sm.slot[at] = static_cast<uint16_t>(packed & 0xffffu);
+              sm.rank[at] = static_cast<uint16_t>((packed >> 16) + __popc(peers & lanemask_lt()));
             }
           }
         }
