@@ -252,6 +252,8 @@ def bench_planner(args, local):
          [workloads.planner_instance(i) for i in range(args.instances)], None),
         ("sweep_heldout_1gib", "512-instance sweep on held-out seeds, n in {7,8,9,10}, 1 GiB memory budget",
          workloads.sweep(512, seed_base=20261203 + 4096), 1 << 30),
+        ("sweep_heldout_256mib", "512-instance sweep on held-out seeds, n in {7,8,9,10}, 256 MiB memory budget",
+         workloads.sweep(512, seed_base=20261203 + 4096), 1 << 28),
     ]
     keys = ("seconds", "device_seconds", "waves", "redo_instances", "states", "successors")
     report, same_all = {}, True

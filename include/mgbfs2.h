@@ -351,6 +351,21 @@ MGBFS2_API int mgbfs2_mlp_rollout_bf16(const void* params_bf16, const float* x_m
  * (crates/mgbfs-runtime/src/generic_memory.rs:82-108). */
 MGBFS2_API int mgbfs2_group_order(const uint32_t* permutations, uint32_t n, uint32_t generators, uint64_t* order);
 
+/* The learned planner's per-graph statics for `count` permutation graphs in
+ * one host call, spread over `threads` host threads (0 = all).  Graph i has
+ * degree[i] <= 20 points and generators[i] >= 1 permutations; the generators
+ * of all graphs are concatenated row-major in `permutations` (graph i's block
+ * is generators[i] x degree[i]), the start labels (dense ids < 256) in
+ * `labels` (degree[i] each).  Writes statics[8i..8i+7] in the layout
+ * mgbfs2_mlp_rollout_bf16 reads (log orbit, n/16, g/8, inverse-closed, mean
+ * and max log generator order, fixed-point and cycle fractions) and states[i]:
+ * |G| (the exact number of states the BFS settles) when the labels are
+ * distinct, else the multinomial n!/prod(c!).  Host only.  No reference
+ * counterpart: the reference's planner is the worst-case bound alone. */
+MGBFS2_API int mgbfs2_graph_statics(uint32_t count, const uint32_t* degree, const uint32_t* generators,
+                                    const uint32_t* permutations, const uint32_t* labels, uint32_t threads,
+                                    float* statics, uint64_t* states);
+
 #ifdef __cplusplus
 }
 #endif

@@ -151,6 +151,8 @@ _SIGNATURES = {
     "mgbfs2_mlp_rollout_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                           C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mgbfs2_group_order": (C.c_int, [C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "mgbfs2_graph_statics": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.c_void_p]),
 }
 
 
@@ -163,6 +165,35 @@ def group_order(generators) -> int:
     out = C.c_uint64()
     check(load().mgbfs2_group_order(flat, n, len(gens), C.byref(out)), "mgbfs2_group_order")
     return int(out.value)
+
+
+def graph_statics(graphs, threads: int = 0):
+    """Planner statics of many permutation graphs in one host call
+    (mgbfs2_graph_statics): a (count, 8) float32 array in the device rollout's
+    layout and a uint64 array of settled-state counts (|G| for distinct
+    labels, else the multinomial bound).  `graphs` are (generators, start)
+    pairs."""
+    import numpy as np
+    degree, gens, perms, labels = [], [], [], []
+    for generators, start in graphs:
+        ids = {}
+        labels.extend(ids.setdefault(v, len(ids)) for v in start)
+        degree.append(len(start))
+        gens.append(len(generators))
+        for g in generators:
+            perms.extend(g)
+    count = len(degree)
+    statics = np.zeros((count, 8), dtype=np.float32)
+    states = np.zeros(count, dtype=np.uint64)
+    if not count:
+        return statics, states
+    d = np.asarray(degree, dtype=np.uint32)
+    k = np.asarray(gens, dtype=np.uint32)
+    p = np.asarray(perms, dtype=np.uint32)
+    lab = np.asarray(labels, dtype=np.uint32)
+    check(load().mgbfs2_graph_statics(count, d.ctypes.data, k.ctypes.data, p.ctypes.data, lab.ctypes.data, threads,
+                                      statics.ctypes.data, states.ctypes.data), "mgbfs2_graph_statics")
+    return statics, states
 
 
 def exported_symbols():

@@ -272,18 +272,27 @@ def rollout(net: PlannerNet, graphs, max_depth=512):
     return layers
 
 
-def rollout_device(net: PlannerNet, graphs, max_depth=512):
+def batch_statics(graphs):
+    """(statics, states) of many graphs in one native call
+    (mgbfs2_graph_statics, host threads): statics is a (count, 8) float32
+    array in the device rollout's layout, equal to `graph_statics` row by row,
+    and states the settled-state count of each graph (|G| for distinct labels,
+    else the multinomial bound)."""
+    return native.graph_statics([(g["action"]["generators"], g["start"]) for g in graphs])
+
+
+def rollout_device(net: PlannerNet, graphs, max_depth=512, statics=None):
     """(peak, total, depth) of every graph's predicted profile, from one
     launch of the device rollout kernel (mgbfs2_mlp_rollout_bf16): the same
     features and bf16 network as `rollout`, with the depth loop on the GPU, so
-    predicting a whole sweep costs one launch instead of one per depth."""
+    predicting a whole sweep costs one launch instead of one per depth.
+    `statics` is `batch_statics(graphs)[0]` when the caller has it."""
     t = net.torch
-    stats = [graph_statics(g["action"]["generators"], g["start"]) for g in graphs]
-    m = len(stats)
-    static = t.tensor([[st.log_orbit, st.n / 16.0, st.gens / 8.0, float(st.inverse_closed), st.mean_log_order,
-                        st.max_log_order, st.fixed_fraction, st.cycle_fraction] for st in stats],
-                      dtype=t.float32, device=net.dev).reshape(m, 8).contiguous()
-    gens = t.tensor([float(st.gens) for st in stats], dtype=t.float32, device=net.dev)
+    if statics is None:
+        statics = batch_statics(graphs)[0]
+    m = len(statics)
+    static = t.from_numpy(statics).to(net.dev).contiguous()
+    gens = (static[:, 2] * 8.0).contiguous()
     mean = t.tensor(net.x_mean, dtype=t.float32, device=net.dev)
     scale = t.tensor(net.x_scale, dtype=t.float32, device=net.dev)
     q = t.empty(net.count, dtype=t.bfloat16, device=net.dev)
@@ -303,9 +312,9 @@ def predicted_capacities(net: PlannerNet, graphs, margin=1.5, floor=4096):
     margin + floor, from the device rollout), never above the exact state count
     |G| (the sweep's instances have distinct labels), which no layer can
     exceed."""
-    peaks, _, _ = rollout_device(net, graphs)
-    return [int(min(group_order(g["action"]["generators"]), peak * margin + floor))
-            for g, peak in zip(graphs, peaks)]
+    statics, states = batch_statics(graphs)
+    peaks, _, _ = rollout_device(net, graphs, statics=statics)
+    return [int(min(int(s), peak * margin + floor)) for s, peak in zip(states, peaks)]
 
 
 def calibrate_margin(net: PlannerNet, graphs, tables, quantile=0.97, slack=1.1) -> float:

@@ -57,3 +57,90 @@ def test_matches_oracle_state_counts_on_seeded_sweep():
             assert order == sum(sizes)
             seen_proper += order < math.factorial(len(start)) // 2
     assert seen_proper > 0
+
+
+def _closure(gens, n):
+    """|<gens>| by enumerating the group (small n only)."""
+    ident = tuple(range(n))
+    seen, frontier = {ident}, [ident]
+    while frontier:
+        nxt = []
+        for a in frontier:
+            for g in gens:
+                c = tuple(g[a[i]] for i in range(n))
+                if c not in seen:
+                    seen.add(c)
+                    nxt.append(c)
+        frontier = nxt
+    return len(seen)
+
+
+def _mobius(p, a, b, c, d):
+    """x -> (a x + b) / (c x + d) on the projective line over F_p (p = infinity)."""
+    out = []
+    for x in range(p + 1):
+        num, den = (a, c) if x == p else ((a * x + b) % p, (c * x + d) % p)
+        out.append(p if den % p == 0 else num * pow(den, -1, p) % p)
+    return out
+
+
+def test_primitive_groups_that_are_not_alternating():
+    # Primitive groups with prime cycles longer than n - 3 only (no Jordan
+    # certificate), which must take the Schreier-Sims path.
+    cases = [
+        ([_mobius(5, 1, 1, 0, 1), _mobius(5, 2, 0, 0, 1), _mobius(5, 0, 1, 1, 0)], 6, 120),  # PGL(2,5)
+        ([_mobius(7, 1, 1, 0, 1), _mobius(7, 2, 0, 0, 1), _mobius(7, 0, 6, 1, 0)], 8, 168),  # PSL(2,7)
+        ([_mobius(7, 1, 1, 0, 1), _mobius(7, 3, 0, 0, 1), _mobius(7, 0, 1, 1, 0)], 8, 336),  # PGL(2,7)
+        ([[(x + 1) % 7 for x in range(7)], [(3 * x) % 7 for x in range(7)]], 7, 42),        # AGL(1,7)
+        ([[(x + 1) % 7 for x in range(7)], [(2 * x) % 7 for x in range(7)]], 7, 21),
+    ]
+    for gens, n, order in cases:
+        assert _closure(gens, n) == order
+        assert native.group_order(gens) == order
+
+
+def test_matches_enumeration_on_random_generator_sets():
+    # Symmetric, alternating, intransitive (common fixed points, two orbits)
+    # and imprimitive (block-preserving) groups.
+    import random
+    rng = random.Random(20261203)
+    for trial in range(240):
+        n = rng.randint(2, 7)
+        fixed = rng.randint(0, 2) if n > 3 else 0
+        m = n - fixed
+        gens = []
+        for _ in range(rng.randint(1, 3)):
+            mode = rng.random()
+            q = list(range(m))
+            if mode < 0.4:
+                rng.shuffle(q)
+            elif mode < 0.7 and m >= 4:
+                h = m // 2
+                a, b = list(range(h)), list(range(h, m))
+                rng.shuffle(a)
+                rng.shuffle(b)
+                q = a + b
+            elif m % 2 == 0:
+                blocks = list(range(m // 2))
+                rng.shuffle(blocks)
+                for i, bi in enumerate(blocks):
+                    flip = rng.random() < 0.5
+                    q[2 * i], q[2 * i + 1] = (2 * bi + flip, 2 * bi + 1 - flip)
+            gens.append(q + list(range(m, n)))
+        assert native.group_order(gens) == _closure(gens, n), gens
+
+
+def test_batched_statics_match_the_python_planner():
+    from multigpubfs_b200 import planner
+    graphs = [workloads.sweep_instance(i, closed) for i in range(40) for closed in (False, True)]
+    graphs += [workloads.planner_instance(i) for i in range(4)]
+    graphs.append({"action": {"generators": [[1, 0, 2, 3, 4], [1, 2, 3, 4, 0]]}, "start": [7, 7, 3, 3, 9]})
+    statics, states = planner.batch_statics(graphs)
+    for row, st_count, g in zip(statics, states, graphs):
+        st = planner.graph_statics(g["action"]["generators"], g["start"])
+        ref = [st.log_orbit, st.n / 16.0, st.gens / 8.0, float(st.inverse_closed), st.mean_log_order,
+               st.max_log_order, st.fixed_fraction, st.cycle_fraction]
+        assert [float(x) for x in row] == [float(__import__("numpy").float32(x)) for x in ref]
+        if len(set(g["start"])) == len(g["start"]):
+            assert int(st_count) == native.group_order(g["action"]["generators"])
+    assert int(states[-1]) == 30  # 5! / (2! 2! 1!)
