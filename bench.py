@@ -222,7 +222,8 @@ def bench_sweep(args, local):
 def bench_planner(args, local):
     """Learned vs plain planner on batched sweeps.  The network is fitted by
     the library's kernels on 4/5 of the layer tables of the 512-instance sweep
-    and its capacity margin is calibrated on the other 1/5.  The plain run
+    plus 32 S11 / S12 instances on other seeds, and its capacity margin is
+    calibrated on the other 1/5.  The plain run
     reserves each instance's orbit bound n!, the learned run its predicted peak
     times the margin (exact rerun on overflow); both must give identical
     tables.  Scenarios: 128 S12 instances with the whole device, and a
@@ -236,7 +237,10 @@ def bench_planner(args, local):
                                           training_set)
     torch.cuda.set_device(local)
     t0 = time.perf_counter()
-    train = workloads.sweep(512)
+    # Layer tables the BFS generates: the 512-instance sweep (n in 7..10) and
+    # 32 S11 / S12 instances on seeds disjoint from the scenarios' instances.
+    train = workloads.sweep(512) + [workloads.planner_instance(i, n=n, seed_base=20261204 + 50000 + 100 * n)
+                                    for n in (11, 12) for i in range(16)]
     with BatchSweep(train, local) as sw:
         sw.run()
         tables = sw.layer_tables()
