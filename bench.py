@@ -198,9 +198,9 @@ def bench_sweep(args, local):
     graphs = workloads.sweep(512)
     with BatchSweep(graphs, local) as sweep:
         for _ in range(args.warmup):
-            sweep.run()
+            sweep.run(host_loop=args.host_loop)
         ref = sweep.layer_tables()
-        runs = [sweep.run() for _ in range(args.steps)]
+        runs = [sweep.run(host_loop=args.host_loop) for _ in range(args.steps)]
         assert sweep.layer_tables() == ref
     dev = sum(r["device_seconds"] for r in runs) / len(runs)
     succ, states = runs[0]["successors"], runs[0]["states"]
@@ -313,6 +313,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["native", "reference"], default="native")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep512", "planner-s12"], default="s13-lrx")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="layers as separate kernel launches with a host round trip each (for a profiler); "
+                         "by default a wave of the sweep, or a fused BFS, is one CUDA-graph launch")
     ap.add_argument("--instances", type=int, default=128, help="planner-s12: number of S12 instances")
     ap.add_argument("--dedup", default=None)
     ap.add_argument("--visited", default=None)
@@ -350,7 +353,7 @@ def main():
 
     # ---- value: resident engine, K whole BFS runs ------------------------------------
     eng = NativeGraph(graph, local)
-    plan = eng.plan(visited=visited, dedup=dedup)
+    plan = eng.plan(visited=visited, dedup=dedup, host_loop=args.host_loop)
     for _ in range(args.warmup):
         r = eng.run()
         assert r.layer_sizes == expect, "layer table mismatch in warm-up"
@@ -391,7 +394,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         with NativeGraph(graph, local) as e:
-            e.plan(visited=visited, dedup=dedup)
+            e.plan(visited=visited, dedup=dedup, host_loop=args.host_loop)
             r = e.run()
             sizes, _ = e.layer_table()
             cur = e.sample(0, 1000)

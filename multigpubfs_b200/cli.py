@@ -55,6 +55,9 @@ def main(argv=None) -> int:
     ap.add_argument("--max-seconds", type=int, default=None)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="one host round trip per layer instead of the whole BFS as one CUDA graph "
+                         "(each layer is then a separate launch, e.g. for a profiler)")
     a = ap.parse_args(argv)
     graph = family(a.graph)
     if a.out:
@@ -66,7 +69,7 @@ def main(argv=None) -> int:
     from .engine import NativeGraph
     with NativeGraph(graph, a.device) as engine:
         plan = engine.plan(visited=a.visited, dedup=a.dedup, capacity=a.capacity, planner=a.planner,
-                           shards=a.shards)
+                           shards=a.shards, host_loop=a.host_loop)
         if a.verb == "plan":
             print(json.dumps({"graph": graph.name, "digest": graph.digest(), "plan": plan}))
             return 0
