@@ -12,10 +12,10 @@
 //                neighbouring groups at a time and the target groups they
 //                share are revisited while still in L2;
 //   per parent = apply each generator, rank the child, atomicOr its bit;
-//   per winner = stage (state, group of the child, rank within the block's
-//                group run) in shared memory; a flush reserves one range per
-//                (block, group) and writes the runs to the next frontier's
-//                group regions.
+//   per winner = stage (state, the slot of the child's group in the block's
+//                group table, rank within that slot's run) in shared memory;
+//                a flush reserves one range per (block, group) and writes
+//                the runs to the next frontier's group regions.
 //
 // With generators that move only a few leading positions into or out of the
 // first K (LRX, adjacent transpositions), the children of one parent group
@@ -37,7 +37,7 @@ namespace mgbfs2 {
 
 constexpr uint32_t kGroupStage = 1024;  // staged winners per block (one pass of 256 x 4 parents)
 constexpr int kGroupBlocksPerSM = 8;    // resident blocks the shared-memory carveout is sized for
-constexpr uint32_t kMaxGroups = 1728;   // 13!/10! = 1716 groups at most
+constexpr uint32_t kMaxGroups = 1728;   // region tables: 13!/10! = 1716 groups at most
 constexpr uint32_t kGroupChunk = 4096;  // parents per work item
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
 static_assert(kGroupStage >= kBlock * 4, "a pass stages up to kBlock * ppt winners, ppt <= 4");
@@ -75,7 +75,6 @@ struct GroupedParams {
 // group finds no slot (a full table) is staged with kNoSlot and written to
 // the spill region.
 constexpr uint32_t kGroupSlots = 256;
-constexpr int kClaimBatch = 1;  // children a thread claims before staging any of them
 constexpr uint32_t kEmptySlot = 0xffffffffu;
 constexpr uint16_t kNoSlot = 0xffff;
 static_assert(kGroupSlots == 256, "group_slot hashes to the top 8 bits");
@@ -245,97 +244,80 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
         const uint32_t pending = sm.count, slots_used = sm.nused;
         __syncthreads();
         if (pending + round > kGroupStage || slots_used > kGroupSlots / 2) grouped_flush(p, sm);
-        // Claim kClaimBatch children per thread before looking at any result:
-        // their bitmap atomics are in flight together.
 #pragma unroll
-        for (int k0 = 0; k0 < 4; k0 += kClaimBatch) {
-          bool won_v[kClaimBatch];
-          uint64_t child_v[kClaimBatch];
-          uint32_t grp_v[kClaimBatch];
-#pragma unroll
-          for (int kk = 0; kk < kClaimBatch; ++kk) {
-            const int k = k0 + kk;
-            const uint32_t g = j + (j >= skip[k] ? 1u : 0u);
-            const bool live = val[k] && g < p.gens;
-            const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
-            bool won = false;
-            uint64_t c = 0;
-            uint32_t grp = 0;
-            if (live && TRANSP) {
-              // Swapping positions t-1 and t changes only those two Lehmer
-              // digits: with a, b the two symbols and c1, c2 their digits,
-              // the new digits are c2 + [a < b] and c1 - [b < a].
-              const uint32_t* ti = transp + 5 * g;
-              const uint32_t t = ti[0];
-              const uint32_t a = static_cast<uint32_t>(par[k] >> (4 * (t - 1))) & 15u;
-              const uint32_t b = static_cast<uint32_t>(par[k] >> (4 * t)) & 15u;
-              const unsigned long long x = static_cast<unsigned long long>(a ^ b);
-              c = (par[k] ^ (x << (4 * (t - 1))) ^ (x << (4 * t))) & ((1ull << (4 * N)) - 1ull);
-              const int c1 = static_cast<int>((pdig[k] >> (4 * (t - 1))) & 15u);
-              const int c2 = static_cast<int>((pdig[k] >> (4 * t)) & 15u);
-              const int lt = a < b ? 1 : 0;
-              const int d1 = c2 + lt - c1, d2 = c1 - (1 - lt) - c2;
-              grp = static_cast<uint32_t>(static_cast<int>(pgrp[k]) + d1 * static_cast<int>(ti[1]) +
-                                          d2 * static_cast<int>(ti[2]));
-              const uint32_t inner = static_cast<uint32_t>(static_cast<int>(pinner[k]) + d1 * static_cast<int>(ti[3]) +
-                                                           d2 * static_cast<int>(ti[4]));
-              if (grp < p.groups && inner < kGroupSize) {
-                const uint32_t bit = 1u << (inner & 31);
-                unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
-                                     (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
-                won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
-              } else {
-                raise_error(&p.control->error, ERR_RANK_RANGE);
-              }
-            } else if (live) {
-              c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
-              if constexpr (kSplitRank) {
-                // Group = the first K Lehmer digits, and the rank inside the group
-                // in 32 bits; (N-K)! is a multiple of 32, so group regions start
-                // on 32-bit words and the claim is a 32-bit atomicOr.
-                uint32_t inner = 0;
-                lehmer_split4<N, K>(c, &grp, &inner);
-                const uint32_t bit = 1u << (inner & 31);
-                unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
-                                     (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
-                won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
-              } else {
-                const uint64_t r = lehmer_rank4<N>(c);
-                const unsigned long long bit = 1ull << (r & 63);
-                won = !(atomic_or_hinted(&p.bitmap[r >> 6], bit, l2_policy_evict_last()) & bit);
-                grp = static_cast<uint32_t>(r / kGroupSize);
-              }
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t g = j + (j >= skip[k] ? 1u : 0u);
+          const bool live = val[k] && g < p.gens;
+          const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
+          bool won = false;
+          uint64_t c = 0;
+          uint32_t grp = 0;
+          if (live && TRANSP) {
+            // Swapping positions t-1 and t changes only those two Lehmer
+            // digits: with a, b the two symbols and c1, c2 their digits,
+            // the new digits are c2 + [a < b] and c1 - [b < a].
+            const uint32_t* ti = transp + 5 * g;
+            const uint32_t t = ti[0];
+            const uint32_t a = static_cast<uint32_t>(par[k] >> (4 * (t - 1))) & 15u;
+            const uint32_t b = static_cast<uint32_t>(par[k] >> (4 * t)) & 15u;
+            const unsigned long long x = static_cast<unsigned long long>(a ^ b);
+            c = (par[k] ^ (x << (4 * (t - 1))) ^ (x << (4 * t))) & ((1ull << (4 * N)) - 1ull);
+            const int c1 = static_cast<int>((pdig[k] >> (4 * (t - 1))) & 15u);
+            const int c2 = static_cast<int>((pdig[k] >> (4 * t)) & 15u);
+            const int lt = a < b ? 1 : 0;
+            const int d1 = c2 + lt - c1, d2 = c1 - (1 - lt) - c2;
+            grp = static_cast<uint32_t>(static_cast<int>(pgrp[k]) + d1 * static_cast<int>(ti[1]) +
+                                        d2 * static_cast<int>(ti[2]));
+            const uint32_t inner = static_cast<uint32_t>(static_cast<int>(pinner[k]) + d1 * static_cast<int>(ti[3]) +
+                                                         d2 * static_cast<int>(ti[4]));
+            if (grp < p.groups && inner < kGroupSize) {
+              const uint32_t bit = 1u << (inner & 31);
+              unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
+                                   (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
+              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+            } else {
+              raise_error(&p.control->error, ERR_RANK_RANGE);
             }
-            won_v[kk] = won;
-            child_v[kk] = c | gtag;
-            grp_v[kk] = grp;
+          } else if (live) {
+            c = apply_terms(par[k], terms, tbegin[g], tbegin[g + 1]);
+            if constexpr (kSplitRank) {
+              // Group = the first K Lehmer digits, and the rank inside the group
+              // in 32 bits; (N-K)! is a multiple of 32, so group regions start
+              // on 32-bit words and the claim is a 32-bit atomicOr.
+              uint32_t inner = 0;
+              lehmer_split4<N, K>(c, &grp, &inner);
+              const uint32_t bit = 1u << (inner & 31);
+              unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
+                                   (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
+              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+            } else {
+              const uint64_t r = lehmer_rank4<N>(c);
+              const unsigned long long bit = 1ull << (r & 63);
+              won = !(atomic_or_hinted(&p.bitmap[r >> 6], bit, l2_policy_evict_last()) & bit);
+              grp = static_cast<uint32_t>(r / kGroupSize);
+            }
           }
-#pragma unroll
-          for (int kk = 0; kk < kClaimBatch; ++kk) {
-            const bool won = won_v[kk];
-            const uint32_t grp = grp_v[kk];
-            const unsigned m = __ballot_sync(kFullMask, won);
-            if (m) {
-              const int leader = __ffs(m) - 1;
-              uint32_t base = 0;
-              if (static_cast<int>(lane) == leader) base = atomicAdd(&sm.count, static_cast<uint32_t>(__popc(m)));
-              base = __shfl_sync(kFullMask, base, leader);
-              if (won) {
-                const unsigned peers = __match_any_sync(m, grp);
-                const int gl = __ffs(peers) - 1;
-                uint32_t packed = 0;  // slot | first rank << 16 (ranks stay below kGroupStage)
-                if (static_cast<int>(lane) == gl) {
-                  const int gs = group_slot(sm, grp);
-                  packed = gs < 0 ? kNoSlot
-                                  : (static_cast<uint32_t>(gs) |
-                                     atomicAdd(&sm.scnt[gs], static_cast<uint32_t>(__popc(peers))) << 16);
-                }
-                packed = __shfl_sync(peers, packed, gl);
-                const uint32_t at = base + __popc(m & lanemask_lt());
-                sm.state[at] = child_v[kk];
-                sm.slot[at] = static_cast<uint16_t>(packed & 0xffffu);
-                sm.rank[at] = static_cast<uint16_t>((packed >> 16) + __popc(peers & lanemask_lt()));
+          const unsigned m = __ballot_sync(kFullMask, won);
+          if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(&sm.count, static_cast<uint32_t>(__popc(m)));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (won) {
+              const unsigned peers = __match_any_sync(m, grp);
+              const int gl = __ffs(peers) - 1;
+              uint32_t packed = 0;  // slot | first rank << 16 (ranks stay below kGroupStage)
+              if (static_cast<int>(lane) == gl) {
+                const int gs = group_slot(sm, grp);
+                packed = gs < 0 ? kNoSlot
+                                : (static_cast<uint32_t>(gs) |
+                                   atomicAdd(&sm.scnt[gs], static_cast<uint32_t>(__popc(peers))) << 16);
               }
+              packed = __shfl_sync(peers, packed, gl);
+              const uint32_t at = base + __popc(m & lanemask_lt());
+              sm.state[at] = c | gtag;
+              sm.slot[at] = static_cast<uint16_t>(packed & 0xffffu);
+              sm.rank[at] = static_cast<uint16_t>((packed >> 16) + __popc(peers & lanemask_lt()));
             }
           }
         }
