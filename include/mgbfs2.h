@@ -268,14 +268,15 @@ MGBFS2_API int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t gener
                                                  void* stream);
 
 /* ------------------------------------------------------------------------ */
-/* Batched sweep: many BFS instances in one device-driven CUDA-graph loop.   */
+/* Batched sweep: many BFS instances, each wave one persistent launch.       */
 
 typedef struct mgbfs2_batch mgbfs2_batch;
 
 typedef struct {
   uint32_t max_depth;       /* layer-table capacity per instance, 0 = 1024 */
   uint32_t blocks_per_sm;   /* batch_expand blocks per SM, 0 = occupancy limit (the tuned shape) */
-  uint32_t host_loop;       /* 1 = host-driven layer loop (one sync per layer) instead of the graph loop */
+  uint32_t host_loop;       /* layer loop of a wave: 0 = one persistent cooperative launch (grid barriers
+                               between layers), 1 = host-driven (one sync per layer), 2 = CUDA-graph WHILE loop */
   uint32_t reserved;
   uint64_t memory_bytes;    /* device bytes available to the waves, 0 = free memory minus reserve */
   uint64_t reserve_bytes;   /* 0 = 2 GiB */

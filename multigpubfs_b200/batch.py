@@ -65,10 +65,17 @@ class BatchSweep:
     def __exit__(self, *exc):
         self.close()
 
-    def run(self, *, capacities=None, memory_bytes=None, max_depth=None, host_loop=False, blocks_per_sm=None) -> dict:
+    def run(self, *, capacities=None, memory_bytes=None, max_depth=None, host_loop=False, graph_loop=False,
+            blocks_per_sm=None) -> dict:
+        """Runs every instance to completion.  Each wave is one persistent
+        cooperative launch by default; `host_loop` launches every layer step
+        from the host (one sync per layer, e.g. for a profiler) and
+        `graph_loop` runs the steps as a CUDA-graph WHILE loop."""
+        if host_loop and graph_loop:
+            raise ValueError("host_loop and graph_loop are exclusive")
         opts = native.BatchOptions()
         opts.max_depth = max_depth or 0
-        opts.host_loop = 1 if host_loop else 0
+        opts.host_loop = 1 if host_loop else (2 if graph_loop else 0)
         opts.memory_bytes = memory_bytes or 0
         opts.blocks_per_sm = blocks_per_sm or 0
         keep = None

@@ -42,6 +42,8 @@ namespace {
 
 constexpr uint32_t kBatchBlock = 256;
 constexpr int kBatchBlocksPerSM = 4;   // default resident batch_expand blocks per SM
+// Layer loop of a wave (mgbfs2_batch_options.host_loop): persistent, host (1) or graph.
+constexpr uint32_t kLoopPersistent = 0, kLoopGraph = 2;
 constexpr uint32_t kBatchPpt = 4;                         // frontier entries per thread per tile
 constexpr uint32_t kBatchTile = kBatchBlock * kBatchPpt;  // entries per tile (one instance per tile)
 constexpr uint32_t kBatchOut = 4096;                      // winners staged in shared memory per block
@@ -62,6 +64,7 @@ struct BatchCtl {
   unsigned long long tiles;      // tiles of the current frontier (tile_prefix[count])
   unsigned long long next_tile;  // work counter of batch_expand, reset by every finalize
   uint32_t parity, depth, max_depth, error;
+  uint32_t bar_count, bar_gen;   // grid barrier of the persistent wave kernel (zero at the wave's start)
 };
 
 struct BatchParams {
@@ -294,8 +297,7 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
 // search of the tile prefix, loads that
 // instance's generator program into shared memory when it changes, and
 // stages its winners for one segment reservation per flush.
-__global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
-  __shared__ BatchSmem s;
+__device__ __forceinline__ void expand_layer(const BatchParams& p, BatchSmem& s) {
   const uint32_t parity = p.ctl->parity;
   const unsigned long long tiles = p.ctl->tiles;
   // Select, not index: a runtime index into the parameter block would copy it
@@ -360,15 +362,23 @@ __global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
   }
 }
 
+__global__ void __launch_bounds__(kBatchBlock) batch_expand(BatchParams p) {
+  __shared__ BatchSmem s;
+  expand_layer(p, s);
+}
+
+
 // One block: record the layer, retire finished or overflowed instances, build
-// the prefix of the new per-instance tile counts, flip the buffers, decide
-// whether to loop.
-__global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphConditionalHandle handle,
-                                                       int use_handle) {
-  __shared__ unsigned long long warp_sums[32];
-  __shared__ unsigned long long carry, entries;
+// the prefix of the new per-instance tile counts, flip the buffers.  Returns
+// the new frontier's tile count (0 ends the wave).
+struct FinalizeSmem {
+  unsigned long long warp_sums[32];
+  unsigned long long carry, entries;
+};
+
+__device__ unsigned long long finalize_layer(const BatchParams& p, FinalizeSmem& f) {
   const uint32_t depth = p.ctl->depth;
-  if (threadIdx.x == 0) carry = entries = 0;
+  if (threadIdx.x == 0) f.carry = f.entries = 0;
   __syncthreads();
   for (uint32_t base = 0; base < p.count; base += blockDim.x) {
     const uint32_t i = base + threadIdx.x;
@@ -388,7 +398,7 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
         } else {
           p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth + depth + 1] = produced;
           c = (produced + kBatchTile - 1) / kBatchTile;
-          atomicAdd(&entries, produced);
+          atomicAdd(&f.entries, produced);
         }
       }
       p.cur_count[i] = c ? produced : 0ull;
@@ -401,31 +411,98 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
       const unsigned long long up = __shfl_up_sync(kFullMask, incl, o);
       if (lane >= static_cast<uint32_t>(o)) incl += up;
     }
-    if (lane == 31) warp_sums[warp] = incl;
+    if (lane == 31) f.warp_sums[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-      unsigned long long v = lane < blockDim.x / 32 ? warp_sums[lane] : 0ull, x = v;
+      unsigned long long v = lane < blockDim.x / 32 ? f.warp_sums[lane] : 0ull, x = v;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const unsigned long long up = __shfl_up_sync(kFullMask, x, o);
         if (lane >= static_cast<uint32_t>(o)) x += up;
       }
-      if (lane < blockDim.x / 32) warp_sums[lane] = x - v;
+      if (lane < blockDim.x / 32) f.warp_sums[lane] = x - v;
     }
     __syncthreads();
-    if (i < p.count) p.tile_prefix[i] = carry + warp_sums[warp] + incl - c;
+    if (i < p.count) p.tile_prefix[i] = f.carry + f.warp_sums[warp] + incl - c;
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry += warp_sums[warp] + incl;
+    if (threadIdx.x == blockDim.x - 1) f.carry += f.warp_sums[warp] + incl;
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    p.tile_prefix[p.count] = carry;
-    p.ctl->tiles = carry;
+    p.tile_prefix[p.count] = f.carry;
+    p.ctl->tiles = f.carry;
     p.ctl->next_tile = 0;
-    p.ctl->total = entries;
+    p.ctl->total = f.entries;
     p.ctl->parity ^= 1u;
     p.ctl->depth = depth + 1;
-    if (use_handle) cudaGraphSetConditional(handle, carry > 0 ? 1u : 0u);
+  }
+  __syncthreads();
+  return f.carry;
+}
+
+// The finalize step as its own one-block launch (graph and host loops); in
+// the graph loop it also sets the WHILE node's condition.
+__global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphConditionalHandle handle,
+                                                       int use_handle) {
+  __shared__ FinalizeSmem f;
+  const unsigned long long tiles = finalize_layer(p, f);
+  if (use_handle && threadIdx.x == 0) cudaGraphSetConditional(handle, tiles > 0 ? 1u : 0u);
+}
+
+constexpr uint32_t kBarrierPolls = 1u << 22;
+
+// Grid-wide barrier of the cooperative wave kernel, with a bounded wait.
+// Thread 0 of each block arrives on ctl->bar_count; the last to arrive resets
+// it and advances ctl->bar_gen with a release store; the others poll bar_gen
+// with acquire loads, at most kBarrierPolls times, after which they raise
+// ERR_WAIT_LIMIT and return false (the kernel then ends; nothing waits
+// forever).  Every thread orders its later loads after the barrier.
+__device__ bool grid_barrier(BatchCtl* ctl) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    unsigned gen;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(&ctl->bar_gen) : "memory");
+    __threadfence();
+    if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
+      ctl->bar_count = 0;
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&ctl->bar_gen), "r"(gen + 1) : "memory");
+    } else {
+      for (uint32_t polls = 0;; ++polls) {
+        unsigned now;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(&ctl->bar_gen) : "memory");
+        if (now != gen) break;
+        if (polls >= kBarrierPolls) {
+          atomicOr(&ctl->error, ERR_WAIT_LIMIT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  __syncthreads();
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+  return ok != 0;
+}
+
+// A whole wave in one cooperative launch: every block expands its tiles of
+// the layer, a grid barrier, block 0 finalizes, a second barrier, and all
+// blocks go on while the new frontier has tiles.  Two barriers per layer
+// replace two kernel launches per layer.
+__global__ void __launch_bounds__(kBatchBlock) batch_wave(BatchParams p) {
+  __shared__ BatchSmem s;
+  __shared__ FinalizeSmem f;
+  __shared__ int more;
+  for (;;) {
+    expand_layer(p, s);
+    if (!grid_barrier(p.ctl)) return;
+    if (blockIdx.x == 0) finalize_layer(p, f);
+    if (!grid_barrier(p.ctl)) return;
+    if (threadIdx.x == 0) more = *reinterpret_cast<volatile unsigned long long*>(&p.ctl->tiles) > 0;
+    __syncthreads();
+    if (!more) return;
   }
 }
 
@@ -590,7 +667,7 @@ static int batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int dev
 
 // Runs one wave (the instances in `ids`, with segment capacities `caps`).
 static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& caps, uint32_t max_depth,
-                    uint32_t ppt, bool use_graph, mgbfs2_batch_status* st, double* kernel_seconds) {
+                    uint32_t ppt, uint32_t loop, mgbfs2_batch_status* st, double* kernel_seconds) {
   const uint32_t W = static_cast<uint32_t>(ids.size());
   std::vector<BatchInst> host(W);
   std::vector<Term> terms;
@@ -678,7 +755,28 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   cudaEventCreate(&e1);
   cudaEventRecord(e0, b->stream);
   uint32_t layers_run = 0;
-  if (use_graph) {
+  if (loop == kLoopPersistent) {
+    // One cooperative launch; its grid must be co-resident, so it is sized by
+    // the occupancy of batch_wave itself under the carveout set above.
+    const int want = ppt ? static_cast<int>(ppt) : kBatchBlocksPerSM;
+    int wave_sm = size_carveout(reinterpret_cast<const void*>(batch_wave), 0, want, kBatchBlock);
+    int resident = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, batch_wave, kBatchBlock, 0) != cudaSuccess) {
+      cudaGetLastError();
+      resident = 1;
+    }
+    wave_sm = std::max(1, std::min(wave_sm, resident));
+    void* args[] = {&p};
+    cudaError_t e = cudaErrorCooperativeLaunchTooLarge;
+    for (; wave_sm >= 1 && e == cudaErrorCooperativeLaunchTooLarge; --wave_sm) {
+      e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(batch_wave), dim3(wave_sm * b->sm_count),
+                                      dim3(kBatchBlock), args, 0, b->stream);
+      if (e == cudaErrorCooperativeLaunchTooLarge) cudaGetLastError();
+    }
+    MG_CHECK_BATCH(e);
+    ++st->kernel_launches;
+    MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
+  } else if (loop == kLoopGraph) {
     cudaGraph_t graph;
     MG_CHECK_BATCH(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle handle;
@@ -732,7 +830,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   MG_CHECK_BATCH(cudaMemcpyAsync(layers.data(), p.layers, layers.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
-  if (use_graph) st->kernel_launches += 2 * hc.depth;
+  if (loop == kLoopGraph) st->kernel_launches += 2 * hc.depth;
   st->layer_steps += hc.depth;
   for (uint32_t k = 0; k < W; ++k) {
     auto& in = b->inst[ids[k]];
@@ -777,7 +875,8 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
   if (options) o = *options;
   const uint32_t max_depth = o.max_depth ? o.max_depth : 1024;
   const uint32_t ppt = o.blocks_per_sm;
-  const bool use_graph = o.host_loop == 0;
+  const uint32_t loop = o.host_loop;
+  if (loop > kLoopGraph) return MGBFS2_INVALID_ARGUMENT;
   MG_CHECK_BATCH(cudaSetDevice(b->device));
   size_t free_bytes = 0, total_bytes = 0;
   MG_CHECK_BATCH(cudaMemGetInfo(&free_bytes, &total_bytes));
@@ -819,7 +918,7 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
         later.push_back(i);
       }
     }
-    rc = run_wave(b, wave, caps, max_depth, ppt, use_graph, &st, &kernel_seconds);
+    rc = run_wave(b, wave, caps, max_depth, ppt, loop, &st, &kernel_seconds);
     ++st.waves;
     for (uint32_t i : wave) {
       if (b->inst[i].status == INST_OVERFLOW) {

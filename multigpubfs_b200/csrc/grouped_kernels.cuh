@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
   constexpr bool kSplitRank = N - K >= 8 && N - K <= 12;  // 32-bit in-group rank, word-aligned groups
   static_assert(!TRANSP || kSplitRank, "the incremental-rank path needs the split rank");
   constexpr uint64_t kGroupWords32 = kGroupSize / 32;
+  constexpr uint64_t kStateMask = N >= 16 ? ~0ull : (1ull << (4 * N)) - 1ull;  // the N packed symbols
   const uint32_t tid = threadIdx.x, lane = lane_id();
   const uint32_t round = kBlock * p.ppt;
   const unsigned long long items = __ldg(&p.item_prefix[p.regions]);
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
             const uint32_t a = static_cast<uint32_t>(par[k] >> (4 * (t - 1))) & 15u;
             const uint32_t b = static_cast<uint32_t>(par[k] >> (4 * t)) & 15u;
             const unsigned long long x = static_cast<unsigned long long>(a ^ b);
-            c = (par[k] ^ (x << (4 * (t - 1))) ^ (x << (4 * t))) & ((1ull << (4 * N)) - 1ull);
+            c = (par[k] ^ (x << (4 * (t - 1))) ^ (x << (4 * t))) & kStateMask;
             const int c1 = static_cast<int>((pdig[k] >> (4 * (t - 1))) & 15u);
             const int c2 = static_cast<int>((pdig[k] >> (4 * t)) & 15u);
             const int lt = a < b ? 1 : 0;

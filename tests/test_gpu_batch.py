@@ -2,7 +2,8 @@
 
 Instances follow the sweep definition (n uniform in {7,8,9,10}, 2-3 seeded
 uniform random permutations; directed, and an inverse-closed variant adding
-inverses), run together in one device-driven CUDA-graph loop.
+inverses), run together, each wave as one persistent cooperative launch (or,
+compared, a CUDA-graph WHILE loop or a host-driven loop).
 """
 import pytest
 
@@ -27,22 +28,37 @@ def test_batch_matches_oracle(closed):
     expect = _oracle_tables(graphs)
     with BatchSweep(graphs) as sweep:
         st = sweep.run()
-        assert st["complete_instances"] == 40 and st["graph_launches"] >= 1 and st["redo_instances"] == 0
+        # One wave: its seed and ONE persistent launch for all layers.
+        assert st["complete_instances"] == 40 and st["waves"] == 1 and st["redo_instances"] == 0
+        assert st["graph_launches"] == 0 and st["kernel_launches"] == 2 and st["layer_steps"] > 10
         assert sweep.layer_tables() == expect
         assert st["states"] == sum(map(sum, expect))
 
 
-def test_batch_host_loop_and_graph_loop_agree():
+def test_batch_loop_modes_agree():
     from multigpubfs_b200.batch import BatchSweep
     graphs = _instances(24, True, 777)
     expect = _oracle_tables(graphs)
     with BatchSweep(graphs) as sweep:
         a = sweep.run(host_loop=True)
         ta = sweep.layer_tables()
-        b = sweep.run()
+        b = sweep.run(graph_loop=True)
         tb = sweep.layer_tables()
-    assert ta == tb == expect
-    assert a["graph_launches"] == 0 and b["graph_launches"] >= 1
+        c = sweep.run()
+        tc = sweep.layer_tables()
+        # Several waves: the persistent kernel starts from fresh barrier state
+        # in each.
+        d = sweep.run(memory_bytes=96 << 20)
+        td = sweep.layer_tables()
+    assert ta == tb == tc == td == expect
+    assert a["graph_launches"] == 0 and b["graph_launches"] >= 1 and c["graph_launches"] == 0
+    assert c["kernel_launches"] == 2 * c["waves"] and d["waves"] > 1 and d["kernel_launches"] == 2 * d["waves"]
+    with pytest.raises(ValueError):
+        sweep_opts = BatchSweep(graphs)
+        try:
+            sweep_opts.run(host_loop=True, graph_loop=True)
+        finally:
+            sweep_opts.close()
 
 
 def test_batch_overflow_reruns_exactly_and_waves():
