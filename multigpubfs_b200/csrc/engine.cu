@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -131,8 +132,8 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
     rc = cuda_status(cudaEventCreate(e));
     if (rc) { set_message(error, cap, "CUDA_EVENT"); delete g; return rc; }
   }
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) g->sm_count = prop.multiProcessorCount;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) g->sm_count = sms;
   g->analyse();
   *out = g;
   return MGBFS2_OK;
@@ -365,25 +366,28 @@ Graph::~Graph() {
 
 void Graph::release() {
   cudaSetDevice(device);
+  // The pinned mirrors go back to the process-wide cache, where another
+  // handle may take them: no copy of this handle's may still be in flight.
+  if (stream) cudaStreamSynchronize(stream);
   for (DeviceBuffer* b : {&bitmap, &front, &next, &table, &bank[0], &bank[1], &bank[2], &program, &control_buf,
                           &scratch})
     b->free();
   wide_release();
   if (host_control) {
-    cudaFreeHost(host_control);
+    pinned_give(host_control);
     host_control = nullptr;
   }
   buckets.free();
   shard_meta.free();
   if (host_meta) {
-    cudaFreeHost(host_meta);
+    pinned_give(host_meta);
     host_meta = nullptr;
   }
   group_meta.free();
   loop_buf.free();
   transp_buf.free();
   if (host_group) {
-    cudaFreeHost(host_group);
+    pinned_give(host_group);
     host_group = nullptr;
   }
   front_grouped = false;
@@ -412,6 +416,51 @@ void DeviceBuffer::free() {
   if (ptr) cudaFreeAsync(ptr, stream);
   ptr = nullptr;
   bytes = 0;
+}
+
+namespace {
+std::mutex pinned_mutex;
+std::multimap<size_t, void*> pinned_free;   // capacity -> idle buffer
+std::map<void*, size_t> pinned_size;        // every buffer the cache made -> capacity
+size_t pinned_idle_bytes = 0;
+constexpr size_t kPinnedIdleLimit = 64ull << 20;
+}  // namespace
+
+int pinned_take(size_t bytes, void** out) {
+  size_t cap = 4096;
+  while (cap < bytes) cap *= 2;
+  {
+    std::lock_guard<std::mutex> lock(pinned_mutex);
+    auto it = pinned_free.find(cap);
+    if (it != pinned_free.end()) {
+      *out = it->second;
+      pinned_free.erase(it);
+      pinned_idle_bytes -= cap;
+      return MGBFS2_OK;
+    }
+  }
+  void* p = nullptr;
+  if (int rc = cuda_status(cudaMallocHost(&p, cap))) return rc;
+  std::lock_guard<std::mutex> lock(pinned_mutex);
+  pinned_size[p] = cap;
+  *out = p;
+  return MGBFS2_OK;
+}
+
+void pinned_give(void* ptr) {
+  if (!ptr) return;
+  std::unique_lock<std::mutex> lock(pinned_mutex);
+  const auto it = pinned_size.find(ptr);
+  if (it == pinned_size.end()) return;
+  const size_t cap = it->second;
+  if (pinned_idle_bytes + cap <= kPinnedIdleLimit) {
+    pinned_free.emplace(cap, ptr);
+    pinned_idle_bytes += cap;
+    return;
+  }
+  pinned_size.erase(it);
+  lock.unlock();
+  cudaFreeHost(ptr);
 }
 
 int retain_pool_memory(int device) {
@@ -583,7 +632,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (p.visited == MGBFS2_VISITED_BITMAP) rc = bitmap.ensure(bitmap_bytes);
   if (!rc) rc = control_buf.ensure(sizeof(Control));
   if (!rc && packed) rc = program.ensure(terms.size() * sizeof(Term) + term_begin.size() * sizeof(uint32_t) + 16);
-  if (!rc && !host_control) rc = cuda_status(cudaMallocHost(&host_control, sizeof(Control)));
+  if (!rc && !host_control) rc = pinned_take(sizeof(Control), reinterpret_cast<void**>(&host_control));
   if (rc) return rc;
   if (packed) {
     MG_CHECK(cudaMemcpyAsync(program.ptr, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, stream));
@@ -822,7 +871,7 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   const uint32_t G = groups, R = groups + 1;
   int rc = MGBFS2_OK;
   const size_t words = group_meta_words(G), bytes = group_meta_bytes(G);
-  if (!host_group && (rc = cuda_status(cudaMallocHost(&host_group, bytes)))) return rc;
+  if (!host_group && (rc = pinned_take(bytes, reinterpret_cast<void**>(&host_group)))) return rc;
   if ((rc = group_meta.ensure(bytes))) return rc;
   uint32_t* order = reinterpret_cast<uint32_t*>(host_group + words);
   unsigned long long* rb = host_group;
@@ -935,7 +984,7 @@ int Graph::bucket_setup(uint64_t work, bool exact) {
   const uint32_t S = bucket_shards;
   int rc = MGBFS2_OK;
   const size_t meta_bytes = (3 * kMaxShards + 1) * sizeof(unsigned long long);
-  if (!host_meta && (rc = cuda_status(cudaMallocHost(&host_meta, meta_bytes)))) return rc;
+  if (!host_meta && (rc = pinned_take(meta_bytes, reinterpret_cast<void**>(&host_meta)))) return rc;
   if ((rc = shard_meta.ensure(meta_bytes))) return rc;
   unsigned long long* begin = host_meta;
   unsigned long long* cap = host_meta + kMaxShards;

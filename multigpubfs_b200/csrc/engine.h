@@ -30,6 +30,11 @@ struct DeviceBuffer {
 };
 
 int retain_pool_memory(int device);
+// Pinned host buffers from a process-wide cache: creating and freeing page-
+// locked memory is slow, and cudaFreeHost synchronises the device, so handles
+// take their small pinned mirrors from the cache and give them back.
+int pinned_take(size_t bytes, void** out);
+void pinned_give(void* ptr);
 uint64_t pool_idle_bytes(int device);
 
 struct WideState;     // int64-key arena path (wide.cu)
