@@ -309,6 +309,14 @@ MGBFS2_API int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options*
 MGBFS2_API int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint64_t* sizes,
                                         size_t capacity, size_t* count);
 
+/* Expansion seconds of each layer of one instance after mgbfs2_batch_run,
+ * aligned with its layer table: entry d >= 1 is the device time (globaltimer)
+ * of the layer step of its wave that produced layer d, shared by every
+ * instance of that wave; entry 0 (the start) is 0.  The per-layer expansion
+ * time of the reference's sweep layers.csv (docs/reproduce-pair-sweeps.md:20). */
+MGBFS2_API int mgbfs2_batch_layer_seconds(const mgbfs2_batch* batch, uint32_t instance, double* seconds,
+                                          size_t capacity, size_t* count);
+
 MGBFS2_API void mgbfs2_batch_destroy(mgbfs2_batch* batch);
 
 /* ------------------------------------------------------------------------ */

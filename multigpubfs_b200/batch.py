@@ -1,18 +1,22 @@
-"""Batched sweep: many BFS instances in one device-driven CUDA-graph loop.
+"""Batched sweep: many BFS instances, each wave one persistent launch.
 
     with BatchSweep(graphs) as sweep:
         status = sweep.run()                 # plain planner: orbit-bound capacities
         tables = sweep.layer_tables()
         status = sweep.run(capacities=[...]) # learned planner: predicted capacities, exact overflow rerun
+        sweep.write_results("out/")          # results.csv, layers.csv, checksums.json
 
 The reference runs such sweeps one graph at a time through a resident worker
 pool (multigpubfs/generic_session.py:139, docs/RESIDENT_SWEEP.md); here one
-mgbfs2_batch_run advances every instance together, a whole wave per graph
-launch.
+mgbfs2_batch_run advances every instance together, a whole wave per launch.
 """
 from __future__ import annotations
 
+import csv
 import ctypes as C
+import hashlib
+import json
+from pathlib import Path
 
 from . import native
 from .graph_definition import GraphDefinition
@@ -99,3 +103,58 @@ class BatchSweep:
 
     def layer_tables(self):
         return [self.layer_table(i) for i in range(self.count)]
+
+    def layer_seconds(self, instance: int):
+        """Per-layer expansion seconds of one instance, aligned with its layer
+        table (entry 0, the start, is 0; entry d is its wave's step that
+        produced layer d)."""
+        count = C.c_size_t()
+        native.check(self.lib.mgbfs2_batch_layer_seconds(self.handle, instance, None, 0, C.byref(count)),
+                     "mgbfs2_batch_layer_seconds")
+        out = (C.c_double * max(count.value, 1))()
+        native.check(self.lib.mgbfs2_batch_layer_seconds(self.handle, instance, out, count.value, C.byref(count)),
+                     "mgbfs2_batch_layer_seconds")
+        return [float(out[i]) for i in range(count.value)]
+
+    def write_results(self, output):
+        """The sweep tables of the last run: see `write_sweep_results`."""
+        names = [g.name or f"instance-{i}" for i, g in enumerate(self.graphs)]
+        degrees = [len(g.start) for g in self.graphs]
+        return write_sweep_results(output, names, degrees, self.layer_tables(),
+                                   [self.layer_seconds(i) for i in range(self.count)])
+
+
+def write_sweep_results(output, names, degrees, tables, seconds):
+    """Writes a sweep's tables in the layout of the reference's sweep outputs
+    (docs/reproduce-pair-sweeps.md:17-23), one row per instance instead of per
+    (n, r) pair:
+
+    - results.csv: instance, name, n, status (COMPLETE / INCOMPLETE), the
+      start's eccentricity when complete, completed depth, visited states,
+      BFS seconds;
+    - layers.csv: instance, depth, state count, cumulative count, expansion
+      seconds (empty for depth zero, which is not expanded);
+    - checksums.json: SHA256 of both files.
+
+    An instance without a table (not completed) is INCOMPLETE with no layers.
+    Returns the checksums."""
+    out = Path(output)
+    out.mkdir(parents=True, exist_ok=True)
+    with open(out / "results.csv", "w", newline="", encoding="utf-8") as f:
+        w = csv.writer(f, lineterminator="\n")
+        w.writerow(["instance", "name", "n", "status", "eccentricity", "completed_depth", "visited", "bfs_seconds"])
+        for i, (name, n, table, secs) in enumerate(zip(names, degrees, tables, seconds)):
+            done = bool(table)
+            w.writerow([i, name, n, "COMPLETE" if done else "INCOMPLETE", len(table) - 1 if done else "",
+                        len(table) - 1 if done else "", sum(table), f"{sum(secs):.9f}"])
+    with open(out / "layers.csv", "w", newline="", encoding="utf-8") as f:
+        w = csv.writer(f, lineterminator="\n")
+        w.writerow(["instance", "depth", "count", "cumulative", "seconds"])
+        for i, (table, secs) in enumerate(zip(tables, seconds)):
+            total = 0
+            for d, count in enumerate(table):
+                total += count
+                w.writerow([i, d, count, total, "" if d == 0 else f"{secs[d]:.9f}"])
+    sums = {name: hashlib.sha256((out / name).read_bytes()).hexdigest() for name in ("results.csv", "layers.csv")}
+    (out / "checksums.json").write_text(json.dumps(sums, indent=1, sort_keys=True) + "\n", encoding="utf-8")
+    return sums

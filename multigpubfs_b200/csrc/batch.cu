@@ -80,6 +80,7 @@ struct BatchParams {
   unsigned long long* cur_count;    // per instance: entries in the current frontier
   unsigned long long* next_count;   // per instance: winners appended to the next frontier
   unsigned long long* layers;       // count x max_depth
+  unsigned long long* stamps;       // max_depth + 1: globaltimer at the seed (0) and after layer step d (d + 1)
   BatchCtl* ctl;
 };
 
@@ -429,6 +430,9 @@ __device__ unsigned long long finalize_layer(const BatchParams& p, FinalizeSmem&
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    if (depth + 1 <= p.ctl->max_depth) p.stamps[depth + 1] = now;
     p.tile_prefix[p.count] = f.carry;
     p.ctl->tiles = f.carry;
     p.ctl->next_tile = 0;
@@ -520,6 +524,9 @@ __global__ void batch_seed(BatchParams p) {
     p.next_count[i] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    p.stamps[0] = now;
     p.tile_prefix[p.count] = p.count;
     p.ctl->tiles = p.count;
     p.ctl->next_tile = 0;
@@ -549,6 +556,7 @@ struct Batch {
     bool inverse_closed = false;
     uint64_t orbit = 0;            // n!
     std::vector<uint64_t> layers;
+    std::vector<double> layer_seconds;  // per layer d >= 1: its wave's expansion of layer d - 1
     uint32_t status = INST_IDLE;
     uint32_t runs = 0;
   };
@@ -707,6 +715,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const size_t o_cur = off; off = al(off + W * 8);
   const size_t o_next = off; off = al(off + W * 8);
   const size_t o_layers = off; off = al(off + static_cast<size_t>(W) * max_depth * 8);
+  const size_t o_stamps = off; off = al(off + (static_cast<size_t>(max_depth) + 1) * 8);
   const size_t o_ctl = off; off = al(off + sizeof(BatchCtl));
   const size_t o_bitmap = off; off = al(off + bitmap_words * 8);
   const size_t o_buf0 = off; off = al(off + seg * 8);
@@ -742,6 +751,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   p.cur_count = reinterpret_cast<unsigned long long*>(base + o_cur);
   p.next_count = reinterpret_cast<unsigned long long*>(base + o_next);
   p.layers = reinterpret_cast<unsigned long long*>(base + o_layers);
+  p.stamps = reinterpret_cast<unsigned long long*>(base + o_stamps);
   p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);
   batch_seed<<<std::max<uint32_t>(1, (W + 255) / 256), 256, 0, b->stream>>>(p);
   ++st->kernel_launches;
@@ -829,6 +839,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   MG_CHECK_BATCH(cudaMemcpyAsync(done.data(), p.inst, W * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(layers.data(), p.layers, layers.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, b->stream));
+  std::vector<unsigned long long> stamps(static_cast<size_t>(max_depth) + 1, 0);
+  MG_CHECK_BATCH(cudaMemcpyAsync(stamps.data(), p.stamps, stamps.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
   if (loop == kLoopGraph) st->kernel_launches += 2 * hc.depth;
   st->layer_steps += hc.depth;
@@ -837,9 +849,15 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     in.status = done[k].status;
     in.runs++;
     in.layers.clear();
+    in.layer_seconds.clear();
     if (in.status == INST_DONE) {
-      for (uint32_t d = 0; d < max_depth && layers[static_cast<size_t>(k) * max_depth + d]; ++d)
+      for (uint32_t d = 0; d < max_depth && layers[static_cast<size_t>(k) * max_depth + d]; ++d) {
         in.layers.push_back(layers[static_cast<size_t>(k) * max_depth + d]);
+        // Layer d >= 1 is the wave's expansion step d - 1 (shared by the
+        // wave's instances); depth 0 is the seed.
+        const double dt = d && stamps[d] > stamps[d - 1] ? (stamps[d] - stamps[d - 1]) * 1e-9 : 0.0;
+        in.layer_seconds.push_back(dt);
+      }
     }
   }
   if (hc.error) st->fatal |= hc.error;
@@ -957,6 +975,16 @@ int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint6
   *count = layers.size();
   for (size_t d = 0; d < layers.size() && d < capacity; ++d)
     if (sizes) sizes[d] = layers[d];
+  return MGBFS2_OK;
+}
+
+int mgbfs2_batch_layer_seconds(const mgbfs2_batch* batch, uint32_t instance, double* seconds, size_t capacity,
+                               size_t* count) {
+  if (!batch || !count || instance >= batch->impl->inst.size()) return MGBFS2_INVALID_ARGUMENT;
+  const auto& t = batch->impl->inst[instance].layer_seconds;
+  *count = t.size();
+  for (size_t d = 0; d < t.size() && d < capacity; ++d)
+    if (seconds) seconds[d] = t[d];
   return MGBFS2_OK;
 }
 

@@ -139,6 +139,8 @@ _SIGNATURES = {
     "mgbfs2_batch_run": (C.c_int, [C.c_void_p, C.POINTER(BatchOptions), C.POINTER(BatchStatus)]),
     "mgbfs2_batch_layer_table": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.c_size_t,
                                            C.POINTER(C.c_size_t)]),
+    "mgbfs2_batch_layer_seconds": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.c_size_t,
+                                             C.POINTER(C.c_size_t)]),
     "mgbfs2_batch_destroy": (None, [C.c_void_p]),
     "mgbfs2_mlp_param_count": (C.c_uint32, [C.c_uint32]),
     "mgbfs2_mlp_forward": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),

@@ -80,3 +80,27 @@ def test_batch_rejects_unsupported():
         BatchSweep([G.permutation_graph([[1, 0, 2]], [0, 0, 1])])  # repeated labels
     with pytest.raises(ValueError):
         BatchSweep([G.matrix_graph(1, 1, [([2], 7)], [3])])
+
+
+def test_batch_results_tables(tmp_path):
+    import csv
+    from multigpubfs_b200.batch import BatchSweep
+    graphs = _instances(12, True, 31)
+    expect = _oracle_tables(graphs)
+    with BatchSweep(graphs) as sweep:
+        st = sweep.run()
+        secs = [sweep.layer_seconds(i) for i in range(len(graphs))]
+        sweep.write_results(tmp_path)
+    for table, s in zip(expect, secs):
+        assert len(s) == len(table) and s[0] == 0.0 and all(x > 0 for x in s[1:])
+    # Every instance of the one wave shares the wave's step times.
+    deepest = max(range(len(expect)), key=lambda i: len(expect[i]))
+    for s in secs:
+        assert s == secs[deepest][:len(s)]
+    assert sum(secs[deepest]) <= st["device_seconds"] * 1.01 + 1e-4
+    with open(tmp_path / "layers.csv", newline="") as f:
+        rows = list(csv.DictReader(f))
+    got = {}
+    for r in rows:
+        got.setdefault(int(r["instance"]), []).append(int(r["count"]))
+    assert [got[i] for i in range(len(expect))] == expect
