@@ -315,7 +315,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep512", "planner-s12"], default="s13-lrx")
     ap.add_argument("--host-loop", action="store_true",
                     help="layers as separate kernel launches with a host round trip each (for a profiler); "
-                         "by default a wave of the sweep, or a fused BFS, is one CUDA-graph launch")
+                         "by default a wave of the sweep, or a fused BFS, is one persistent launch")
     ap.add_argument("--instances", type=int, default=128, help="planner-s12: number of S12 instances")
     ap.add_argument("--dedup", default=None)
     ap.add_argument("--visited", default=None)

@@ -56,7 +56,7 @@ def main(argv=None) -> int:
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--out", default=None)
     ap.add_argument("--host-loop", action="store_true",
-                    help="one host round trip per layer instead of the whole BFS as one CUDA graph "
+                    help="one host round trip per layer instead of the whole BFS as one persistent launch "
                          "(each layer is then a separate launch, e.g. for a profiler)")
     a = ap.parse_args(argv)
     graph = family(a.graph)

@@ -453,44 +453,6 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
   if (use_handle && threadIdx.x == 0) cudaGraphSetConditional(handle, tiles > 0 ? 1u : 0u);
 }
 
-constexpr uint32_t kBarrierPolls = 1u << 22;
-
-// Grid-wide barrier of the cooperative wave kernel, with a bounded wait.
-// Thread 0 of each block arrives on ctl->bar_count; the last to arrive resets
-// it and advances ctl->bar_gen with a release store; the others poll bar_gen
-// with acquire loads, at most kBarrierPolls times, after which they raise
-// ERR_WAIT_LIMIT and return false (the kernel then ends; nothing waits
-// forever).  Every thread orders its later loads after the barrier.
-__device__ bool grid_barrier(BatchCtl* ctl) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ok = 1;
-    unsigned gen;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(&ctl->bar_gen) : "memory");
-    __threadfence();
-    if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
-      ctl->bar_count = 0;
-      asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&ctl->bar_gen), "r"(gen + 1) : "memory");
-    } else {
-      for (uint32_t polls = 0;; ++polls) {
-        unsigned now;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(&ctl->bar_gen) : "memory");
-        if (now != gen) break;
-        if (polls >= kBarrierPolls) {
-          atomicOr(&ctl->error, ERR_WAIT_LIMIT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-  }
-  __syncthreads();
-  asm volatile("fence.acq_rel.gpu;" ::: "memory");
-  return ok != 0;
-}
-
 // A whole wave in one cooperative launch: every block expands its tiles of
 // the layer, a grid barrier, block 0 finalizes, a second barrier, and all
 // blocks go on while the new frontier has tiles.  Two barriers per layer
@@ -501,9 +463,9 @@ __global__ void __launch_bounds__(kBatchBlock) batch_wave(BatchParams p) {
   __shared__ int more;
   for (;;) {
     expand_layer(p, s);
-    if (!grid_barrier(p.ctl)) return;
+    if (!grid_barrier(&p.ctl->bar_count, &p.ctl->bar_gen, &p.ctl->error)) return;
     if (blockIdx.x == 0) finalize_layer(p, f);
-    if (!grid_barrier(p.ctl)) return;
+    if (!grid_barrier(&p.ctl->bar_count, &p.ctl->bar_gen, &p.ctl->error)) return;
     if (threadIdx.x == 0) more = *reinterpret_cast<volatile unsigned long long*>(&p.ctl->tiles) > 0;
     __syncthreads();
     if (!more) return;

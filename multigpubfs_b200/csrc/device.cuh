@@ -47,6 +47,45 @@ __device__ __forceinline__ void raise_error(unsigned int* error, uint32_t bits) 
   atomicOr(error, bits);
 }
 
+constexpr uint32_t kBarrierPolls = 1u << 22;
+
+// Grid-wide barrier of a cooperative launch, with a bounded wait.  Thread 0
+// of each block arrives on *count; the last to arrive resets it and advances
+// *gen with a release store; the others poll *gen with acquire loads, at most
+// kBarrierPolls times, after which they raise ERR_WAIT_LIMIT in *error and
+// return false (the caller then ends the kernel: nothing waits forever).
+// Every thread orders its later loads after the barrier.  *count and *gen
+// start at zero for each launch.
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen, unsigned int* error) {
+  __shared__ int barrier_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    barrier_ok = 1;
+    unsigned int g;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(gen) : "memory");
+    __threadfence();
+    if (atomicAdd(count, 1u) == gridDim.x - 1) {
+      *count = 0;
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(gen), "r"(g + 1) : "memory");
+    } else {
+      for (uint32_t polls = 0;; ++polls) {
+        unsigned int now;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(gen) : "memory");
+        if (now != g) break;
+        if (polls >= kBarrierPolls) {
+          raise_error(error, ERR_WAIT_LIMIT);
+          barrier_ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  __syncthreads();
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+  return barrier_ok != 0;
+}
+
 __device__ __forceinline__ uint64_t apply_terms(uint64_t p, const Term* t, uint32_t begin, uint32_t end) {
   uint64_t c = 0;
   for (uint32_t k = begin; k < end; ++k) c |= ((p >> t[k].rshift) << t[k].lshift) & t[k].mask;

@@ -1175,6 +1175,8 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
   h.buf[0] = static_cast<unsigned long long*>(front.ptr);
   h.buf[1] = static_cast<unsigned long long*>(next.ptr);
   h.max_entries = kEntries;
+  h.layers = layers;
+  h.stamps = stamps;
   MG_CHECK(cudaMemcpyAsync(ls, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
   MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
   ExpandParams p = *pp;
@@ -1189,33 +1191,67 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
     if (graph) cudaGraphDestroy(graph);
     if (cap_stream) cudaStreamDestroy(cap_stream);
   };
-  cudaError_t e = cudaGraphCreate(&graph, 0);
+  // Persistent form first: one cooperative launch runs every layer, with two
+  // grid barriers per layer instead of two graph nodes.  Its grid must be
+  // co-resident; a device or carveout that cannot hold it falls back to the
+  // graph form below.
+  bool persistent_done = false;
+  cudaError_t e = cudaSuccess;
+  {
+    int resident = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, fn, kBlock, smem) != cudaSuccess) {
+      cudaGetLastError();
+      resident = 0;
+    }
+    const auto known = carveout_blocks.find(fn);
+    const int per_sm = std::min(resident, known != carveout_blocks.end() ? known->second : resident);
+    if (per_sm >= 1) {
+      ExpandParams q = p;
+      q.persistent = 1;
+      void* args[] = {&q};
+      e = cudaEventRecord(ev_kernel[0], stream);
+      if (e == cudaSuccess) {
+        loop_start<<<1, 1, 0, stream>>>(stamps);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) {
+        e = cudaLaunchCooperativeKernel(fn, dim3(per_sm * sm_count), dim3(kBlock), args, smem, stream);
+        if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
+          cudaGetLastError();
+          e = cudaSuccess;  // the graph form below runs the BFS instead
+        } else if (e == cudaSuccess) {
+          persistent_done = true;
+        }
+      }
+    }
+  }
+  if (!persistent_done && e == cudaSuccess) e = cudaGraphCreate(&graph, 0);
   cudaGraphConditionalHandle handle{};
-  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  if (!persistent_done && e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
   cudaGraphNodeParams cp = {};
   cp.type = cudaGraphNodeTypeConditional;
   cp.conditional.handle = handle;
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t node;
-  if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess)
+  if (!persistent_done && e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  if (!persistent_done && e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking);
+  if (!persistent_done && e == cudaSuccess)
     e = cudaStreamBeginCaptureToGraph(cap_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                       cudaStreamCaptureModeRelaxed);
-  if (e == cudaSuccess) {
+  if (!persistent_done && e == cudaSuccess) {
     reinterpret_cast<void (*)(ExpandParams)>(const_cast<void*>(fn))<<<grid, kBlock, smem, cap_stream>>>(p);
-    loop_finalize<<<1, 1, 0, cap_stream>>>(ls, p.control, layers, stamps, handle);
+    loop_finalize<<<1, 1, 0, cap_stream>>>(ls, p.control, handle);
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     e = cudaStreamEndCapture(cap_stream, &body);
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e == cudaSuccess) e = cudaEventRecord(ev_kernel[0], stream);
-  if (e == cudaSuccess) {
+  if (!persistent_done && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (!persistent_done && e == cudaSuccess) e = cudaEventRecord(ev_kernel[0], stream);
+  if (!persistent_done && e == cudaSuccess) {
     loop_start<<<1, 1, 0, stream>>>(stamps);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream);
+  if (!persistent_done && e == cudaSuccess) e = cudaGraphLaunch(exec, stream);
   if (e == cudaSuccess) e = cudaEventRecord(ev_kernel[1], stream);
   LoopState out{};
   std::vector<unsigned long long> sizes(kEntries), times(kEntries);
@@ -1241,7 +1277,7 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
     st->successors += c * gens;
     st->visited_tests += c * gens - (parent_skip && d > 0 ? c : 0);
   }
-  launches += 1 + 2 * expanded;
+  launches += persistent_done ? 2 : 1 + 2 * expanded;
   if (out.parity) std::swap(front, next);
   *count = D ? sizes[D] : 1;
   *visited = out.visited;

@@ -26,6 +26,9 @@ struct LoopState {
   unsigned long long count, visited, capacity;
   unsigned long long* buf[2];
   uint32_t parity, depth, max_entries, stop;  // stop: 0 running, 1 exhausted, 2 error, 3 table full of layers
+  unsigned long long* layers;  // max_entries layer sizes
+  unsigned long long* stamps;  // max_entries globaltimer readings (stamp d = end of layer d)
+  uint32_t bar_count, bar_gen; // grid barrier of the persistent form (zero at launch)
 };
 
 struct ExpandParams {
@@ -40,7 +43,8 @@ struct ExpandParams {
   // (g + 1) << gen_shift for the generator g that produced it; generator
   // inverse[g] applied to it returns to the previous layer and is skipped.
   // gen_shift = 0 disables tagging.
-  uint32_t gen_shift, pad0;
+  uint32_t gen_shift;
+  uint32_t persistent;  // with `loop`: one cooperative launch runs every layer (grid barriers between)
   Control* control;
   unsigned long long* bitmap;
   MultisetDomain ms;
@@ -132,6 +136,34 @@ __device__ __forceinline__ void flush_block(const ExpandParams& p, unsigned long
   __syncthreads();
 }
 
+// Graph mode, after each expansion: record the new layer, stop on an empty
+// layer, a device error or a full layer table, else make the new layer the
+// frontier.  Returns the stop reason (0 = go on).  layers/stamps hold
+// max_entries sizes and globaltimer readings (stamp d = end of layer d).
+__device__ __forceinline__ uint32_t loop_step(LoopState* s, Control* c) {
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  const unsigned long long produced = c->next_count;
+  uint32_t stop = 0;
+  if (c->error || produced > s->capacity) {
+    stop = 2;
+  } else if (produced == 0) {
+    stop = 1;
+  } else {
+    const uint32_t d = s->depth + 1;
+    s->layers[d] = produced;
+    s->stamps[d] = now;
+    s->count = produced;
+    s->visited += produced;
+    s->parity ^= 1u;
+    s->depth = d;
+    c->next_count = 0;
+    if (d + 1 >= s->max_entries) stop = 3;
+  }
+  s->stop = stop;
+  return stop;
+}
+
 template <int V, int N, bool WARP>
 __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
   extern __shared__ __align__(16) unsigned char program_smem[];
@@ -146,71 +178,81 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
   if (threadIdx.x == 0) out_count = 0;
   __syncthreads();
 
-  unsigned long long count = p.count;
-  const unsigned long long* frontier = p.frontier;
-  unsigned long long* next = p.next;
-  if (p.loop) {
-    count = p.loop->count;
-    const uint32_t parity = p.loop->parity;
-    frontier = p.loop->buf[parity];
-    next = p.loop->buf[parity ^ 1u];
-  }
-  const uint32_t lane = lane_id();
-  const uint32_t tile = blockDim.x * p.ppt;
-  const unsigned long long tiles = (count + tile - 1) / tile;
-  for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const unsigned long long base = t * tile;
-    uint64_t par[4];
-    bool val[4];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      par[2 * j] = par[2 * j + 1] = 0;
-      val[2 * j] = val[2 * j + 1] = false;
-      if (2 * j < static_cast<int>(p.ppt)) {
-        const unsigned long long i0 = base + 2ull * (j * blockDim.x + threadIdx.x);
-        if (i0 + 1 < count) {
-          const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(frontier + i0);
-          par[2 * j] = v.x;
-          par[2 * j + 1] = v.y;
-          val[2 * j] = val[2 * j + 1] = true;
-        } else if (i0 < count) {
-          par[2 * j] = frontier[i0];
-          val[2 * j] = true;
+  for (;;) {
+    unsigned long long count = p.count;
+    const unsigned long long* frontier = p.frontier;
+    unsigned long long* next = p.next;
+    if (p.loop) {
+      count = p.loop->count;
+      const uint32_t parity = p.loop->parity;
+      frontier = p.loop->buf[parity];
+      next = p.loop->buf[parity ^ 1u];
+    }
+    const uint32_t lane = lane_id();
+    const uint32_t tile = blockDim.x * p.ppt;
+    const unsigned long long tiles = (count + tile - 1) / tile;
+    for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+      const unsigned long long base = t * tile;
+      uint64_t par[4];
+      bool val[4];
+  #pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        par[2 * j] = par[2 * j + 1] = 0;
+        val[2 * j] = val[2 * j + 1] = false;
+        if (2 * j < static_cast<int>(p.ppt)) {
+          const unsigned long long i0 = base + 2ull * (j * blockDim.x + threadIdx.x);
+          if (i0 + 1 < count) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(frontier + i0);
+            par[2 * j] = v.x;
+            par[2 * j + 1] = v.y;
+            val[2 * j] = val[2 * j + 1] = true;
+          } else if (i0 < count) {
+            par[2 * j] = frontier[i0];
+            val[2 * j] = true;
+          }
         }
       }
-    }
-    uint32_t skip[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
-      skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
-    }
-    for (uint32_t g = 0; g < p.gens; ++g) {
-      const uint32_t tb = begin[g], te = begin[g + 1];
-      const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
-#pragma unroll
+      uint32_t skip[4];
+  #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        if (k >= static_cast<int>(p.ppt)) break;
-        const bool v = val[k] && g != skip[k];
-        const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
-        const bool won = claim<V, N, WARP>(p, c, v);
-        const unsigned m = __ballot_sync(kFullMask, won);
-        if (m) {
-          const int leader = __ffs(m) - 1;
-          uint32_t wb = 0;
-          if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
-          wb = __shfl_sync(kFullMask, wb, leader);
-          if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
+        const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par[k] >> p.gen_shift) : 0u;
+        skip[k] = tag ? inverse[tag - 1] : 0xffffffffu;
+      }
+      for (uint32_t g = 0; g < p.gens; ++g) {
+        const uint32_t tb = begin[g], te = begin[g + 1];
+        const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
+  #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (k >= static_cast<int>(p.ppt)) break;
+          const bool v = val[k] && g != skip[k];
+          const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
+          const bool won = claim<V, N, WARP>(p, c, v);
+          const unsigned m = __ballot_sync(kFullMask, won);
+          if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t wb = 0;
+            if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
+            wb = __shfl_sync(kFullMask, wb, leader);
+            if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
+          }
+        }
+        if (g + 1 < p.gens) {
+          __syncthreads();
+          const uint32_t pending = out_count;
+          __syncthreads();
+          if (pending + tile > kOutCap) flush_block(p, next, out, &out_count, &out_base);
         }
       }
-      if (g + 1 < p.gens) {
-        __syncthreads();
-        const uint32_t pending = out_count;
-        __syncthreads();
-        if (pending + tile > kOutCap) flush_block(p, next, out, &out_count, &out_base);
-      }
+      flush_block(p, next, out, &out_count, &out_base);
     }
-    flush_block(p, next, out, &out_count, &out_base);
+    // Persistent form: the layer is done when every block is; block 0 records
+    // it and makes it the frontier, and all blocks go on unless the loop stops.
+    if (!p.persistent) return;
+    LoopState* ls = p.loop;
+    if (!grid_barrier(&ls->bar_count, &ls->bar_gen, &p.control->error)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) loop_step(ls, p.control);
+    if (!grid_barrier(&ls->bar_count, &ls->bar_gen, &p.control->error)) return;
+    if (*reinterpret_cast<volatile uint32_t*>(&ls->stop)) return;
   }
 }
 
@@ -282,33 +324,10 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
   }
 }
 
-// Graph mode, after each expansion: record the new layer, stop on an empty
-// layer, a device error or a full layer table, else make the new layer the
-// frontier; the WHILE node repeats while `stop` is 0.  layers/stamps hold
-// max_entries sizes and globaltimer readings (stamp d = end of layer d).
-static __global__ void loop_finalize(LoopState* s, Control* c, unsigned long long* layers, unsigned long long* stamps,
-                                     cudaGraphConditionalHandle handle) {
-  unsigned long long now;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-  const unsigned long long produced = c->next_count;
-  uint32_t stop = 0;
-  if (c->error || produced > s->capacity) {
-    stop = 2;
-  } else if (produced == 0) {
-    stop = 1;
-  } else {
-    const uint32_t d = s->depth + 1;
-    layers[d] = produced;
-    stamps[d] = now;
-    s->count = produced;
-    s->visited += produced;
-    s->parity ^= 1u;
-    s->depth = d;
-    c->next_count = 0;
-    if (d + 1 >= s->max_entries) stop = 3;
-  }
-  s->stop = stop;
-  cudaGraphSetConditional(handle, stop ? 0u : 1u);
+// The step as its own launch in the graph form: the WHILE node repeats while
+// `stop` is 0.
+static __global__ void loop_finalize(LoopState* s, Control* c, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, loop_step(s, c) ? 0u : 1u);
 }
 
 static __global__ void loop_start(unsigned long long* stamps) {
