@@ -190,7 +190,7 @@ def reference_arm(args, rank):
 
 def bench_sweep(args, local):
     """Batched sweep: 512 instances (256 seeds x {directed, inverse-closed}),
-    one device-driven CUDA-graph loop per wave."""
+    each wave one persistent cooperative launch."""
     import torch
     from multigpubfs_b200 import workloads
     from multigpubfs_b200.batch import BatchSweep
@@ -209,11 +209,11 @@ def bench_sweep(args, local):
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": "batched sweep: 512 instances (256 seeds x directed / inverse-closed), n in "
                                    "{7,8,9,10}, 2-3 seeded random generators, exact per-instance Lehmer bitmaps, "
-                                   "one CUDA-graph WHILE loop per wave",
+                                   "each wave one persistent cooperative launch",
                        "instances": len(graphs), "states_per_step": states, "successors_per_step": succ},
             "settled_states_per_s": states / dev,
             "wall_ms_per_step": sum(r["seconds"] for r in runs) / len(runs) * 1e3,
-            "waves": runs[0]["waves"], "graph_launches_per_step": runs[0]["graph_launches"],
+            "waves": runs[0]["waves"], "launches_per_step": runs[0]["kernel_launches"],
             "layer_steps": runs[0]["layer_steps"], "gpu_launches": sum(r["kernel_launches"] for r in runs)}
     print(json.dumps(line), flush=True)
     return 0
