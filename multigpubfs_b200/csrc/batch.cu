@@ -457,7 +457,9 @@ __global__ void __launch_bounds__(1024) batch_finalize(BatchParams p, cudaGraphC
 // the layer, a grid barrier, block 0 finalizes, a second barrier, and all
 // blocks go on while the new frontier has tiles.  Two barriers per layer
 // replace two kernel launches per layer.
-__global__ void __launch_bounds__(kBatchBlock) batch_wave(BatchParams p) {
+// Four blocks per SM (as many as its shared memory and registers allow):
+// the bound lets the compiler keep 64 registers, 1 % faster than 48 on S12.
+__global__ void __launch_bounds__(kBatchBlock, kBatchBlocksPerSM) batch_wave(BatchParams p) {
   __shared__ BatchSmem s;
   __shared__ FinalizeSmem f;
   __shared__ int more;
