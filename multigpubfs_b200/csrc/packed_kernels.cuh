@@ -19,9 +19,10 @@ constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
 constexpr uint32_t kBlock = 256;
 constexpr int kPackedBlocksPerSM = 4;  // resident expand_packed blocks: the 164 KB configuration, 92 KB left as L1
 
-// Device-resident layer loop (graph mode): the frontier size, which of the
-// two buffers holds it, and the loop's stop reason live on the device, so one
-// CUDA graph with a WHILE node runs a whole BFS without host round trips.
+// Device-resident layer loop: the frontier size, which of the two buffers
+// holds it, and the loop's stop reason live on the device, so one persistent
+// cooperative launch (or, as the fallback, one CUDA graph with a WHILE node)
+// runs a whole BFS without host round trips.
 struct LoopState {
   unsigned long long count, visited, capacity;
   unsigned long long* buf[2];
