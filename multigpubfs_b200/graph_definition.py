@@ -10,6 +10,8 @@ from __future__ import annotations
 import copy
 import hashlib
 import json
+import math
+import numbers
 
 I64_MIN = -(1 << 63)
 I64_MAX = (1 << 63) - 1
@@ -134,52 +136,27 @@ class GraphDefinition:
             raise ValueError("GRAPH_ACTION_KIND")
         return self
 
+    def with_start(self, start):
+        """The same graph searched from another start state."""
+        value = self.to_dict()
+        value["start"] = list(start)
+        return GraphDefinition(value)
+
     def inverse_closed(self):
-        """True iff every generator's inverse is a generator (the graph is
-        undirected), which admits the three-layer-bank history.  Same rules as
-        graph_definition.py:84-108, including the int64-overflow guard and the
-        canonical-start requirement for modular matrices."""
-        a = self._data["action"]
-        gs = a["generators"]
-        if a["kind"] == "permutation":
-            available = {tuple(g) for g in gs}
-            for g in gs:
-                inv = [0] * len(g)
-                for i, x in enumerate(g):
-                    inv[x] = i
-                if tuple(inv) not in available:
-                    return False
-            return True
-        n = a["rows"]
-        if len({g["modulo"] for g in gs}) != 1:
-            return False
-        mod = gs[0]["modulo"]
-        if mod and mod & (mod - 1):
-            for g in gs:
-                for i in range(n):
-                    if sum(abs(v) * (mod - 1) for v in g["matrix"][i * n:(i + 1) * n]) > I64_MAX:
-                        return False
-        eye = [int(i == j) for i in range(n) for j in range(n)]
-
-        def wrap(x):
-            return ((x + (1 << 63)) & ((1 << 64) - 1)) - (1 << 63)
-
-        def compose(g, h):
-            right = [v % mod for v in h["matrix"]] if mod else h["matrix"]
-            out = []
-            for i in range(n):
-                for j in range(n):
-                    t = wrap(sum(g["matrix"][i * n + k] * right[k * n + j] for k in range(n)))
-                    out.append(t % mod if mod else t)
-            return out
-
-        for g in gs:
-            if not any(compose(g, h) == eye and compose(h, g) == eye for h in gs):
-                return False
-        for g in gs:
-            if g["modulo"] and any(not 0 <= x < g["modulo"] for x in self._data["start"]):
-                return False
-        return True
+        """True iff the inverse of every generator is also a generator, so the
+        graph is undirected and a layer's neighbours lie within one layer of
+        it (the premise of the three-layer-bank history).  Rules of
+        graph_definition.py:84-108: a permutation's inverse is compared as a
+        tuple; a matrix's inverse must compose to the identity on both sides
+        under the action's own arithmetic (int64 wrap, then the modulus), all
+        generators must share one modulus, a non-power-of-two modulus must
+        keep every row product inside int64, and a modular action needs a
+        start whose entries are already reduced."""
+        action = self._data["action"]
+        if action["kind"] == "permutation":
+            present = set(map(tuple, action["generators"]))
+            return all(_permutation_inverse(g) in present for g in action["generators"])
+        return _matrices_inverse_closed(action["rows"], action["generators"], self._data["start"])
 
     def successor(self, state, generator):
         """One successor, evaluated by the GPU kernel mgbfs2_successors_i64."""
@@ -192,41 +169,105 @@ class GraphDefinition:
         return [int(x) for x in children[0, generator].tolist()]
 
 
+def _permutation_inverse(g):
+    """Inverse of a permutation in image form: the positions sorted by image."""
+    return tuple(sorted(range(len(g)), key=g.__getitem__))
+
+
+def _wrap64(x):
+    """Two's-complement int64 value of an integer."""
+    x &= (1 << 64) - 1
+    return x - (1 << 64) if x >> 63 else x
+
+
+def _matrices_inverse_closed(n, generators, start):
+    moduli = {g["modulo"] for g in generators}
+    if len(moduli) != 1:
+        return False
+    (mod,) = moduli
+    if mod and mod & (mod - 1):
+        # With wrap-before-modulus arithmetic a product row whose reduced
+        # magnitude could leave int64 no longer acts as a group element.
+        for g in generators:
+            rows = [g["matrix"][r * n:(r + 1) * n] for r in range(n)]
+            if any(sum(abs(v) for v in row) * (mod - 1) > I64_MAX for row in rows):
+                return False
+    identity = [1 if r == c else 0 for r in range(n) for c in range(n)]
+
+    def product(a, b):
+        # The action applied to a matrix state: right operand already reduced.
+        b = [v % mod for v in b] if mod else b
+        out = [0] * (n * n)
+        for r in range(n):
+            for c in range(n):
+                v = _wrap64(sum(a[r * n + k] * b[k * n + c] for k in range(n)))
+                out[r * n + c] = v % mod if mod else v
+        return out
+
+    matrices = [g["matrix"] for g in generators]
+    for a in matrices:
+        if not any(product(a, b) == identity and product(b, a) == identity for b in matrices):
+            return False
+    return not mod or all(0 <= x < mod for x in start)
+
+
 def _flatten(value):
-    if hasattr(value, "tolist"):
-        value = value.tolist()
-    if isinstance(value, (list, tuple)):
-        return [x for item in value for x in _flatten(item)]
-    if isinstance(value, bool):
+    """Labels of a (possibly nested, possibly tensor) state as a flat list of
+    int64 values.  Integral floats become ints; booleans, fractions, strings,
+    infinities and NaN raise GRAPH_NONINTEGER_SCALAR, values outside int64
+    GRAPH_INT64_RANGE (graph_definition.py:118-129)."""
+    flat, pending = [], [value]
+    while pending:
+        item = pending.pop()
+        if hasattr(item, "tolist"):
+            item = item.tolist()
+        if isinstance(item, (list, tuple)):
+            pending.extend(reversed(item))
+            continue
+        flat.append(_label(item))
+    return flat
+
+
+def _label(x):
+    if isinstance(x, bool):
         raise ValueError("GRAPH_NONINTEGER_SCALAR")
-    try:
-        converted = int(value)
-    except (TypeError, ValueError, OverflowError):
-        raise ValueError("GRAPH_NONINTEGER_SCALAR") from None
-    if converted != value:
-        raise ValueError("GRAPH_NONINTEGER_SCALAR")
-    return [_integer(converted)]
+    if isinstance(x, numbers.Integral):
+        return _integer(int(x))
+    if isinstance(x, numbers.Real) and math.isfinite(x) and float(x).is_integer():
+        return _integer(int(x))
+    raise ValueError("GRAPH_NONINTEGER_SCALAR")
+
+
+def _cayley_definition(obj):
+    """The CayleyPy definition behind a graph object (or the object itself)."""
+    if hasattr(obj, "generators_type"):
+        return obj
+    for attribute in ("definition", "graph_def"):
+        if hasattr(obj, attribute):
+            return getattr(obj, attribute)
+    return obj
+
+
+def _matrix_degree(matrix):
+    return int(matrix.shape[0]) if hasattr(matrix, "shape") else len(matrix)
 
 
 def from_cayleypy(definition):
-    """CayleyPy graph (or its definition) -> GraphDefinition; generators and
-    start are preserved exactly (graph_definition.py:130-143)."""
-    if not hasattr(definition, "generators_type"):
-        if hasattr(definition, "definition"):
-            definition = definition.definition
-        elif hasattr(definition, "graph_def"):
-            definition = definition.graph_def
-    kind = definition.generators_type.name
-    start = _flatten(definition.central_state)
-    options = {"name": definition.name, "generator_names": list(definition.generator_names)}
+    """CayleyPy graph or definition -> GraphDefinition, with generators, start,
+    name and generator names carried over exactly (the attributes read by
+    graph_definition.py:130-143 of the reference)."""
+    d = _cayley_definition(definition)
+    kind = d.generators_type.name
+    start = _flatten(d.central_state)
+    labels = {"name": d.name, "generator_names": list(d.generator_names)}
     if kind == "PERMUTATION":
-        return GraphDefinition.permutation([_flatten(g) for g in definition.generators_permutations], start, **options)
+        return GraphDefinition.permutation(list(map(_flatten, d.generators_permutations)), start, **labels)
     if kind == "MATRIX":
-        generators = definition.generators_matrices
-        first = generators[0].matrix
-        n = int(first.shape[0]) if hasattr(first, "shape") else len(first)
-        if len(start) % n:
+        gens = list(d.generators_matrices)
+        n = _matrix_degree(gens[0].matrix)
+        cols, ragged = divmod(len(start), n)
+        if ragged:
             raise ValueError("GRAPH_MATRIX_SHAPE")
-        return GraphDefinition.matrix(n, len(start) // n, [(_flatten(g.matrix), int(g.modulo)) for g in generators],
-                                      start, **options)
+        pairs = [(_flatten(g.matrix), int(g.modulo)) for g in gens]
+        return GraphDefinition.matrix(n, cols, pairs, start, **labels)
     raise ValueError("GRAPH_ACTION_KIND")
