@@ -71,7 +71,10 @@ typedef struct {
   uint32_t dedup;          /* MGBFS2_DEDUP_* */
   uint64_t capacity;       /* max states per frontier, 0 = from the state bound */
   uint64_t reserve_bytes;  /* device bytes never planned, 0 = 2 GiB */
-  uint32_t shards;         /* bucket shards for MGBFS2_DEDUP_BUCKET, 0 = 64 */
+  uint32_t shards;         /* MGBFS2_DEDUP_BUCKET on the bitmap: 0 = states sharing their first k symbols,
+                              k the smallest of 1, 2 whose (n-k)!-bit bitmap slice is <= 8 MiB (S13: 156
+                              shards); non-zero = k = 2 when degree < shards, else k = 1.  Ignored by
+                              the other dedup modes (grouped layers use 1-3-symbol prefix groups). */
   uint32_t block;          /* threads per block, 0 = tuned */
   uint32_t planner;        /* MGBFS2_PLANNER_* */
   uint32_t bucket_margin;  /* extra entries per shard bucket, 0 = 4096; UINT32_MAX = none */
@@ -86,8 +89,10 @@ typedef struct {
 #define MGBFS2_OPTION_NO_PARENT_SKIP 1u
 /* Plans whose frontier buffers and visited set are sized up front (the fused
  * bitmap or all-visited hash layers, no limits or callback) run the whole BFS
- * as ONE CUDA graph whose WHILE node repeats {expand layer, finalize} on the
- * device; this option keeps the host-driven layer loop instead. */
+ * on the device: one persistent cooperative launch with bounded grid barriers
+ * between layers, or, where the grid cannot be co-resident, one CUDA graph
+ * whose WHILE node repeats {expand layer, finalize}.  This option keeps the
+ * host-driven layer loop instead (one launch and one readback per layer). */
 #define MGBFS2_OPTION_HOST_LOOP 2u
 /* Grouped layers over adjacent-transposition generators derive each child's
  * rank from its parent's Lehmer digits (two digits change); this option makes
@@ -298,9 +303,11 @@ typedef struct {
 MGBFS2_API int mgbfs2_batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int device, mgbfs2_batch** out,
                                    char* error, size_t error_capacity);
 
-/* Runs every instance to completion in waves that fit the memory budget; each
- * wave is ONE CUDA-graph launch whose WHILE node repeats {expand every active
- * instance's layer, finalize} until the device finds no active instance.  An
+/* Runs every instance to completion in waves that fit the memory budget.  By
+ * default a wave is ONE persistent cooperative launch that expands every active
+ * instance's layer, finalizes it behind a bounded grid barrier and repeats
+ * until the device finds no active instance (options->host_loop selects the
+ * CUDA-graph WHILE form or a host-driven loop instead).  An
  * instance that overflows its (predicted) frontier capacity is rerun from depth
  * 0 with its orbit bound, so tables never change. */
 MGBFS2_API int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, mgbfs2_batch_status* status);

@@ -12,6 +12,7 @@ import pytest
 
 from oracle import graph_oracle as G
 from oracle import packed_oracle as P
+from tests.conftest import golden
 
 pytestmark = pytest.mark.gpu
 
@@ -187,9 +188,12 @@ def test_coxeter_grouped_incremental_rank(n, full_rank):
     assert out[2] == [list(range(n))[::-1]]
 
 
-def test_lrx12_three_bank_hash():
-    sizes_ref, _, _ = P.packed_bfs(G.lrx_generators(10), list(range(10)))
-    out = run(G.permutation_graph(G.lrx_generators(10), list(range(10))), visited="hash3")
+@pytest.mark.parametrize("n", [10, 11])
+def test_lrx_three_bank_hash(n):
+    """S10 / S11 LRX through the three-layer banks against the reference's own
+    packed-search tables (fixture)."""
+    sizes_ref = golden("lrx_layers.json")["layers"][str(n)]
+    out = run(G.permutation_graph(G.lrx_generators(n), list(range(n))), visited="hash3")
     assert out[0]["history_layers"] == 3
     assert out[1].layer_sizes == sizes_ref
 
