@@ -131,65 +131,71 @@ uint32_t occupancy_grid(const void* fn, size_t smem, int device) {
   return static_cast<uint32_t>(sms * per_sm);
 }
 
-}  // namespace
+// Largest count * generators whose scratch size layer_layout can represent:
+// the bucket region is 8 bytes per successor.
+constexpr uint64_t kMaxLayerSuccessors = (UINT64_MAX / 2) / sizeof(unsigned long long);
 
-// Enqueues the layer expansion into `scratch` (device memory laid out by
-// layer_layout).  Shared by the caller-scratch entry point.
-int expand_layer_into(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
-                      const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
-                      uint64_t next_capacity, uint64_t* next_count, uint32_t* error, unsigned char* scratch,
-                      uint64_t scratch_bytes, cudaStream_t stream) {
-  if (degree < 2 || degree > 16 || !generators || generators > kLayerMaxGens || !permutations_host || !bitmap ||
-      !next_count || !scratch || (count && (!frontier || !next)))
-    return MGBFS2_INVALID_ARGUMENT;
-  const LayerLayout l = layer_layout(count * generators);
-  if (scratch_bytes < l.total) return MGBFS2_CAPACITY;
+bool layer_arguments_ok(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                        const uint64_t* frontier, uint64_t count, const uint64_t* bitmap, const uint64_t* next,
+                        const uint64_t* next_count) {
+  return degree >= 2 && degree <= 16 && generators && generators <= kLayerMaxGens && permutations_host && bitmap &&
+         next_count && (!count || (frontier && next));
+}
+
+// The generator program of one layer call, as the kernels read it from scratch.
+struct LayerProgram {
   std::vector<Term> terms;
   std::vector<uint32_t> begin;
-  if (!build_layer_program(degree, generators, permutations_host, &terms, &begin)) return MGBFS2_INVALID_ARGUMENT;
-  const uint32_t prefix = layer_prefix(degree);
-  LayerKernels k{};
-  if (!pick_layer_kernels(degree, prefix, &k)) return MGBFS2_UNSUPPORTED;
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
-  if (e != cudaSuccess) return cuda_status(e);
+  uint32_t prefix = 1;
+  LayerKernels kernels{};
+  size_t bytes() const { return terms.size() * sizeof(Term) + begin.size() * sizeof(uint32_t); }
+};
+
+int prepare_layer_program(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                          LayerProgram* prog) {
+  if (!build_layer_program(degree, generators, permutations_host, &prog->terms, &prog->begin))
+    return MGBFS2_INVALID_ARGUMENT;
+  prog->prefix = layer_prefix(degree);
+  if (!pick_layer_kernels(degree, prog->prefix, &prog->kernels)) return MGBFS2_UNSUPPORTED;
+  return MGBFS2_OK;
+}
+
+// Enqueues count -> layout -> route -> accept -> publish on `stream`, with the
+// generator program already in scratch at l.program and the control block and
+// shard metadata already zeroed.  Both layer entry points end here.
+int enqueue_layer(const LayerProgram& prog, uint32_t degree, uint32_t generators, const uint64_t* frontier,
+                  uint64_t count, uint64_t* bitmap, uint64_t* next, uint64_t next_capacity, uint64_t* next_count,
+                  uint32_t* error, unsigned char* scratch, const LayerLayout& l, int device, cudaStream_t stream) {
   Control* control = reinterpret_cast<Control*>(scratch + l.control);
   unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
   Term* program = reinterpret_cast<Term*>(scratch + l.program);
-  uint32_t* program_begin = reinterpret_cast<uint32_t*>(scratch + l.program + terms.size() * sizeof(Term));
-  if ((e = cudaMemsetAsync(control, 0, sizeof(Control), stream)) != cudaSuccess ||
-      (e = cudaMemsetAsync(meta, 0, (3 * kMaxShards + 1) * sizeof(unsigned long long), stream)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(program, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, stream)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(program_begin, begin.data(), begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                           stream)) != cudaSuccess)
-    return cuda_status(e);
   uint64_t fact = 1;
-  for (uint32_t i = degree - prefix + 1; i <= degree; ++i) fact *= i;
+  for (uint32_t i = degree - prog.prefix + 1; i <= degree; ++i) fact *= i;
   RouteParams rp{};
   rp.frontier = reinterpret_cast<const unsigned long long*>(frontier);
   rp.count = count;
   rp.terms = program;
-  rp.term_begin = program_begin;
+  rp.term_begin = reinterpret_cast<const uint32_t*>(program + prog.terms.size());
   rp.gens = generators;
-  rp.total_terms = static_cast<uint32_t>(terms.size());
+  rp.total_terms = static_cast<uint32_t>(prog.terms.size());
   rp.ppt = generators <= 3 ? 4 : (generators <= 6 ? 2 : 1);
   rp.group = kMaxEntries / rp.ppt;
   rp.gen_shift = 0;
   rp.shards = static_cast<uint32_t>(fact);  // n!/(n-prefix)!
-  rp.prefix = prefix;
+  rp.prefix = prog.prefix;
   rp.buckets = reinterpret_cast<unsigned long long*>(scratch + l.buckets);
   rp.shard_begin = meta;
   rp.shard_cap = meta + kMaxShards;
   rp.shard_count = meta + 2 * kMaxShards;
   rp.control = control;
-  const size_t program_bytes = terms.size() * sizeof(Term) + begin.size() * sizeof(uint32_t);
+  const LayerKernels& k = prog.kernels;
+  cudaError_t e = cudaSuccess;
   if (count) {
-    const size_t count_smem = kMaxShards * sizeof(uint32_t) + program_bytes;
+    const size_t count_smem = kMaxShards * sizeof(uint32_t) + prog.bytes();
     k.count<<<occupancy_grid(reinterpret_cast<const void*>(k.count), count_smem, device), kBlock, count_smem,
               stream>>>(rp);
     layout_shards<<<1, 32, 0, stream>>>(meta, rp.shards);
-    const size_t route_smem = sizeof(RouteSmem) + program_bytes;
+    const size_t route_smem = sizeof(RouteSmem) + prog.bytes();
     if ((e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k.route), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(route_smem))) != cudaSuccess)
       return cuda_status(e);
@@ -209,6 +215,38 @@ int expand_layer_into(uint32_t degree, uint32_t generators, const uint32_t* perm
   }
   publish_layer<<<1, 32, 0, stream>>>(control, reinterpret_cast<unsigned long long*>(next_count), error);
   return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+// Enqueues the layer expansion into `scratch` (device memory laid out by
+// layer_layout): the caller-scratch entry point.
+int expand_layer_into(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                      const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
+                      uint64_t next_capacity, uint64_t* next_count, uint32_t* error, unsigned char* scratch,
+                      uint64_t scratch_bytes, cudaStream_t stream) {
+  if (!scratch || !layer_arguments_ok(degree, generators, permutations_host, frontier, count, bitmap, next, next_count))
+    return MGBFS2_INVALID_ARGUMENT;
+  if (count > kMaxLayerSuccessors / generators) return MGBFS2_CAPACITY;
+  const LayerLayout l = layer_layout(count * generators);
+  if (scratch_bytes < l.total) return MGBFS2_CAPACITY;
+  LayerProgram prog;
+  if (int rc = prepare_layer_program(degree, generators, permutations_host, &prog)) return rc;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_status(e);
+  Control* control = reinterpret_cast<Control*>(scratch + l.control);
+  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  unsigned char* program = scratch + l.program;
+  if ((e = cudaMemsetAsync(control, 0, sizeof(Control), stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(meta, 0, (3 * kMaxShards + 1) * sizeof(unsigned long long), stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(program, prog.terms.data(), prog.terms.size() * sizeof(Term), cudaMemcpyHostToDevice,
+                           stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(program + prog.terms.size() * sizeof(Term), prog.begin.data(),
+                           prog.begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+    return cuda_status(e);
+  return enqueue_layer(prog, degree, generators, frontier, count, bitmap, next, next_capacity, next_count, error,
+                       scratch, l, device, stream);
 }
 
 uint64_t expand_layer_scratch_bytes(uint64_t count, uint32_t generators) {
@@ -243,7 +281,10 @@ unsigned char* g_static_address[kStaticMaxDevices] = {};
 
 // Device address of g_static_scratch on `device` (the current device).  The
 // host-side name is only a stand-in for the symbol, never a device address,
-// so it is resolved once per device with cudaGetSymbolAddress.
+// so it is resolved with cudaGetSymbolAddress on the first call per device
+// and kept for the process.  The address belongs to the device's primary
+// context, the one the CUDA runtime uses: callers on their own driver-API
+// contexts, or after cudaDeviceReset, are not supported.
 int static_scratch(int device, unsigned char** out) {
   if (device < 0 || device >= kStaticMaxDevices) return MGBFS2_UNSUPPORTED;
   std::lock_guard<std::mutex> hold(g_static_lock);
@@ -262,6 +303,9 @@ struct StagedProgram {
   uint32_t begin[2 * kLayerMaxGens + 1];
   uint32_t total_terms, begin_entries;
 };
+// Passed by value as a kernel parameter: kernel parameters above 4 KB need
+// CUDA 12.1 or newer (limit 32,764 bytes).
+static_assert(sizeof(StagedProgram) <= 32764, "StagedProgram exceeds the kernel parameter limit");
 
 // Writes the program into scratch and zeroes the control block and shard
 // metadata (counts, capacities, work counter).
@@ -283,78 +327,32 @@ __global__ void stage_static_layer(StagedProgram prog, Term* terms, uint32_t* be
 int expand_layer_static(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
                         const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,
                         uint64_t next_capacity, uint64_t* next_count, uint32_t* error, cudaStream_t stream) {
-  if (degree < 2 || degree > 16 || !generators || generators > kLayerMaxGens || !permutations_host || !bitmap ||
-      !next_count || (count && (!frontier || !next)))
+  if (!layer_arguments_ok(degree, generators, permutations_host, frontier, count, bitmap, next, next_count))
     return MGBFS2_INVALID_ARGUMENT;
+  // count * generators above the static bucket room (checked without forming
+  // a product that could wrap).
+  if (count > kMaxLayerSuccessors / generators) return MGBFS2_CAPACITY;
   const LayerLayout l = layer_layout(count * generators);
-  if (l.total > kStaticScratchBytes) return MGBFS2_CAPACITY;  // count * generators above the static bucket room
-  static thread_local StagedProgram prog;
-  std::vector<Term> terms;
-  std::vector<uint32_t> begin;
-  if (!build_layer_program(degree, generators, permutations_host, &terms, &begin)) return MGBFS2_INVALID_ARGUMENT;
-  std::copy(terms.begin(), terms.end(), prog.terms);
-  std::copy(begin.begin(), begin.end(), prog.begin);
-  prog.total_terms = static_cast<uint32_t>(terms.size());
-  prog.begin_entries = static_cast<uint32_t>(begin.size());
-  const uint32_t prefix = layer_prefix(degree);
-  LayerKernels k{};
-  if (!pick_layer_kernels(degree, prefix, &k)) return MGBFS2_UNSUPPORTED;
+  if (l.total > kStaticScratchBytes) return MGBFS2_CAPACITY;
+  LayerProgram prog;
+  if (int rc = prepare_layer_program(degree, generators, permutations_host, &prog)) return rc;
+  static thread_local StagedProgram staged;
+  std::copy(prog.terms.begin(), prog.terms.end(), staged.terms);
+  std::copy(prog.begin.begin(), prog.begin.end(), staged.begin);
+  staged.total_terms = static_cast<uint32_t>(prog.terms.size());
+  staged.begin_entries = static_cast<uint32_t>(prog.begin.size());
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
   if (e != cudaSuccess) return cuda_status(e);
   unsigned char* scratch = nullptr;
-  int rc = static_scratch(device, &scratch);
-  if (rc) return rc;
-  Control* control = reinterpret_cast<Control*>(scratch + l.control);
-  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  if (int rc = static_scratch(device, &scratch)) return rc;
   Term* program = reinterpret_cast<Term*>(scratch + l.program);
-  uint32_t* program_begin = reinterpret_cast<uint32_t*>(scratch + l.program + terms.size() * sizeof(Term));
-  stage_static_layer<<<1, kBlock, 0, stream>>>(prog, program, program_begin, control, meta);
-  uint64_t fact = 1;
-  for (uint32_t i = degree - prefix + 1; i <= degree; ++i) fact *= i;
-  RouteParams rp{};
-  rp.frontier = reinterpret_cast<const unsigned long long*>(frontier);
-  rp.count = count;
-  rp.terms = program;
-  rp.term_begin = program_begin;
-  rp.gens = generators;
-  rp.total_terms = prog.total_terms;
-  rp.ppt = generators <= 3 ? 4 : (generators <= 6 ? 2 : 1);
-  rp.group = kMaxEntries / rp.ppt;
-  rp.gen_shift = 0;
-  rp.shards = static_cast<uint32_t>(fact);
-  rp.prefix = prefix;
-  rp.buckets = reinterpret_cast<unsigned long long*>(scratch + l.buckets);
-  rp.shard_begin = meta;
-  rp.shard_cap = meta + kMaxShards;
-  rp.shard_count = meta + 2 * kMaxShards;
-  rp.control = control;
-  const size_t program_bytes = terms.size() * sizeof(Term) + begin.size() * sizeof(uint32_t);
-  if (count) {
-    const size_t count_smem = kMaxShards * sizeof(uint32_t) + program_bytes;
-    k.count<<<occupancy_grid(reinterpret_cast<const void*>(k.count), count_smem, device), kBlock, count_smem,
-              stream>>>(rp);
-    layout_shards<<<1, 32, 0, stream>>>(meta, rp.shards);
-    const size_t route_smem = sizeof(RouteSmem) + program_bytes;
-    if ((e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k.route), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(route_smem))) != cudaSuccess)
-      return cuda_status(e);
-    k.route<<<occupancy_grid(reinterpret_cast<const void*>(k.route), route_smem, device), kBlock, route_smem,
-              stream>>>(rp);
-    AcceptParams ap{};
-    ap.buckets = rp.buckets;
-    ap.shard_begin = meta;
-    ap.shard_count = meta + 2 * kMaxShards;
-    ap.shards = rp.shards;
-    ap.bitmap = reinterpret_cast<unsigned long long*>(bitmap);
-    ap.next = reinterpret_cast<unsigned long long*>(next);
-    ap.capacity = next_capacity;
-    ap.work = meta + 3 * kMaxShards;
-    ap.control = control;
-    k.accept<<<occupancy_grid(reinterpret_cast<const void*>(k.accept), 0, device), kBlock, 0, stream>>>(ap);
-  }
-  publish_layer<<<1, 32, 0, stream>>>(control, reinterpret_cast<unsigned long long*>(next_count), error);
-  return cuda_status(cudaGetLastError());
+  stage_static_layer<<<1, kBlock, 0, stream>>>(staged, program,
+                                               reinterpret_cast<uint32_t*>(program + prog.terms.size()),
+                                               reinterpret_cast<Control*>(scratch + l.control),
+                                               reinterpret_cast<unsigned long long*>(scratch + l.meta));
+  return enqueue_layer(prog, degree, generators, frontier, count, bitmap, next, next_capacity, next_count, error,
+                       scratch, l, device, stream);
 }
 
 }  // namespace mgbfs2

@@ -103,3 +103,42 @@ def test_static_layer_full_bfs_and_limit():
     at_limit = torch.full((STATIC_LIMIT // len(gens),), P.pack(list(range(n)), 4), dtype=torch.int64, device="cuda")
     rc, _, k, err = _call(lib, True, n, gens, at_limit, bitmap, 1)
     assert rc == 0 and k == 0 and err == 0  # every successor already visited
+
+
+def test_static_layer_allocates_nothing():
+    """The defining property: after a first call on the device (which loads the
+    kernels and resolves the array's address), further calls change neither
+    the device's free memory nor torch's allocator.  Every buffer is made
+    before the measured calls."""
+    import torch
+    from multigpubfs_b200 import native
+    lib = native.require_device()
+    n = 9
+    gens = G.lrx_generators(n)
+    flat = (C.c_uint32 * (n * len(gens)))(*[x for g in gens for x in g])
+    bitmap = torch.zeros((math.factorial(n) + 63) // 64, dtype=torch.int64, device="cuda")
+    frontier = torch.tensor([P.pack(list(range(n)), 4)], dtype=torch.int64, device="cuda")
+    nxt = torch.empty(1 << 16, dtype=torch.int64, device="cuda")
+    count = torch.zeros(1, dtype=torch.int64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = native.stream_handle()
+
+    def layer(src, k):
+        rc = lib.mgbfs2_expand_layer_bitmap_static(n, len(gens), flat, src.data_ptr(), k, bitmap.data_ptr(),
+                                                   nxt.data_ptr(), nxt.numel(), count.data_ptr(), err.data_ptr(),
+                                                   stream)
+        assert rc == 0
+
+    layer(frontier, 1)  # warm-up: module load and symbol address
+    bitmap.zero_()
+    bitmap[0] = 1
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    torch_before = torch.cuda.memory_allocated()
+    layer(frontier, 1)
+    layer(frontier, 1)  # the start's children are visited now: nothing new
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == torch_before
+    assert free_after == free_before
+    assert int(count.item()) == 0 and int(err.item()) == 0
