@@ -49,3 +49,16 @@ def cuda_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def sweep_fixture(key):
+    """Oracle layer tables of one batched workload (tests/golden/sweep_tables.json,
+    made by tests/golden/make_sweep_golden.py): dict with seed_base,
+    generators_sha256 and tables."""
+    return golden("sweep_tables.json")[key]
+
+
+def generator_digest(graph):
+    import hashlib
+    text = json.dumps(graph["action"]["generators"], separators=(",", ":"))
+    return hashlib.sha256(text.encode()).hexdigest()
