@@ -1,5 +1,7 @@
-"""Replica runs on several GPUs: one process per GPU, each running the whole
-BFS of its own copy of the graph, then one exchange of results.
+"""Runs on several GPUs, one process per GPU, with no collective on the data
+path: N replicas of one single-graph BFS (their tables checked against each
+other once, after the runs), or a batched sweep whose instances are split
+between the ranks by work and whose tables are gathered to rank 0.
 
 The reference splits ONE search across GPUs by state ownership
 (multigpubfs/launch.py:350-378, one `graph-rank` process per GPU) and, after
@@ -56,3 +58,64 @@ def exchange(layer_sizes, device_seconds: float, successors: int, *, device=None
         bad = [k for k, r in enumerate(rows) if r != rows[0]]
         raise ReplicaMismatch(f"LAYER_CONSENSUS_MISMATCH: ranks {bad} differ from rank 0")
     return {"world": world, "device_seconds_max": float(t.item()), "successors_total": int(s.item())}
+
+
+# ---------------------------------------------------------------------------
+# Batched sweeps on several GPUs: the instances are independent, so each rank
+# takes a share of them and runs it as its own waves, with no exchange on the
+# data path; rank 0 gathers the tables afterwards.
+
+def partition_instances(work, world: int) -> list[int]:
+    """Owner rank of every instance, balancing the summed `work` (e.g. the
+    exact successor count g * |G| of each instance) over `world` ranks: the
+    largest instances first, each to the least-loaded rank (ties: lower rank,
+    lower instance index), so the split is deterministic on every rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0] * world
+    owner = [0] * len(work)
+    for i in sorted(range(len(work)), key=lambda k: (-int(work[k]), k)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += int(work[i])
+    return owner
+
+
+def gather_tables(ids, tables, count: int, *, device=None, group=None):
+    """All ranks call this once, in the same order.  `ids` are the instance
+    indices this rank ran and `tables` their layer tables.  Rank 0 returns the
+    `count` tables ordered by instance index; the other ranks return None.
+    Raises on rank 0 if an instance is missing or reported twice."""
+    import torch
+    import torch.distributed as dist
+
+    dev = device if device is not None else torch.device("cpu")
+    world = dist.get_world_size(group)
+    flat = []
+    for i, t in zip(ids, tables):
+        flat += [int(i), len(t)] + [int(x) for x in t]
+    size = torch.tensor([len(flat)], dtype=torch.int64, device=dev)
+    sizes = [torch.empty_like(size) for _ in range(world)]
+    dist.all_gather(sizes, size, group=group)
+    longest = max(int(s.item()) for s in sizes)
+    mine = torch.full((max(longest, 1),), -1, dtype=torch.int64, device=dev)
+    if flat:
+        mine[:len(flat)] = torch.tensor(flat, dtype=torch.int64, device=dev)
+    every = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(every, mine, group=group)
+    if dist.get_rank(group) != 0:
+        return None
+    out = [None] * count
+    for r, buf in enumerate(every):
+        words = buf[:int(sizes[r].item())].cpu().tolist()
+        k = 0
+        while k < len(words):
+            i, n = words[k], words[k + 1]
+            if not 0 <= i < count or out[i] is not None:
+                raise RuntimeError(f"GATHER_INSTANCE {i} from rank {r}")
+            out[i] = words[k + 2:k + 2 + n]
+            k += 2 + n
+    missing = [i for i, t in enumerate(out) if t is None]
+    if missing:
+        raise RuntimeError(f"GATHER_MISSING {missing[:8]}")
+    return out
