@@ -18,32 +18,46 @@ import hashlib
 import json
 from pathlib import Path
 
+import numpy as np
+
 from . import native
 from .graph_definition import GraphDefinition
 
 
 class BatchSweep:
     def __init__(self, graphs, device: int = 0):
+        """`graphs`: schema-2 dicts or GraphDefinitions of permutation graphs.
+        Their generators and starts are packed into two flat arrays that the
+        descriptors point into; mgbfs2_batch_create validates them (generator
+        permutations, distinct labels, degree and generator limits)."""
         self.lib = native.require_device()
-        self.graphs = [g if isinstance(g, GraphDefinition) else GraphDefinition.from_dict(g) for g in graphs]
+        self.graphs = [g.to_dict() if isinstance(g, GraphDefinition) else g for g in graphs]
         n = len(self.graphs)
+        if not n:
+            raise ValueError("BATCH_ARGUMENT: no instances")
+        if any(g["action"]["kind"] != "permutation" for g in self.graphs):
+            raise ValueError("BATCH_REQUIRES_PERMUTATION_ACTION")
+        degree = [len(g["start"]) for g in self.graphs]
+        gens = [len(g["action"]["generators"]) for g in self.graphs]
+        starts = np.ascontiguousarray(np.concatenate([np.asarray(g["start"], dtype=np.int64) for g in self.graphs]))
+        perms = np.ascontiguousarray(np.concatenate(
+            [np.asarray(g["action"]["generators"], dtype=np.int64).ravel() for g in self.graphs]))
+        if perms.size and (perms.min() < 0 or perms.max() > 0xFFFFFFFF):
+            raise ValueError("GRAPH_PERMUTATION_GENERATOR")
+        perms = perms.astype(np.uint32)
+        self._keep = [starts, perms]
         descs = (native.GraphDesc * n)()
-        self._keep = []
-        for k, g in enumerate(self.graphs):
-            a = g.action
-            if a["kind"] != "permutation":
-                raise ValueError("BATCH_REQUIRES_PERMUTATION_ACTION")
-            start = g.start
-            st = (C.c_int64 * len(start))(*start)
-            flat = (C.c_uint32 * (len(start) * g.generator_count))(*[x for gen in a["generators"] for x in gen])
-            self._keep += [st, flat]
+        s_off = p_off = 0
+        for k in range(n):
             d = descs[k]
             d.kind = 0
-            d.elements = d.rows = len(start)
+            d.elements = d.rows = degree[k]
             d.cols = 1
-            d.generators = g.generator_count
-            d.permutations = C.cast(flat, C.POINTER(C.c_uint32))
-            d.start = C.cast(st, C.POINTER(C.c_int64))
+            d.generators = gens[k]
+            d.permutations = C.cast(perms.ctypes.data + 4 * p_off, C.POINTER(C.c_uint32))
+            d.start = C.cast(starts.ctypes.data + 8 * s_off, C.POINTER(C.c_int64))
+            s_off += degree[k]
+            p_off += degree[k] * gens[k]
         handle = C.c_void_p()
         err = C.create_string_buffer(512)
         rc = self.lib.mgbfs2_batch_create(descs, n, device, C.byref(handle), err, len(err))
@@ -102,7 +116,17 @@ class BatchSweep:
         return [int(sizes[i]) for i in range(count.value)]
 
     def layer_tables(self):
-        return [self.layer_table(i) for i in range(self.count)]
+        """Every instance's layer table, from one native call."""
+        offsets = np.zeros(self.count + 1, dtype=np.uint64)
+        native.check(self.lib.mgbfs2_batch_layer_tables(self.handle, None, 0, offsets.ctypes.data),
+                     "mgbfs2_batch_layer_tables")
+        total = int(offsets[-1])
+        flat = np.zeros(max(total, 1), dtype=np.uint64)
+        native.check(self.lib.mgbfs2_batch_layer_tables(self.handle, flat.ctypes.data, total, offsets.ctypes.data),
+                     "mgbfs2_batch_layer_tables")
+        values = flat.tolist()
+        cuts = offsets.tolist()
+        return [values[cuts[i]:cuts[i + 1]] for i in range(self.count)]
 
     def layer_seconds(self, instance: int):
         """Per-layer expansion seconds of one instance, aligned with its layer
@@ -118,8 +142,8 @@ class BatchSweep:
 
     def write_results(self, output):
         """The sweep tables of the last run: see `write_sweep_results`."""
-        names = [g.name or f"instance-{i}" for i, g in enumerate(self.graphs)]
-        degrees = [len(g.start) for g in self.graphs]
+        names = [g.get("name") or f"instance-{i}" for i, g in enumerate(self.graphs)]
+        degrees = [len(g["start"]) for g in self.graphs]
         return write_sweep_results(output, names, degrees, self.layer_tables(),
                                    [self.layer_seconds(i) for i in range(self.count)])
 

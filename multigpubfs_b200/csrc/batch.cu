@@ -17,9 +17,18 @@
 // prefix of the per-instance tile counts, so the degree, the generator
 // program and the segment are uniform over the block (the rank is unrolled
 // for that degree).  Winners are staged in shared memory and appended to the
-// instance's segment with one reservation per block flush.  A segment overflow
-// stops that instance and marks it; the host reruns it from depth 0 with its
-// plain (orbit-bound) capacity in a later wave, so results never change.
+// instance's segment with one reservation per block flush.
+//
+// Segments sized by a prediction (the learned planner) can overflow.  A winner
+// that finds no room in the segment clears its bitmap bit again, so after the
+// layer the bitmap holds exactly the visited states plus the winners that were
+// stored.  The finalize step then gives the instance a larger next segment
+// from a spare pool region of the wave (the exact winner count of the failed
+// attempt bounds the layer), the stored winners are moved there by all blocks,
+// and the instance expands the same layer again while the others go on: the
+// overflow costs one layer, and the table is the same.  Only when the pool is
+// exhausted is the instance retired and rerun from depth 0 with its orbit
+// bound in a later wave.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -44,8 +53,10 @@ constexpr uint32_t kBatchBlock = 256;
 constexpr int kBatchBlocksPerSM = 4;   // default resident batch_expand blocks per SM
 // Layer loop of a wave (mgbfs2_batch_options.host_loop): persistent, host (1) or graph.
 constexpr uint32_t kLoopPersistent = 0, kLoopGraph = 2;
-constexpr uint32_t kBatchPpt = 4;                         // frontier entries per thread per tile
-constexpr uint32_t kBatchTile = kBatchBlock * kBatchPpt;  // entries per tile (one instance per tile)
+constexpr uint32_t kBatchPpt = 4;                         // most frontier entries per thread per tile
+constexpr uint32_t kBatchTile = kBatchBlock * kBatchPpt;  // most entries per tile (one instance per tile)
+// A wave's tile is kBatchBlock * ppt entries, ppt in {1, 2, 4} (the tuned
+// shape; 4 by default).
 constexpr uint32_t kBatchOut = 4096;                      // winners staged in shared memory per block
 constexpr uint32_t kMaxBatchGens = 16;
 constexpr uint32_t kMaxBatchTerms = kMaxBatchGens * 15;   // <= n distinct displacements per generator
@@ -56,14 +67,27 @@ struct BatchInst {
   uint32_t gen_shift, status;           // parent-edge tag position (0 = none)
   uint32_t sel_off, bytes;              // byte-permute selectors (6 per generator) when bytes != 0
   unsigned long long bitmap_off;        // first bitmap word
-  unsigned long long seg_off, seg_cap;  // frontier segment (same in both buffers)
+  // Frontier segments: offset and capacity in buf[0] and in buf[1]; the
+  // current layer is in buf[par], the next one is written to buf[par ^ 1].
+  unsigned long long seg_off[2], seg_cap[2];
+  uint32_t par, depth;                  // this instance's buffer parity and its current depth
+};
+
+// A move of the stored winners of an overflowed layer into the instance's new
+// segment (entries of buf[buf]).
+struct BatchReloc {
+  unsigned long long src, dst, count;
+  uint32_t buf, pad;
 };
 
 struct BatchCtl {
   unsigned long long total;  // entries in the current frontier
   unsigned long long tiles;      // tiles of the current frontier (tile_prefix[count])
   unsigned long long next_tile;  // work counter of batch_expand, reset by every finalize
-  uint32_t parity, depth, max_depth, error;
+  unsigned long long pool_base, pool_cap, pool_used;  // spare segment region (entries, same in both buffers)
+  uint32_t step, max_depth, error, reloc_count;       // step: layer steps taken by the wave
+  uint32_t redo_layers, max_steps;                    // max_steps: entries of the stamp array - 1
+  uint32_t ppt, pad;                                  // frontier entries per thread of a tile
   uint32_t bar_count, bar_gen;   // grid barrier of the persistent wave kernel (zero at the wave's start)
 };
 
@@ -80,7 +104,9 @@ struct BatchParams {
   unsigned long long* cur_count;    // per instance: entries in the current frontier
   unsigned long long* next_count;   // per instance: winners appended to the next frontier
   unsigned long long* layers;       // count x max_depth
-  unsigned long long* stamps;       // max_depth + 1: globaltimer at the seed (0) and after layer step d (d + 1)
+  uint32_t* layer_step;             // count x max_depth: the wave's step that produced each layer
+  unsigned long long* stamps;       // max_steps + 1: globaltimer at the seed (0) and after step t (t + 1)
+  BatchReloc* reloc;                // count entries: moves queued by the last finalize
   BatchCtl* ctl;
 };
 
@@ -92,8 +118,10 @@ struct BatchSmem {
   uint32_t sel[kMaxBatchGens * 6];
   uint32_t begin[kMaxBatchGens + 1];
   uint32_t inverse[kMaxBatchGens];
-  unsigned long long bitmap_off, seg_off, seg_cap, count, tile, local_tile, out_base;
-  uint32_t inst, found, n, gens, shift, out_count, bytes;
+  const unsigned long long* front;  // the instance's current segment
+  unsigned long long* next;         // the instance's next segment
+  unsigned long long bitmap_off, seg_cap, count, tile, local_tile, out_base;
+  uint32_t inst, found, n, gens, shift, out_count, bytes, ppt;
 };
 
 __device__ __forceinline__ uint32_t find_instance(const unsigned long long* prefix, uint32_t count,
@@ -107,28 +135,38 @@ __device__ __forceinline__ uint32_t find_instance(const unsigned long long* pref
   return lo;
 }
 
-// Appends the block's staged winners to the current instance's next segment
-// with one reservation.  Positions at or past the segment's capacity are not
-// written; batch_finalize sees the count above capacity and retires the
-// instance as overflowed.  Called by all threads of the block.
 // The pointers a tile needs, passed by value (a reference to the kernel
 // parameter block would copy it to local memory).
 struct TileArgs {
-  const unsigned long long* front;
-  unsigned long long* next;
   unsigned long long* bitmap;
   unsigned long long* next_count;
 };
 
+// Appends the block's staged winners to the current instance's next segment
+// with one reservation.  A winner whose position is at or past the segment's
+// capacity is not written and clears its bitmap bit again (with an atomic of
+// the claim's width), so that a redo of the layer finds it unvisited;
+// batch_finalize sees the count above capacity and redoes the layer in a
+// larger segment.  Called by all threads of the block.
 __device__ __forceinline__ void batch_flush(const TileArgs a, BatchSmem& s) {
   __syncthreads();
   const uint32_t n = s.out_count;
   if (threadIdx.x == 0 && n) s.out_base = atomicAdd(&a.next_count[s.inst], static_cast<unsigned long long>(n));
   __syncthreads();
   const unsigned long long base = s.out_base, cap = s.seg_cap;
-  unsigned long long* seg = a.next + s.seg_off;
-  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x)
-    if (base + k < cap) seg[base + k] = s.out[k];
+  unsigned long long* seg = s.next;
+  for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+    if (base + k < cap) {
+      seg[base + k] = s.out[k];
+    } else {
+      const uint64_t w = s.out[k] & ((1ull << (4 * s.n)) - 1ull);
+      const uint64_t r = lehmer_rank4_n(w, s.n);
+      if (s.bytes)
+        atomicAnd(reinterpret_cast<unsigned int*>(a.bitmap + s.bitmap_off) + (r >> 5), ~(1u << (r & 31)));
+      else
+        atomicAnd(a.bitmap + s.bitmap_off + (r >> 6), ~(1ull << (r & 63)));
+    }
+  }
   __syncthreads();
   if (threadIdx.x == 0) s.out_count = 0;
   __syncthreads();
@@ -177,9 +215,10 @@ __device__ __forceinline__ uint32_t lehmer_rank_bytes(const uint32_t (&b)[3]) {
 template <int N>
 __device__ __forceinline__ void batch_tile_bytes(const TileArgs a, BatchSmem& s) {
   const uint32_t lane = lane_id();
-  const unsigned long long count = s.count, base = s.local_tile * kBatchTile;
+  const uint32_t ppt = s.ppt, tile = kBatchBlock * ppt;
+  const unsigned long long count = s.count, base = s.local_tile * tile;
   const uint32_t gens = s.gens, shift = s.shift;
-  const unsigned long long* seg = a.front + s.seg_off;
+  const unsigned long long* seg = s.front;
   unsigned int* bitmap = reinterpret_cast<unsigned int*>(a.bitmap + s.bitmap_off);
   uint32_t eb[kBatchPpt][3];
   uint32_t skip[kBatchPpt];
@@ -187,7 +226,7 @@ __device__ __forceinline__ void batch_tile_bytes(const TileArgs a, BatchSmem& s)
 #pragma unroll
   for (uint32_t k = 0; k < kBatchPpt; ++k) {
     const unsigned long long idx = base + k * kBatchBlock + threadIdx.x;
-    val[k] = idx < count;
+    val[k] = k < ppt && idx < count;
     uint64_t w = val[k] ? seg[idx] : 0ull;
     const uint32_t tag = shift ? static_cast<uint32_t>(w >> shift) : 0u;
     skip[k] = tag ? s.inverse[tag - 1] : 0xffffffffu;
@@ -200,6 +239,7 @@ __device__ __forceinline__ void batch_tile_bytes(const TileArgs a, BatchSmem& s)
     const unsigned long long gtag = shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull;
 #pragma unroll
     for (uint32_t k = 0; k < kBatchPpt; ++k) {
+      if (k >= ppt) break;  // block-uniform
       const bool live = val[k] && g != skip[k];
       bool won = false;
       uint32_t cb[3];
@@ -224,14 +264,14 @@ __device__ __forceinline__ void batch_tile_bytes(const TileArgs a, BatchSmem& s)
       __syncthreads();
       const uint32_t pending = s.out_count;
       __syncthreads();
-      if (pending + kBatchTile > kBatchOut) batch_flush(a, s);
+      if (pending + tile > kBatchOut) batch_flush(a, s);
     }
   }
   batch_flush(a, s);
 }
 
-// One tile (kBatchTile consecutive entries of one instance's frontier) with a
-// compile-time degree, so the Lehmer rank is fully unrolled.
+// One tile (ppt * kBatchBlock consecutive entries of one instance's frontier)
+// with a compile-time degree, so the Lehmer rank is fully unrolled.
 template <int N>
 __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
   if constexpr (N <= 12) {
@@ -241,9 +281,10 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
     }
   }
   const uint32_t lane = lane_id();
-  const unsigned long long count = s.count, base = s.local_tile * kBatchTile;
+  const uint32_t ppt = s.ppt, tile = kBatchBlock * ppt;
+  const unsigned long long count = s.count, base = s.local_tile * tile;
   const uint32_t gens = s.gens, shift = s.shift;
-  const unsigned long long* seg = a.front + s.seg_off;
+  const unsigned long long* seg = s.front;
   unsigned long long* bitmap = a.bitmap + s.bitmap_off;
   uint64_t par[kBatchPpt];
   uint32_t skip[kBatchPpt];
@@ -251,7 +292,7 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
 #pragma unroll
   for (uint32_t k = 0; k < kBatchPpt; ++k) {
     const unsigned long long idx = base + k * kBatchBlock + threadIdx.x;
-    val[k] = idx < count;
+    val[k] = k < ppt && idx < count;
     par[k] = val[k] ? seg[idx] : 0ull;
     const uint32_t tag = shift ? static_cast<uint32_t>(par[k] >> shift) : 0u;
     skip[k] = tag ? s.inverse[tag - 1] : 0xffffffffu;
@@ -262,6 +303,7 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
     const unsigned long long gtag = shift ? static_cast<unsigned long long>(g + 1) << shift : 0ull;
 #pragma unroll
     for (uint32_t k = 0; k < kBatchPpt; ++k) {
+      if (k >= ppt) break;  // block-uniform
       const bool live = val[k] && g != skip[k];
       bool won = false;
       uint64_t c = 0;
@@ -284,7 +326,7 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
       __syncthreads();
       const uint32_t pending = s.out_count;
       __syncthreads();
-      if (pending + kBatchTile > kBatchOut) batch_flush(a, s);
+      if (pending + tile > kBatchOut) batch_flush(a, s);
     }
   }
   batch_flush(a, s);
@@ -299,14 +341,12 @@ __device__ __forceinline__ void batch_tile(const TileArgs a, BatchSmem& s) {
 // instance's generator program into shared memory when it changes, and
 // stages its winners for one segment reservation per flush.
 __device__ __forceinline__ void expand_layer(const BatchParams& p, BatchSmem& s) {
-  const uint32_t parity = p.ctl->parity;
   const unsigned long long tiles = p.ctl->tiles;
-  // Select, not index: a runtime index into the parameter block would copy it
-  // to local memory.
-  const TileArgs a{parity ? p.buf[1] : p.buf[0], parity ? p.buf[0] : p.buf[1], p.bitmap, p.next_count};
+  const TileArgs a{p.bitmap, p.next_count};
   if (threadIdx.x == 0) {
     s.out_count = 0;
     s.inst = 0xffffffffu;
+    s.ppt = p.ctl->ppt;
   }
   for (;;) {
     __syncthreads();
@@ -332,14 +372,18 @@ __device__ __forceinline__ void expand_layer(const BatchParams& p, BatchSmem& s)
       if (in.bytes)
         for (uint32_t k = threadIdx.x; k < 6 * in.gens; k += blockDim.x) s.sel[k] = p.sel[in.sel_off + k];
       if (threadIdx.x == 0) {
+        // Select, not index: a runtime index into the parameter block would
+        // copy it to local memory.
+        const uint32_t cur = in.par, nxt = in.par ^ 1u;
         s.inst = i;
         s.n = in.n;
         s.gens = in.gens;
         s.shift = in.gen_shift;
         s.bytes = in.bytes;
         s.bitmap_off = in.bitmap_off;
-        s.seg_off = in.seg_off;
-        s.seg_cap = in.seg_cap;
+        s.front = (cur ? p.buf[1] : p.buf[0]) + (cur ? in.seg_off[1] : in.seg_off[0]);
+        s.next = (nxt ? p.buf[1] : p.buf[0]) + (nxt ? in.seg_off[1] : in.seg_off[0]);
+        s.seg_cap = nxt ? in.seg_cap[1] : in.seg_cap[0];
         s.count = p.cur_count[i];
       }
       __syncthreads();
@@ -378,8 +422,11 @@ struct FinalizeSmem {
 };
 
 __device__ unsigned long long finalize_layer(const BatchParams& p, FinalizeSmem& f) {
-  const uint32_t depth = p.ctl->depth;
-  if (threadIdx.x == 0) f.carry = f.entries = 0;
+  const uint32_t step = p.ctl->step, max_depth = p.ctl->max_depth;
+  if (threadIdx.x == 0) {
+    f.carry = f.entries = 0;
+    p.ctl->reloc_count = 0;  // the moves of the previous step are done
+  }
   __syncthreads();
   for (uint32_t base = 0; base < p.count; base += blockDim.x) {
     const uint32_t i = base + threadIdx.x;
@@ -387,22 +434,47 @@ __device__ unsigned long long finalize_layer(const BatchParams& p, FinalizeSmem&
     if (i < p.count) {
       BatchInst& in = p.inst[i];
       const unsigned long long produced = p.next_count[i];
-      p.next_count[i] = 0;
+      unsigned long long frontier = 0;  // the instance's frontier entries in the next step
+      unsigned long long stored = 0;    // entries already in its next segment at the next step
       if (in.status == INST_ACTIVE) {
-        if (produced > in.seg_cap) {
-          in.status = INST_OVERFLOW;
+        const uint32_t nb = in.par ^ 1u;
+        const unsigned long long cap = in.seg_cap[nb];
+        if (produced > cap) {
+          // Every winner of the failed attempt was counted, so `produced`
+          // bounds the layer: a segment of that size cannot overflow again.
+          // The first `cap` winners were stored (and keep their bits); they
+          // move to the new segment, the rest are found again by the redo.
+          const unsigned long long off = atomicAdd(&p.ctl->pool_used, produced);
+          if (off + produced <= p.ctl->pool_cap) {
+            const uint32_t j = atomicAdd(&p.ctl->reloc_count, 1u);
+            p.reloc[j] = BatchReloc{in.seg_off[nb], p.ctl->pool_base + off, cap, nb, 0u};
+            in.seg_off[nb] = p.ctl->pool_base + off;
+            in.seg_cap[nb] = produced;
+            stored = cap;
+            frontier = p.cur_count[i];
+            atomicAdd(&p.ctl->redo_layers, 1u);
+          } else {
+            in.status = INST_OVERFLOW;  // pool exhausted: rerun from depth 0 later
+          }
         } else if (produced == 0) {
           in.status = INST_DONE;
-        } else if (depth + 1 >= p.ctl->max_depth) {
+        } else if (in.depth + 1 >= max_depth) {
           in.status = INST_OVERFLOW;
           atomicOr(&p.ctl->error, ERR_FRONTIER_OVERFLOW);
         } else {
-          p.layers[static_cast<unsigned long long>(i) * p.ctl->max_depth + depth + 1] = produced;
-          c = (produced + kBatchTile - 1) / kBatchTile;
-          atomicAdd(&f.entries, produced);
+          const unsigned long long row = static_cast<unsigned long long>(i) * max_depth + in.depth + 1;
+          p.layers[row] = produced;
+          p.layer_step[row] = step;
+          in.depth += 1;
+          in.par = nb;
+          frontier = produced;
         }
       }
-      p.cur_count[i] = c ? produced : 0ull;
+      p.next_count[i] = stored;
+      p.cur_count[i] = frontier;
+      const unsigned long long tile = kBatchBlock * p.ctl->ppt;
+      c = (frontier + tile - 1) / tile;
+      if (frontier) atomicAdd(&f.entries, frontier);
     }
     // Block-wide exclusive scan of c.
     unsigned long long incl = c;
@@ -432,16 +504,33 @@ __device__ unsigned long long finalize_layer(const BatchParams& p, FinalizeSmem&
   if (threadIdx.x == 0) {
     unsigned long long now;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-    if (depth + 1 <= p.ctl->max_depth) p.stamps[depth + 1] = now;
+    if (step + 1 <= p.ctl->max_steps) p.stamps[step + 1] = now;
     p.tile_prefix[p.count] = f.carry;
     p.ctl->tiles = f.carry;
     p.ctl->next_tile = 0;
     p.ctl->total = f.entries;
-    p.ctl->parity ^= 1u;
-    p.ctl->depth = depth + 1;
+    p.ctl->step = step + 1;
   }
   __syncthreads();
   return f.carry;
+}
+
+// The moves queued by the last finalize, by every thread of the grid.
+__device__ __forceinline__ void relocate_segments(const BatchParams& p, uint32_t moves) {
+  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  for (uint32_t j = 0; j < moves; ++j) {
+    const BatchReloc r = p.reloc[j];
+    unsigned long long* b = r.buf ? p.buf[1] : p.buf[0];
+    for (unsigned long long k = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; k < r.count;
+         k += stride)
+      b[r.dst + k] = b[r.src + k];
+  }
+}
+
+// The moves as their own launch (graph and host loops), after batch_finalize.
+__global__ void __launch_bounds__(kBatchBlock) batch_relocate(BatchParams p) {
+  const uint32_t moves = *reinterpret_cast<volatile uint32_t*>(&p.ctl->reloc_count);
+  relocate_segments(p, moves);
 }
 
 // The finalize step as its own one-block launch (graph and host loops); in
@@ -463,13 +552,24 @@ __global__ void __launch_bounds__(kBatchBlock, kBatchBlocksPerSM) batch_wave(Bat
   __shared__ BatchSmem s;
   __shared__ FinalizeSmem f;
   __shared__ int more;
+  __shared__ uint32_t moves;
   for (;;) {
     expand_layer(p, s);
     if (!grid_barrier(&p.ctl->bar_count, &p.ctl->bar_gen, &p.ctl->error)) return;
     if (blockIdx.x == 0) finalize_layer(p, f);
     if (!grid_barrier(&p.ctl->bar_count, &p.ctl->bar_gen, &p.ctl->error)) return;
-    if (threadIdx.x == 0) more = *reinterpret_cast<volatile unsigned long long*>(&p.ctl->tiles) > 0;
+    if (threadIdx.x == 0) {
+      more = *reinterpret_cast<volatile unsigned long long*>(&p.ctl->tiles) > 0;
+      moves = *reinterpret_cast<volatile uint32_t*>(&p.ctl->reloc_count);
+    }
     __syncthreads();
+    // A layer redo moves stored winners first; only then may the redo claim.
+    // `moves` is the same in every block (read after the barrier that follows
+    // the finalize), so all blocks take this barrier or none.
+    if (moves) {
+      relocate_segments(p, moves);
+      if (!grid_barrier(&p.ctl->bar_count, &p.ctl->bar_gen, &p.ctl->error)) return;
+    }
     if (!more) return;
   }
 }
@@ -480,7 +580,7 @@ __global__ void batch_seed(BatchParams p) {
     // Identity-coded start: code c at position c.  Its rank is 0.
     unsigned long long start = 0;
     for (uint32_t e = 0; e < in.n; ++e) start |= static_cast<unsigned long long>(e) << (4 * e);
-    p.buf[0][in.seg_off] = start;
+    p.buf[0][in.seg_off[0]] = start;
     p.bitmap[in.bitmap_off] |= 1ull;
     p.tile_prefix[i] = i;  // one entry, one tile per instance
     p.cur_count[i] = 1;
@@ -495,9 +595,11 @@ __global__ void batch_seed(BatchParams p) {
     p.ctl->tiles = p.count;
     p.ctl->next_tile = 0;
     p.ctl->total = p.count;
-    p.ctl->parity = 0;
-    p.ctl->depth = 0;
+    p.ctl->step = 0;
     p.ctl->error = 0;
+    p.ctl->reloc_count = 0;
+    p.ctl->redo_layers = 0;
+    p.ctl->pool_used = 0;
   }
 }
 
@@ -637,9 +739,12 @@ static int batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int dev
   return MGBFS2_OK;
 }
 
-// Runs one wave (the instances in `ids`, with segment capacities `caps`).
-static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& caps, uint32_t max_depth,
-                    uint32_t ppt, uint32_t loop, mgbfs2_batch_status* st, double* kernel_seconds) {
+// Runs one wave (the instances in `ids`, with segment capacities `caps`, and
+// `pool` spare entries in each frontier buffer for layer redos).
+static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& caps, uint64_t pool,
+                    uint32_t max_depth, uint32_t ppt, uint32_t tile_ppt, uint32_t loop, mgbfs2_batch_status* st,
+                    double* kernel_seconds) {
+  TraceRange range("batch.wave");
   const uint32_t W = static_cast<uint32_t>(ids.size());
   std::vector<BatchInst> host(W);
   std::vector<Term> terms;
@@ -662,10 +767,15 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     h.status = INST_ACTIVE;
     h.bitmap_off = bitmap_words;
     bitmap_words += (in.orbit + 63) / 64;
-    h.seg_off = seg;
-    h.seg_cap = caps[k];
+    h.seg_off[0] = h.seg_off[1] = seg;
+    h.seg_cap[0] = h.seg_cap[1] = caps[k];
+    h.par = 0;
+    h.depth = 0;
     seg += caps[k] + 1;  // +1 keeps every segment non-empty
   }
+  // Every layer is redone at most once (a redo's segment holds the failed
+  // attempt's exact winner count), so a wave takes at most 2 * max_depth steps.
+  const uint32_t max_steps = 2 * max_depth;
   // Arena: instance table | terms | tbegin | inverse | tile prefix | counts | next counts | layers | ctl |
   // bitmaps | buf0 | buf1
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -679,17 +789,23 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   const size_t o_cur = off; off = al(off + W * 8);
   const size_t o_next = off; off = al(off + W * 8);
   const size_t o_layers = off; off = al(off + static_cast<size_t>(W) * max_depth * 8);
-  const size_t o_stamps = off; off = al(off + (static_cast<size_t>(max_depth) + 1) * 8);
+  const size_t o_step = off; off = al(off + static_cast<size_t>(W) * max_depth * 4);
+  const size_t o_stamps = off; off = al(off + (static_cast<size_t>(max_steps) + 1) * 8);
+  const size_t o_reloc = off; off = al(off + W * sizeof(BatchReloc));
   const size_t o_ctl = off; off = al(off + sizeof(BatchCtl));
   const size_t o_bitmap = off; off = al(off + bitmap_words * 8);
-  const size_t o_buf0 = off; off = al(off + seg * 8);
-  const size_t o_buf1 = off; off = al(off + seg * 8);
+  const size_t o_buf0 = off; off = al(off + (seg + pool) * 8);
+  const size_t o_buf1 = off; off = al(off + (seg + pool) * 8);
   // Exact size: waves are planned against the memory budget, so no headroom.
   int rc = b->arena.ensure(off, true);
   if (rc) return rc;
   char* base = static_cast<char*>(b->arena.ptr);
   BatchCtl ctl{};
   ctl.max_depth = max_depth;
+  ctl.max_steps = max_steps;
+  ctl.pool_base = seg;
+  ctl.pool_cap = pool;
+  ctl.ppt = tile_ppt;
   MG_CHECK_BATCH(cudaMemcpyAsync(base + o_inst, host.data(), W * sizeof(BatchInst), cudaMemcpyHostToDevice, b->stream));
   if (!terms.empty())
     MG_CHECK_BATCH(cudaMemcpyAsync(base + o_terms, terms.data(), terms.size() * sizeof(Term), cudaMemcpyHostToDevice, b->stream));
@@ -715,7 +831,9 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   p.cur_count = reinterpret_cast<unsigned long long*>(base + o_cur);
   p.next_count = reinterpret_cast<unsigned long long*>(base + o_next);
   p.layers = reinterpret_cast<unsigned long long*>(base + o_layers);
+  p.layer_step = reinterpret_cast<uint32_t*>(base + o_step);
   p.stamps = reinterpret_cast<unsigned long long*>(base + o_stamps);
+  p.reloc = reinterpret_cast<BatchReloc*>(base + o_reloc);
   p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);
   batch_seed<<<std::max<uint32_t>(1, (W + 255) / 256), 256, 0, b->stream>>>(p);
   ++st->kernel_launches;
@@ -768,6 +886,7 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     MG_CHECK_BATCH(cudaStreamBeginCaptureToGraph(cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     batch_expand<<<grid, kBatchBlock, 0, cap_stream>>>(p);
     batch_finalize<<<1, 1024, 0, cap_stream>>>(p, handle, 1);
+    batch_relocate<<<grid, kBatchBlock, 0, cap_stream>>>(p);
     MG_CHECK_BATCH(cudaStreamEndCapture(cap_stream, &body));
     cudaGraphExec_t exec;
     MG_CHECK_BATCH(cudaGraphInstantiate(&exec, graph, 0));
@@ -781,7 +900,8 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     for (;;) {
       batch_expand<<<grid, kBatchBlock, 0, b->stream>>>(p);
       batch_finalize<<<1, 1024, 0, b->stream>>>(p, cudaGraphConditionalHandle{}, 0);
-      st->kernel_launches += 2;
+      batch_relocate<<<grid, kBatchBlock, 0, b->stream>>>(p);
+      st->kernel_launches += 3;
       BatchCtl h{};
       MG_CHECK_BATCH(cudaMemcpyAsync(&h, p.ctl, sizeof(h), cudaMemcpyDeviceToHost, b->stream));
       MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
@@ -803,11 +923,14 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   MG_CHECK_BATCH(cudaMemcpyAsync(done.data(), p.inst, W * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(layers.data(), p.layers, layers.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, b->stream));
-  std::vector<unsigned long long> stamps(static_cast<size_t>(max_depth) + 1, 0);
+  std::vector<unsigned long long> stamps(static_cast<size_t>(max_steps) + 1, 0);
   MG_CHECK_BATCH(cudaMemcpyAsync(stamps.data(), p.stamps, stamps.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  std::vector<uint32_t> steps(static_cast<size_t>(W) * max_depth);
+  MG_CHECK_BATCH(cudaMemcpyAsync(steps.data(), p.layer_step, steps.size() * 4, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
-  if (loop == kLoopGraph) st->kernel_launches += 2 * hc.depth;
-  st->layer_steps += hc.depth;
+  if (loop == kLoopGraph) st->kernel_launches += 3 * hc.step;
+  st->layer_steps += hc.step;
+  st->redo_layers += hc.redo_layers;
   for (uint32_t k = 0; k < W; ++k) {
     auto& in = b->inst[ids[k]];
     in.status = done[k].status;
@@ -817,9 +940,13 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     if (in.status == INST_DONE) {
       for (uint32_t d = 0; d < max_depth && layers[static_cast<size_t>(k) * max_depth + d]; ++d) {
         in.layers.push_back(layers[static_cast<size_t>(k) * max_depth + d]);
-        // Layer d >= 1 is the wave's expansion step d - 1 (shared by the
-        // wave's instances); depth 0 is the seed.
-        const double dt = d && stamps[d] > stamps[d - 1] ? (stamps[d] - stamps[d - 1]) * 1e-9 : 0.0;
+        // Layer d >= 1 came from the wave's step t (shared by the wave's
+        // instances, stamped at its end); depth 0 is the seed.
+        double dt = 0.0;
+        if (d) {
+          const uint32_t t = steps[static_cast<size_t>(k) * max_depth + d];
+          if (t < max_steps && stamps[t + 1] > stamps[t]) dt = (stamps[t + 1] - stamps[t]) * 1e-9;
+        }
         in.layer_seconds.push_back(dt);
       }
     }
@@ -859,10 +986,13 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
   const uint32_t ppt = o.blocks_per_sm;
   const uint32_t loop = o.host_loop;
   if (loop > kLoopGraph) return MGBFS2_INVALID_ARGUMENT;
+  const uint32_t tile = o.tile_entries ? o.tile_entries : kBatchTile;
+  if (tile != kBatchBlock && tile != 2 * kBatchBlock && tile != 4 * kBatchBlock) return MGBFS2_INVALID_ARGUMENT;
+  const uint32_t tile_ppt = tile / kBatchBlock;
   MG_CHECK_BATCH(cudaSetDevice(b->device));
   size_t free_bytes = 0, total_bytes = 0;
   MG_CHECK_BATCH(cudaMemGetInfo(&free_bytes, &total_bytes));
-  free_bytes += pool_idle_bytes(b->device) + b->arena.bytes;
+  free_bytes += pool_idle_bytes(b->device) + device_cache_bytes(b->device) + b->arena.bytes;
   const uint64_t reserve = o.reserve_bytes ? o.reserve_bytes : (2ull << 30);
   uint64_t budget = o.memory_bytes ? o.memory_bytes : (free_bytes > reserve ? free_bytes - reserve : 0);
   mgbfs2_batch_status st{};
@@ -886,21 +1016,35 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
   int rc = MGBFS2_OK;
   while (!pending.empty() && !rc) {
     // Fill a wave up to the memory budget (bitmap + two segments + tables).
+    // Waves whose capacities are predictions keep an eighth of the budget as
+    // the redo pool: an instance whose layer outgrows its segment moves to a
+    // larger one from there and redoes that layer only.
     std::vector<uint32_t> wave;
     std::vector<uint64_t> caps;
-    uint64_t used = 1 << 20;
+    uint64_t used = 1 << 20, short_by = 0, orbits = 0;
+    bool predicted = false;
+    for (uint32_t i : pending) predicted = predicted || cap[i] < b->inst[i].orbit;
+    const uint64_t fill = predicted ? budget - budget / 8 : budget;
     std::vector<uint32_t> later;
     for (uint32_t i : pending) {
-      const uint64_t need = (b->inst[i].orbit + 63) / 64 * 8 + 2 * (cap[i] + 1) * 8 + 8ull * max_depth + 128;
-      if (wave.empty() || used + need <= budget) {
+      const uint64_t need = (b->inst[i].orbit + 63) / 64 * 8 + 2 * (cap[i] + 1) * 8 + 12ull * max_depth + 160;
+      if (wave.empty() || used + need <= fill) {
         wave.push_back(i);
         caps.push_back(cap[i]);
         used += need;
+        short_by += b->inst[i].orbit - cap[i];
+        orbits += b->inst[i].orbit;
       } else {
         later.push_back(i);
       }
     }
-    rc = run_wave(b, wave, caps, max_depth, ppt, loop, &st, &kernel_seconds);
+    // Pool entries (both buffers): what is left of the budget, at most twice
+    // the wave's orbits.  An instance redoes each layer at most once, with a
+    // segment of that layer's winner count (a state won again after a winner
+    // released its bit counts again), so its redo segments rarely sum to more
+    // than twice its orbit; a pool that runs out falls back to the rerun.
+    const uint64_t pool = predicted && short_by && budget > used ? std::min((budget - used) / 16, 2 * orbits) : 0;
+    rc = run_wave(b, wave, caps, pool, max_depth, ppt, tile_ppt, loop, &st, &kernel_seconds);
     ++st.waves;
     for (uint32_t i : wave) {
       if (b->inst[i].status == INST_OVERFLOW) {
@@ -942,6 +1086,22 @@ int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint6
   return MGBFS2_OK;
 }
 
+int mgbfs2_batch_layer_tables(const mgbfs2_batch* batch, uint64_t* tables, uint64_t capacity, uint64_t* offsets) {
+  if (!batch || !offsets) return MGBFS2_INVALID_ARGUMENT;
+  const auto& inst = batch->impl->inst;
+  uint64_t run = 0;
+  for (size_t i = 0; i < inst.size(); ++i) {
+    offsets[i] = run;
+    run += inst[i].layers.size();
+  }
+  offsets[inst.size()] = run;
+  if (!tables) return MGBFS2_OK;
+  if (capacity < run) return MGBFS2_CAPACITY;
+  for (size_t i = 0; i < inst.size(); ++i)
+    std::copy(inst[i].layers.begin(), inst[i].layers.end(), tables + offsets[i]);
+  return MGBFS2_OK;
+}
+
 int mgbfs2_batch_layer_seconds(const mgbfs2_batch* batch, uint32_t instance, double* seconds, size_t capacity,
                                size_t* count) {
   if (!batch || !count || instance >= batch->impl->inst.size()) return MGBFS2_INVALID_ARGUMENT;
@@ -956,7 +1116,10 @@ void mgbfs2_batch_destroy(mgbfs2_batch* batch) {
   if (!batch) return;
   Batch* b = batch->impl;
   cudaSetDevice(b->device);
-  b->arena.free();
+  // Nothing of the batch is in flight after this: the arena goes to the
+  // device cache, where the next batch or graph handle takes it.
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  b->arena.release_to_cache(b->device);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   delete batch;

@@ -61,14 +61,35 @@ def test_batch_loop_modes_agree():
             sweep_opts.close()
 
 
-def test_batch_overflow_reruns_exactly_and_waves():
+def test_batch_overflow_redoes_layers_exactly():
     from multigpubfs_b200.batch import BatchSweep
     graphs = _instances(24, False, 99)
     expect = _oracle_tables(graphs)
     with BatchSweep(graphs) as sweep:
-        # Capacities far too small: every instance overflows once and is rerun
-        # with its orbit bound; a small memory budget forces several waves.
-        st = sweep.run(capacities=[4] * len(graphs), memory_bytes=96 << 20)
+        # Capacities far too small: every instance overflows, and each
+        # overflowing layer is redone in a larger segment from the wave's pool
+        # (with the whole device's budget the pool never runs out).
+        st = sweep.run(capacities=[4] * len(graphs))
+        assert sweep.layer_tables() == expect
+        assert st["redo_layers"] >= len(graphs) and st["redo_instances"] == 0 and st["waves"] == 1
+        # The same through the graph and host loops (the moves as their own launch).
+        for kw in ({"graph_loop": True}, {"host_loop": True}):
+            other = sweep.run(capacities=[4] * len(graphs), **kw)
+            assert sweep.layer_tables() == expect
+            assert other["redo_layers"] >= len(graphs) and other["redo_instances"] == 0
+        # A tighter budget: redos while the pool lasts, reruns after.
+        tight = sweep.run(capacities=[4] * len(graphs), memory_bytes=96 << 20)
+        assert sweep.layer_tables() == expect and tight["redo_layers"] > 0
+
+
+def test_batch_exhausted_pool_reruns_exactly_and_waves():
+    from multigpubfs_b200.batch import BatchSweep
+    graphs = _instances(24, False, 99)
+    expect = _oracle_tables(graphs)
+    with BatchSweep(graphs) as sweep:
+        # A budget so small that the redo pool runs out: those instances are
+        # rerun from depth 0 with their orbit bound in later waves.
+        st = sweep.run(capacities=[4] * len(graphs), memory_bytes=16 << 20)
         assert sweep.layer_tables() == expect
         assert st["redo_instances"] > 0 and st["waves"] > 1
 
@@ -104,3 +125,49 @@ def test_batch_results_tables(tmp_path):
     for r in rows:
         got.setdefault(int(r["instance"]), []).append(int(r["count"]))
     assert [got[i] for i in range(len(expect))] == expect
+
+
+# ---------------------------------------------------------------------------
+# The batched workloads exactly as the benchmark runs them, against the
+# oracle's tables in tests/golden/sweep_tables.json.
+
+def test_sweep512_matches_fixture():
+    """All 512 sweep instances in one run (one wave on a B200)."""
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    from tests.conftest import sweep_fixture
+    expect = sweep_fixture("sweep512")["tables"]
+    with BatchSweep(workloads.sweep(512)) as sweep:
+        st = sweep.run()
+        assert sweep.layer_tables() == expect
+    assert st["complete_instances"] == 512 and st["states"] == sum(map(sum, expect))
+
+
+def test_heldout_sweep_matches_fixture_in_many_waves():
+    """The held-out sweep under a 256 MiB budget: dozens of waves."""
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    from tests.conftest import sweep_fixture
+    expect = sweep_fixture("sweep512_heldout")["tables"]
+    with BatchSweep(workloads.sweep(512, seed_base=20261203 + 4096)) as sweep:
+        st = sweep.run(memory_bytes=256 << 20)
+        assert sweep.layer_tables() == expect
+    assert st["waves"] > 10 and st["complete_instances"] == 512
+
+
+def test_planner_s12_instances_match_fixture():
+    """Eight S12 planner instances (2-4 random generators plus inverses), with
+    the plain capacities and with capacities far below their peak layers
+    (every instance overflows and is recovered exactly)."""
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    from tests.conftest import sweep_fixture
+    fixture = sweep_fixture("planner_s12")
+    graphs = [workloads.planner_instance(i) for i in fixture["indices"]]
+    with BatchSweep(graphs) as sweep:
+        plain = sweep.run()
+        assert sweep.layer_tables() == fixture["tables"]
+        small = sweep.run(capacities=[max(t) // 3 for t in fixture["tables"]])
+        assert sweep.layer_tables() == fixture["tables"]
+    assert plain["redo_layers"] == plain["redo_instances"] == 0
+    assert small["redo_layers"] >= len(graphs) and small["redo_instances"] == 0
