@@ -80,7 +80,24 @@ typedef struct {
   uint32_t bucket_margin;  /* extra entries per shard bucket, 0 = 4096; UINT32_MAX = none */
   uint64_t bucket_min_work; /* successors per layer from which layers are bucketed or grouped, 0 = 2^22 */
   uint32_t options;        /* MGBFS2_OPTION_* bits */
-  uint32_t reserved;
+  uint32_t hash_load_percent; /* largest fill of the all-visited hash table before it grows, in percent
+                                 (10..95, 0 = 50) */
+  /* MGBFS2_PLANNER_LEARNED: the predicted number of states the BFS settles and
+   * its predicted largest layer (e.g. |G| by Schreier-Sims and the planner
+   * network's rollout).  Required with that planner (MGBFS2_INVALID_ARGUMENT
+   * without them).  They replace the worst-case state bound when choosing
+   * between the bitmap and the hash (auto) and when sizing the hash table,
+   * and pre-size the frontier buffers; an under-prediction costs a table
+   * growth or a buffer growth, never a different table.  Ignored by the plain
+   * planner. */
+  uint64_t predicted_states;
+  uint64_t predicted_peak;
+  /* Shapes (the autotuner's choices): parents per work item of grouped layers
+   * (0 = 4096), and resident blocks per SM of the layer-expansion kernels
+   * (0 = each kernel's default; capped by what its registers and shared
+   * memory allow).  They change speed only. */
+  uint32_t group_chunk;
+  uint32_t blocks_per_sm;
 } mgbfs2_plan_request;
 
 /* Inverse-closed packed graphs tag every frontier state with the generator
@@ -98,6 +115,11 @@ typedef struct {
  * rank from its parent's Lehmer digits (two digits change); this option makes
  * them rank every child from scratch instead. */
 #define MGBFS2_OPTION_FULL_RANK 4u
+/* The all-visited hash of one-word states keeps each key in a 32-bit slot
+ * when its bits allow (the slot index and the slot together hold a bijective
+ * mix of the key: exact, half the bytes); this option keeps 64-bit slots
+ * holding the key itself instead. */
+#define MGBFS2_OPTION_WIDE_SLOTS 8u
 
 typedef struct {
   uint32_t visited, dedup;
@@ -115,6 +137,12 @@ typedef struct {
   uint32_t planner;
   uint32_t parent_skip;     /* 1 = parent-edge skip active */
   uint32_t bucket_prefix;   /* bucket shards: states sharing their first k symbols */
+  uint32_t table_slot_bytes; /* all-visited hash: 4 = quotient slots, 8 = key slots, 0 = no table */
+  uint32_t hash_load_percent; /* the table's growth threshold */
+  uint32_t group_chunk;      /* parents per grouped work item */
+  uint32_t blocks_per_sm;    /* requested resident blocks per SM, 0 = kernel defaults */
+  uint32_t rank_components;  /* bitmap: position components of the rank domain (1 = the whole multiset) */
+  uint32_t reserved;
 } mgbfs2_plan_info;
 
 typedef struct {
@@ -174,10 +202,49 @@ MGBFS2_API int mgbfs2_layer_table(const mgbfs2_graph* graph, uint64_t* sizes, do
  * row-major, elements per row. */
 MGBFS2_API int mgbfs2_sample(mgbfs2_graph* graph, uint32_t which, int64_t* out, size_t capacity_rows, size_t* rows);
 
+/* Checkpoint of a BFS between layers (after mgbfs2_run returned at a layer
+ * limit, deadline or cancel, or complete): the layer table, the visited
+ * structure (bitmap or all-visited hash), the deepest layer and the small-layer
+ * samples, written to `path`.  Bitmap and all-visited hash plans of one-word
+ * states (three-bank histories and wide states: MGBFS2_UNSUPPORTED). */
+MGBFS2_API int mgbfs2_checkpoint_write(mgbfs2_graph* graph, const char* path);
+
+/* Loads a checkpoint into a handle planned for the same graph and visited
+ * structure (MGBFS2_INVALID_ARGUMENT when the file, generators, coding or
+ * structure differ); the next mgbfs2_run goes on from the checkpoint's depth
+ * and gives the table of an uninterrupted run.  The reference keeps a layer
+ * archive and restarts from its manifest (scripts/bfs_tail_archive.py,
+ * crates/mgbfs-runtime/src/archive.rs) without resuming a search. */
+MGBFS2_API int mgbfs2_checkpoint_resume(mgbfs2_graph* graph, const char* path);
+
+/* The deepest layer's packed states (parent-edge tags removed): *count
+ * receives its size; with out non-NULL and capacity >= *count they are copied
+ * to out.  Valid after mgbfs2_run and inside its layer callback (the layer just
+ * recorded), so a caller can archive every layer, as the reference's layer
+ * archive does (scripts/bfs_tail_archive.py:96-131). */
+MGBFS2_API int mgbfs2_frontier_words(mgbfs2_graph* graph, uint64_t* out, size_t capacity, size_t* count);
+
 /* Static message for a status code (reference: native_fault.rs error markers). */
 MGBFS2_API const char* mgbfs2_status_string(int code);
 
+/* Destroying a handle keeps its device buffers in a per-device cache of the
+ * library (and the stream-ordered pool keeps freed memory reserved), so the
+ * next handle on the device allocates nothing.  This returns both to the
+ * device: it frees the cached buffers and trims the pool.  Call it with no
+ * handle or batch of the device running.  No reference counterpart: the
+ * reference runs each graph in a CLI process whose exit frees everything
+ * (crates/mgbfs-cli/src/main.rs:191-200). */
+MGBFS2_API int mgbfs2_trim_memory(int device);
+
 MGBFS2_API void mgbfs2_destroy(mgbfs2_graph* graph);
+
+/* A named range on a profiler's timeline (NVTX), for callers that mark their
+ * own phases around the library's; the library marks its own (plan, run, each
+ * layer by kernel family, batch waves).  Replaces mgbfs_trace_range_push/pop,
+ * cuda/profile_ranges.cpp:6-24, which are compiled in only with MGBFS_NVTX;
+ * NVTX v3 is header-only, so these are always present. */
+MGBFS2_API void mgbfs2_trace_range_push(const char* label);
+MGBFS2_API void mgbfs2_trace_range_pop(void);
 
 /* ------------------------------------------------------------------------ */
 /* Kernel-level entry points (caller-owned device buffers, no allocation).    */
@@ -204,6 +271,20 @@ MGBFS2_API int mgbfs2_successors_packed(uint32_t degree, uint32_t bits, uint32_t
  * Invalid states get rank UINT64_MAX and set *error bit 4 (rank range). */
 MGBFS2_API int mgbfs2_rank_packed(uint32_t degree, uint32_t bits, uint32_t distinct, const uint32_t* counts_host,
                        const uint64_t* words, uint64_t count, uint64_t* ranks, uint32_t* error, void* stream);
+
+/* Rank of packed states in the product of the generators' position
+ * components' multiset domains (the bitmap domain of graphs whose generators
+ * keep groups of positions apart): codes_host[i] is the code at position i of
+ * the start (dense codes < distinct), permutations_host the generators
+ * (generators x degree).  *domain_size (optional) receives the product size.
+ * Invalid states get rank UINT64_MAX and set *error bit 4.  Replaces
+ * bitmap_rank over component descriptors, cuda/permutation_bitmap.cuh:62-83,
+ * with the domain of PositionOrbitDomain,
+ * crates/mgbfs-runtime/src/permutation_bitmap.rs:61-143. */
+MGBFS2_API int mgbfs2_rank_components(uint32_t degree, uint32_t bits, uint32_t distinct, const uint32_t* codes_host,
+                                      uint32_t generators, const uint32_t* permutations_host, const uint64_t* words,
+                                      uint64_t count, uint64_t* ranks, uint64_t* domain_size, uint32_t* error,
+                                      void* stream);
 
 /* Test-and-set claim of ranks in a bitmap of `domain` bits; won[i] = 1 for
  * exactly one occurrence of every rank not set before.  warp = 1 merges bits of
@@ -282,18 +363,21 @@ typedef struct {
   uint32_t blocks_per_sm;   /* batch_expand blocks per SM, 0 = occupancy limit (the tuned shape) */
   uint32_t host_loop;       /* layer loop of a wave: 0 = one persistent cooperative launch (grid barriers
                                between layers), 1 = host-driven (one sync per layer), 2 = CUDA-graph WHILE loop */
-  uint32_t reserved;
+  uint32_t tile_entries;    /* frontier entries per work tile: 256, 512 or 1024 (0 = 1024; the tuned shape) */
   uint64_t memory_bytes;    /* device bytes available to the waves, 0 = free memory minus reserve */
   uint64_t reserve_bytes;   /* 0 = 2 GiB */
   const uint64_t* predicted_capacity; /* per instance frontier capacity (learned planner); NULL or 0 = orbit bound */
 } mgbfs2_batch_options;
 
 typedef struct {
-  uint32_t instances, complete_instances, waves, redo_instances;
+  uint32_t instances, complete_instances, waves;
+  uint32_t redo_instances;  /* instances rerun from depth 0 (their wave's redo pool was exhausted) */
   uint32_t graph_launches, kernel_launches, layer_steps, fatal;
   uint64_t states, successors;
   double seconds;           /* wall time of mgbfs2_batch_run */
   double device_seconds;    /* CUDA-event time of the waves' layer loops */
+  uint32_t redo_layers;     /* layers redone in a larger segment after overflowing a predicted capacity */
+  uint32_t reserved;
 } mgbfs2_batch_status;
 
 /* Instances: permutation graphs of degree 2..15 with distinct labels and at
@@ -307,14 +391,25 @@ MGBFS2_API int mgbfs2_batch_create(const mgbfs2_graph_desc* graphs, uint32_t cou
  * default a wave is ONE persistent cooperative launch that expands every active
  * instance's layer, finalizes it behind a bounded grid barrier and repeats
  * until the device finds no active instance (options->host_loop selects the
- * CUDA-graph WHILE form or a host-driven loop instead).  An
- * instance that overflows its (predicted) frontier capacity is rerun from depth
- * 0 with its orbit bound, so tables never change. */
+ * CUDA-graph WHILE form or a host-driven loop instead).  With predicted
+ * capacities an eighth of the budget is kept as a redo pool: a layer that
+ * overflows its instance's segment is redone in a larger segment from the pool
+ * within the same launch (winners that found no room release their bitmap bit,
+ * the stored ones move), so only that layer is repeated.  An instance whose
+ * pool is exhausted is rerun from depth 0 with its orbit bound in a later
+ * wave.  Tables never depend on the capacities. */
 MGBFS2_API int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, mgbfs2_batch_status* status);
 
 /* Layer table of one instance after mgbfs2_batch_run. */
 MGBFS2_API int mgbfs2_batch_layer_table(const mgbfs2_batch* batch, uint32_t instance, uint64_t* sizes,
                                         size_t capacity, size_t* count);
+
+/* Every instance's layer table in one call: instance i's table is
+ * tables[offsets[i] .. offsets[i + 1]) (offsets: count + 1 entries).  With
+ * tables NULL (or capacity too small) only the offsets are written, and
+ * MGBFS2_CAPACITY is returned when tables is given but too small. */
+MGBFS2_API int mgbfs2_batch_layer_tables(const mgbfs2_batch* batch, uint64_t* tables, uint64_t capacity,
+                                         uint64_t* offsets);
 
 /* Expansion seconds of each layer of one instance after mgbfs2_batch_run,
  * aligned with its layer table: entry d >= 1 is the device time (globaltimer)

@@ -1,5 +1,6 @@
-"""Pilot-run autotuner: picks the visited-set path of one graph by timing the
-candidate plans on the graph's own first layers, and caches the choice.
+"""Pilot-run autotuner: picks the visited-set path of one graph, then the
+shapes of that path, by timing candidate plans on the graph's own first
+layers, and caches the choice.
 
 Mirrors the reference's tuning layer in what it decides and how (re-designed
 for this engine's plans, not ported):
@@ -13,12 +14,16 @@ for this engine's plans, not ported):
 * a profile cache (multigpubfs/profile_cache.py) keyed by graph digest, device
   name and library build, so a graph is piloted once per machine.
 
-Candidates are the engine's exact paths for the graph: the plain bitmap with
-per-lane or warp-merged atomics, owner-routed bucket layers with one- or
-two-symbol shard prefixes, grouped claim-then-route layers, the
+Stage 1 candidates are the engine's exact paths for the graph: the plain
+bitmap with per-lane or warp-merged atomics, owner-routed bucket layers with
+one- or two-symbol shard prefixes, grouped claim-then-route layers, the
 open-addressing hash and, for inverse-closed graphs, the three-bank hash.
-Results never depend on the choice: every path is exact and the plan only
-changes speed.
+Stage 2 varies the shapes of the path stage 1 kept (`shape_candidates`): the
+work-item size and resident blocks per SM of grouped layers, the bucket
+margin of routed layers, the growth threshold of the hash table, and the
+resident blocks of the fused kernels; the stage-1 plan with default shapes is
+the default trial.  Results never depend on the choice: every path and shape
+is exact and only changes speed.
 """
 from __future__ import annotations
 
@@ -69,6 +74,27 @@ def candidate_plans(graph: GraphDefinition) -> list[dict]:
     return out
 
 
+def shape_candidates(plan: dict, resolved: dict) -> list[dict]:
+    """Stage 2: shape variations of the plan stage 1 kept, default first.
+    `resolved` is the plan info mgbfs2_plan returned for it (the path it
+    resolved to when the request said auto)."""
+    out = [dict(plan)]
+    dedup, visited = resolved.get("dedup"), resolved.get("visited")
+    if dedup == "grouped":
+        for chunk in (2048, 4096, 8192):
+            for blocks in (6, 8):
+                if (chunk, blocks) != (4096, 8):
+                    out.append(dict(plan, group_chunk=chunk, blocks_per_sm=blocks))
+    elif dedup == "bucket":
+        out += [dict(plan, bucket_margin=m) for m in (1024, 16384)]
+    elif visited == "hash":
+        out += [dict(plan, hash_load_percent=f) for f in (50, 90)]
+        out += [dict(plan, blocks_per_sm=b) for b in (4, 8)]
+    elif visited == "bitmap":
+        out += [dict(plan, blocks_per_sm=b) for b in (3, 6)]
+    return out
+
+
 def cache_key(graph: GraphDefinition, device_name: str, build: str) -> str:
     return f"{graph.digest()}|{device_name}|{build}"
 
@@ -111,17 +137,30 @@ def pilot_depth(layer_sizes: list[int], gens: int, work: int = PILOT_WORK) -> in
     return len(layer_sizes)
 
 
-def _run_pilot(graph, plan, device, max_layers, max_seconds):
+def _run_pilot(graph, plan, device, max_layers, max_seconds, info=None):
     from .engine import NativeGraph
     from . import native
     try:
         with NativeGraph(graph, device) as eng:
-            eng.plan(**plan)
+            resolved = eng.plan(**plan)
+            if info is not None:
+                info.update(resolved)
             eng.run(max_layers=max_layers, max_seconds=max_seconds)   # warm: pool memory, module load
             r = eng.run(max_layers=max_layers, max_seconds=max_seconds)
             return r
     except native.NativeError:
         return None
+
+
+def _trials(graph, plans, device, depth, per_trial, first, started, budget_seconds):
+    trials = []
+    for plan in plans:
+        if time.perf_counter() - started > budget_seconds:
+            break
+        r = _run_pilot(graph, plan, device, depth, per_trial)
+        ok = r is not None and r.layer_sizes[:depth] == first.layer_sizes[:depth] and len(r.layer_sizes) >= depth
+        trials.append({"plan": plan, "seconds": r.device_seconds if ok else None})
+    return trials
 
 
 def choose_profile(graph: GraphDefinition, device: int = 0, *, budget_seconds: float = 60.0,
@@ -149,14 +188,16 @@ def choose_profile(graph: GraphDefinition, device: int = 0, *, budget_seconds: f
     if first is None:
         return {"plan": dict(DEFAULT), "source": "pilot", "trials": []}
     depth = pilot_depth(first.layer_sizes, graph.generator_count)
-    trials = []
-    for plan in plans:
-        if time.perf_counter() - started > budget_seconds:
-            break
-        r = _run_pilot(graph, plan, device, depth, per_trial)
-        ok = r is not None and r.layer_sizes[:depth] == first.layer_sizes[:depth] and len(r.layer_sizes) >= depth
-        trials.append({"plan": plan, "seconds": r.device_seconds if ok else None})
+    trials = _trials(graph, plans, device, depth, per_trial, first, started, budget_seconds)
     choice = pick(trials)
+    # Stage 2: the shapes of the kept path, with the same rule.
+    resolved = {}
+    if _run_pilot(graph, choice, device, 1, per_trial, info=resolved) is not None:
+        shapes = shape_candidates(choice, resolved)
+        if len(shapes) > 1:
+            shape_trials = _trials(graph, shapes, device, depth, per_trial, first, started, budget_seconds)
+            choice = pick(shape_trials)
+            trials += shape_trials
     if use_cache:
         entries = load_cache(path)
         entries[key] = {"plan": choice, "trials": trials, "pilot_layers": depth}

@@ -67,9 +67,13 @@ def main(argv=None) -> int:
         print(json.dumps({k: report[k] for k in ("status", "reason", "layer_sizes", "bfs_seconds", "backend")}))
         return 0
     from .engine import NativeGraph
+    learned = {"planner": "plain"}
+    if a.planner == "learned":
+        from .planner import choose_path
+        learned = choose_path(graph.to_dict(), device=a.device)
     with NativeGraph(graph, a.device) as engine:
-        plan = engine.plan(visited=a.visited, dedup=a.dedup, capacity=a.capacity, planner=a.planner,
-                           shards=a.shards, host_loop=a.host_loop)
+        plan = engine.plan(visited=a.visited, dedup=a.dedup, capacity=a.capacity, shards=a.shards,
+                           host_loop=a.host_loop, **learned)
         if a.verb == "plan":
             print(json.dumps({"graph": graph.name, "digest": graph.digest(), "plan": plan}))
             return 0

@@ -47,15 +47,28 @@ __device__ __forceinline__ void raise_error(unsigned int* error, uint32_t bits) 
   atomicOr(error, bits);
 }
 
-constexpr uint32_t kBarrierPolls = 1u << 22;
+// A grid barrier waits for the slowest block to finish its share of a layer,
+// so its bound is device time, not a poll count: 30 s of %globaltimer, two
+// orders of magnitude above the longest layer of the workloads here (the
+// largest fused S13 layer takes about 60 ms; a block's wait is at most one
+// layer).  The poll cap is a second bound that holds even if the timer were
+// to stop.
+constexpr unsigned long long kBarrierWaitNs = 30ull * 1000 * 1000 * 1000;
+constexpr uint32_t kBarrierPolls = 1u << 30;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  return now;
+}
 
 // Grid-wide barrier of a cooperative launch, with a bounded wait.  Thread 0
 // of each block arrives on *count; the last to arrive resets it and advances
-// *gen with a release store; the others poll *gen with acquire loads, at most
-// kBarrierPolls times, after which they raise ERR_WAIT_LIMIT in *error and
-// return false (the caller then ends the kernel: nothing waits forever).
-// Every thread orders its later loads after the barrier.  *count and *gen
-// start at zero for each launch.
+// *gen with a release store; the others poll *gen with acquire loads until
+// kBarrierWaitNs have passed (or kBarrierPolls polls), after which they raise
+// ERR_WAIT_LIMIT in *error and return false (the caller then ends the kernel:
+// nothing waits forever).  Every thread orders its later loads after the
+// barrier.  *count and *gen start at zero for each launch.
 __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen, unsigned int* error) {
   __shared__ int barrier_ok;
   __syncthreads();
@@ -68,11 +81,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* 
       *count = 0;
       asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(gen), "r"(g + 1) : "memory");
     } else {
+      const unsigned long long started = global_ns();
       for (uint32_t polls = 0;; ++polls) {
         unsigned int now;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(gen) : "memory");
         if (now != g) break;
-        if (polls >= kBarrierPolls) {
+        if (polls >= kBarrierPolls || ((polls & 255u) == 255u && global_ns() - started > kBarrierWaitNs)) {
           raise_error(error, ERR_WAIT_LIMIT);
           barrier_ok = 0;
           break;
@@ -231,18 +245,16 @@ __device__ __forceinline__ uint64_t scale_floor(uint64_t ways, uint32_t f, uint3
   return (ways / r) * f + ((ways % r) * f) / r;
 }
 
-__device__ __forceinline__ bool multiset_rank(uint64_t w, const MultisetDomain& d, uint64_t* out) {
-  // Byte-lane counts: lane c of (c_lo, c_hi) holds counts[c] (<= 16).
-  uint64_t c_lo = 0, c_hi = 0;
-  for (uint32_t c = 0; c < d.distinct; ++c) {
-    if (c < 8) c_lo |= static_cast<uint64_t>(d.counts[c]) << (8 * c);
-    else c_hi |= static_cast<uint64_t>(d.counts[c]) << (8 * (c - 8));
-  }
-  const uint64_t sym_mask = (1ull << d.bits) - 1;
-  uint64_t ways = d.total, rank = 0;
-  for (uint32_t e = 0; e < d.n; ++e) {
-    const uint32_t s = static_cast<uint32_t>((w >> (d.bits * e)) & sym_mask);
-    if (s >= d.distinct) return false;
+// The rank over byte-lane counts: lane c of (c_lo, c_hi) holds the
+// multiplicity of code c (<= 16); codes of multiplicity 0 may appear in the
+// alphabet and never in the state.
+__device__ __forceinline__ bool multiset_rank_lanes(uint64_t w, uint32_t n, uint32_t bits, uint32_t distinct,
+                                                    uint64_t total, uint64_t c_lo, uint64_t c_hi, uint64_t* out) {
+  const uint64_t sym_mask = (1ull << bits) - 1;
+  uint64_t ways = total, rank = 0;
+  for (uint32_t e = 0; e < n; ++e) {
+    const uint32_t s = static_cast<uint32_t>((w >> (bits * e)) & sym_mask);
+    if (s >= distinct) return false;
     const uint32_t cnt = s < 8 ? static_cast<uint32_t>((c_lo >> (8 * s)) & 0xff)
                                : static_cast<uint32_t>((c_hi >> (8 * (s - 8))) & 0xff);
     if (!cnt) return false;
@@ -251,13 +263,66 @@ __device__ __forceinline__ bool multiset_rank(uint64_t w, const MultisetDomain& 
     uint64_t below_hi = s <= 8 ? 0 : (c_hi & ((1ull << (8 * (s - 8))) - 1));
     const uint32_t less = static_cast<uint32_t>(((below_lo * 0x0101010101010101ull) >> 56) +
                                                 ((below_hi * 0x0101010101010101ull) >> 56));
-    const uint32_t remaining = d.n - e;
+    const uint32_t remaining = n - e;
     rank += scale_floor(ways, less, remaining);
     ways = scale_floor(ways, cnt, remaining);
     if (s < 8) c_lo -= 1ull << (8 * s);
     else c_hi -= 1ull << (8 * (s - 8));
   }
-  if (rank >= d.total || ways != 1) return false;
+  if (rank >= total || ways != 1) return false;
+  *out = rank;
+  return true;
+}
+
+__device__ __forceinline__ bool multiset_rank(uint64_t w, const MultisetDomain& d, uint64_t* out) {
+  uint64_t c_lo = 0, c_hi = 0;
+  for (uint32_t c = 0; c < d.distinct; ++c) {
+    if (c < 8) c_lo |= static_cast<uint64_t>(d.counts[c]) << (8 * c);
+    else c_hi |= static_cast<uint64_t>(d.counts[c]) << (8 * (c - 8));
+  }
+  return multiset_rank_lanes(w, d.n, d.bits, d.distinct, d.total, c_lo, c_hi, out);
+}
+
+// Product of multiset domains over position components: the positions that
+// the generators connect (i ~ g[i]) form components, each keeping its own
+// multiset of labels, so the reachable states lie in the product of the
+// components' multiset permutations.  The rank is mixed-radix over the
+// components in order of their first position, each digit the multiset rank
+// of the component's codes in position order (the contract of
+// cuda/permutation_bitmap.cuh:62-83 and PositionOrbitDomain,
+// crates/mgbfs-runtime/src/permutation_bitmap.rs:61-143).
+constexpr uint32_t kMaxComponents = 16;
+// The visited structure of a packed plan.  V_HASHQ: the all-visited set as
+// a quotient table of 32-bit slots.  V_PRODUCT: a bitmap over the product of
+// the position components' multiset domains.
+enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3, V_HASHQ = 4, V_PRODUCT = 5 };
+
+struct ProductDomain {
+  uint32_t components, bits, distinct, pad;
+  unsigned long long total;
+  unsigned long long positions[kMaxComponents];  // 4-bit position indices, the first in the low nibble
+  unsigned long long radix[kMaxComponents];      // multiset permutations of each component
+  unsigned long long lanes[kMaxComponents][2];   // byte-lane label counts of each component
+  uint32_t length[kMaxComponents];
+};
+
+__device__ __forceinline__ bool product_rank(uint64_t w, const ProductDomain& d, uint64_t* out) {
+  const uint64_t sym_mask = (1ull << d.bits) - 1;
+  uint64_t rank = 0;
+  for (uint32_t c = 0; c < d.components; ++c) {
+    const uint32_t len = d.length[c];
+    const uint64_t pos = d.positions[c];
+    uint64_t compact = 0;
+    for (uint32_t j = 0; j < len; ++j) {
+      const uint32_t at = static_cast<uint32_t>(pos >> (4 * j)) & 15u;
+      compact |= ((w >> (d.bits * at)) & sym_mask) << (d.bits * j);
+    }
+    uint64_t digit = 0;
+    if (!multiset_rank_lanes(compact, len, d.bits, d.distinct, d.radix[c], d.lanes[c][0], d.lanes[c][1], &digit))
+      return false;
+    rank = rank * d.radix[c] + digit;
+  }
+  if (rank >= d.total) return false;
   *out = rank;
   return true;
 }
@@ -285,6 +350,71 @@ __device__ __forceinline__ int hash_insert(unsigned long long* table, uint64_t m
     slot = (slot + 1) & mask;
   }
   return -1;  // probe limit
+}
+
+// ---------------------------------------------------------------------------
+// Quotient set of packed keys in 32-bit slots.  A key of B bits is first
+// mixed by a bijection of the B-bit integers (xorshift-multiply rounds, the
+// construction of MurmurHash3's 64-bit finaliser restricted to B bits: every
+// round is invertible modulo 2^B).  The low s bits of the mixed value x pick
+// the home slot of a table of 2^s slots; the slot stores the other B - s bits
+// of x together with the probe distance j + 1 in its low D = 32 - (B - s)
+// bits (0 = empty).  Slot t then holds the key whose mixed value is
+// (stored >> D) << s | (t - j), so equality is exact and a table of 40 M
+// 44-bit keys takes 4 bytes per slot instead of 8.  Slots only ever go from
+// empty to a key, so a stale read is harmless: an empty read is settled by the
+// CAS, and a key read stays that key.
+__device__ __host__ __forceinline__ uint64_t mix_bits(uint64_t k, uint32_t bits) {
+  const uint64_t m = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+  const uint32_t h = (bits + 1) / 2;
+  uint64_t x = k & m;
+  x ^= x >> h;
+  x = (x * 0xff51afd7ed558ccdull) & m;
+  x ^= x >> h;
+  x = (x * 0xc4ceb9fe1a85ec53ull) & m;
+  x ^= x >> h;
+  return x;
+}
+
+struct QuotientSlots {
+  unsigned int* slots;
+  uint64_t mask;        // 2^s - 1
+  uint32_t s, bits, d;  // log2 slots, key bits B, distance bits D = 32 - (B - s)
+  uint32_t limit;       // probe limit, < 2^D - 1
+};
+
+__device__ __forceinline__ unsigned int load_slot(const unsigned int* slot) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(slot) : "memory");
+  return v;
+}
+
+// First probe of `key`: the home slot's current value.
+__device__ __forceinline__ unsigned int qhash_first(const QuotientSlots& q, uint64_t key) {
+  return load_slot(q.slots + (mix_bits(key, q.bits) & q.mask));
+}
+
+// Insert `key`, given the home slot's value read before (`v`).  Returns 1 if
+// inserted, 0 if present, -1 at the probe limit.
+__device__ __forceinline__ int qhash_resolve(const QuotientSlots& q, uint64_t key, unsigned int v) {
+  const uint64_t x = mix_bits(key, q.bits);
+  const uint64_t home = x & q.mask, rem = x >> q.s;
+  for (uint32_t j = 0; j < q.limit; ++j) {
+    const unsigned int want = static_cast<unsigned int>((rem << q.d) | (j + 1));
+    unsigned int* slot = q.slots + ((home + j) & q.mask);
+    if (j) v = load_slot(slot);
+    if (v == 0u) {
+      const unsigned int prev = atomicCAS(slot, 0u, want);
+      if (prev == 0u) return 1;
+      v = prev;
+    }
+    if (v == want) return 0;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int qhash_insert(const QuotientSlots& q, uint64_t key) {
+  return qhash_resolve(q, key, qhash_first(q, key));
 }
 
 __device__ __forceinline__ bool hash_contains(const unsigned long long* table, uint64_t mask, uint64_t key,

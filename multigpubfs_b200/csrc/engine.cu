@@ -139,6 +139,62 @@ int Graph::create(const mgbfs2_graph_desc* d, int dev, Graph** out, char* error,
   return MGBFS2_OK;
 }
 
+// The product of the position components' multiset domains
+// (permutation_bitmap.rs:61-143): components are the classes of i ~ g[i] over
+// all generators, ordered by their first position, with their positions
+// ascending.  False when a component's domain or the product overflows, or
+// there are more than kMaxComponents components.
+bool build_product_domain(uint32_t n, uint32_t bits, uint32_t distinct, const uint32_t* codes, uint32_t gens,
+                          const uint32_t* perms, ProductDomain* out) {
+  if (!n || n > 16 || (bits != 4 && bits != 8) || !distinct || distinct > 16 || n * bits > 64) return false;
+  std::vector<uint32_t> parent(n);
+  for (uint32_t i = 0; i < n; ++i) parent[i] = i;
+  auto root = [&](uint32_t x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  for (uint32_t k = 0; k < gens; ++k)
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t v = perms[static_cast<size_t>(k) * n + i];
+      if (v >= n) return false;
+      parent[root(i)] = root(v);
+    }
+  std::map<uint32_t, std::vector<uint32_t>> members;  // first position -> positions
+  std::map<uint32_t, uint32_t> first;                  // root -> first position
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t r = root(i);
+    if (!first.count(r)) first[r] = i;
+    members[first[r]].push_back(i);
+  }
+  if (members.size() > kMaxComponents) return false;
+  ProductDomain d{};
+  d.bits = bits;
+  d.distinct = distinct;
+  d.total = 1;
+  for (auto& kv : members) {
+    const uint32_t c = d.components++;
+    std::vector<uint32_t> counts(distinct, 0);
+    for (uint32_t j = 0; j < kv.second.size(); ++j) {
+      d.positions[c] |= static_cast<unsigned long long>(kv.second[j]) << (4 * j);
+      if (codes[kv.second[j]] >= distinct) return false;
+      counts[codes[kv.second[j]]]++;
+    }
+    d.length[c] = static_cast<uint32_t>(kv.second.size());
+    std::vector<uint32_t> present;
+    for (uint32_t code = 0; code < distinct; ++code) {
+      if (counts[code]) present.push_back(counts[code]);
+      if (code < 8) d.lanes[c][0] |= static_cast<unsigned long long>(counts[code]) << (8 * code);
+      else d.lanes[c][1] |= static_cast<unsigned long long>(counts[code]) << (8 * (code - 8));
+    }
+    d.radix[c] = multinomial(present);
+    if (d.radix[c] == UINT64_MAX) return false;
+    d.total = sat_mul(d.total, d.radix[c]);
+    if (d.total == UINT64_MAX) return false;
+  }
+  *out = d;
+  return true;
+}
+
 // Packing, inverse closure, rank domain, state bound and Coxeter certificate.
 void Graph::analyse() {
   const uint32_t n = elements;
@@ -199,6 +255,12 @@ void Graph::analyse() {
       for (auto& kv : c.second) counts.push_back(kv.second);
       state_bound = sat_mul(state_bound, multinomial(counts));
     }
+    // The product domain, when the components split the positions and it is
+    // smaller than the whole multiset domain.
+    product = false;
+    if (packed && (bits == 4 || bits == 8) && distinct <= 16 && comp.size() > 1 && n <= 16 && state_bound < rank_total)
+      product = build_product_domain(n, bits, distinct, codes.data(), gens, perms.data(), &product_domain) &&
+                product_domain.components > 1;
     if (orbit_bound) state_bound = std::min(state_bound, orbit_bound);
     // Coxeter certificate: generators = all adjacent transpositions, distinct
     // labels -> layer k holds the permutations with k inversions.
@@ -369,23 +431,20 @@ void Graph::release() {
   // The pinned mirrors go back to the process-wide cache, where another
   // handle may take them: no copy of this handle's may still be in flight.
   if (stream) cudaStreamSynchronize(stream);
+  // Nothing is in flight now: the buffers go to the device cache, where the
+  // next handle on this device takes them without a pool allocation.
   for (DeviceBuffer* b : {&bitmap, &front, &next, &table, &bank[0], &bank[1], &bank[2], &program, &control_buf,
-                          &scratch})
-    b->free();
+                          &scratch, &buckets, &shard_meta, &group_meta, &loop_buf, &transp_buf})
+    b->release_to_cache(device);
   wide_release();
   if (host_control) {
     pinned_give(host_control);
     host_control = nullptr;
   }
-  buckets.free();
-  shard_meta.free();
   if (host_meta) {
     pinned_give(host_meta);
     host_meta = nullptr;
   }
-  group_meta.free();
-  loop_buf.free();
-  transp_buf.free();
   if (host_group) {
     pinned_give(host_group);
     host_group = nullptr;
@@ -402,7 +461,21 @@ int DeviceBuffer::ensure(size_t want, bool exact) {
   const size_t grown = exact ? want : std::max(want, bytes + bytes / 2);
   free();
   void* p = nullptr;
+  int device = 0;
+  size_t cached = 0;
+  if (cudaGetDevice(&device) == cudaSuccess && device_cache_take(device, grown, &p, &cached)) {
+    ptr = p;
+    bytes = cached;
+    return MGBFS2_OK;
+  }
   cudaError_t e = cudaMallocAsync(&p, grown, stream);
+  if (e == cudaErrorMemoryAllocation && device_cache_bytes(device)) {
+    // Plans count the cached buffers as free memory: give them back to the
+    // pool (stream-ordered, so this stream may reuse them at once) and retry.
+    cudaGetLastError();
+    device_cache_drain(device, stream);
+    e = cudaMallocAsync(&p, grown, stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? MGBFS2_OUT_OF_MEMORY : cuda_status(e);
@@ -416,6 +489,90 @@ void DeviceBuffer::free() {
   if (ptr) cudaFreeAsync(ptr, stream);
   ptr = nullptr;
   bytes = 0;
+}
+
+void DeviceBuffer::release_to_cache(int device) {
+  if (ptr) device_cache_give(device, ptr, bytes);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+namespace {
+std::mutex device_cache_mutex;
+std::map<int, std::multimap<size_t, void*>> device_cache;  // device -> (bytes -> buffer)
+std::map<int, uint64_t> device_cache_total;
+constexpr size_t kDeviceCacheEntries = 64;  // per device; the smallest are freed beyond it
+}  // namespace
+
+bool device_cache_take(int device, size_t want, void** ptr, size_t* bytes) {
+  std::lock_guard<std::mutex> lock(device_cache_mutex);
+  auto d = device_cache.find(device);
+  if (d == device_cache.end()) return false;
+  auto it = d->second.lower_bound(want);
+  if (it == d->second.end()) return false;
+  *ptr = it->second;
+  *bytes = it->first;
+  device_cache_total[device] -= it->first;
+  d->second.erase(it);
+  return true;
+}
+
+void device_cache_give(int device, void* ptr, size_t bytes) {
+  void* evicted = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(device_cache_mutex);
+    auto& entries = device_cache[device];
+    entries.emplace(bytes, ptr);
+    device_cache_total[device] += bytes;
+    if (entries.size() > kDeviceCacheEntries) {
+      evicted = entries.begin()->second;
+      device_cache_total[device] -= entries.begin()->first;
+      entries.erase(entries.begin());
+    }
+  }
+  // An evicted buffer has no work in flight either: free it in stream order
+  // on the legacy stream of the current device, which is `device` here.
+  if (evicted) cudaFreeAsync(evicted, 0);
+}
+
+uint64_t device_cache_bytes(int device) {
+  std::lock_guard<std::mutex> lock(device_cache_mutex);
+  auto it = device_cache_total.find(device);
+  return it == device_cache_total.end() ? 0 : it->second;
+}
+
+// Frees every cached buffer of `device` into its pool, in the order of
+// `stream` (the current device must be `device`).
+void device_cache_drain(int device, cudaStream_t stream) {
+  std::multimap<size_t, void*> entries;
+  {
+    std::lock_guard<std::mutex> lock(device_cache_mutex);
+    entries.swap(device_cache[device]);
+    device_cache_total[device] = 0;
+  }
+  for (auto& kv : entries) cudaFreeAsync(kv.second, stream);
+}
+
+// Frees every cached buffer of `device` and returns the pool's unused memory
+// to the device.
+int device_cache_release(int device) {
+  std::multimap<size_t, void*> entries;
+  {
+    std::lock_guard<std::mutex> lock(device_cache_mutex);
+    entries.swap(device_cache[device]);
+    device_cache_total[device] = 0;
+  }
+  int previous = 0;
+  cudaError_t e = cudaGetDevice(&previous);
+  if (e == cudaSuccess) e = cudaSetDevice(device);
+  for (auto& kv : entries)
+    if (e == cudaSuccess) e = cudaFreeAsync(kv.second, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaMemPool_t pool;
+  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, device);
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+  cudaSetDevice(previous);
+  return cuda_status(e);
 }
 
 namespace {
@@ -486,6 +643,7 @@ uint64_t pool_idle_bytes(int device) {
 // Plain planner.
 
 int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
+  TraceRange range("mgbfs2.plan");
   mgbfs2_plan_request r{};
   if (req) r = *req;
   if (r.visited > MGBFS2_VISITED_HASH3 || r.dedup > MGBFS2_DEDUP_GROUPED || r.planner > MGBFS2_PLANNER_LEARNED)
@@ -493,7 +651,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   MG_CHECK(cudaSetDevice(device));
   size_t free_bytes = 0, total_bytes = 0;
   MG_CHECK(cudaMemGetInfo(&free_bytes, &total_bytes));
-  free_bytes += pool_idle_bytes(device);
+  free_bytes += pool_idle_bytes(device) + device_cache_bytes(device);
   const uint64_t reserve = r.reserve_bytes ? r.reserve_bytes : (2ull << 30);
   if (free_bytes <= reserve) return MGBFS2_OUT_OF_MEMORY;
   const uint64_t budget = free_bytes - reserve;
@@ -504,6 +662,22 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   p.state_bound = state_bound;
   p.inverse_closed = inverse_closed;
   p.planner = r.planner;
+  // The learned planner replaces the worst-case bound by its prediction
+  // where the bound only sizes or chooses; exactness never depends on it.
+  const bool learned = r.planner == MGBFS2_PLANNER_LEARNED;
+  if (learned && !r.predicted_states) return MGBFS2_INVALID_ARGUMENT;
+  const uint64_t expected = learned ? (state_bound ? std::min(state_bound, r.predicted_states) : r.predicted_states)
+                                    : state_bound;
+  learned_peak = learned ? r.predicted_peak : 0;
+  // Routed and grouped layers rank over the whole Lehmer domain; asked for
+  // explicitly, they keep it even where the product domain is smaller.
+  use_product = product && r.dedup != MGBFS2_DEDUP_BUCKET && r.dedup != MGBFS2_DEDUP_GROUPED;
+  if (r.group_chunk && (r.group_chunk < 256 || r.group_chunk > (1u << 20))) return MGBFS2_INVALID_ARGUMENT;
+  if (r.blocks_per_sm > 32) return MGBFS2_INVALID_ARGUMENT;
+  group_chunk = r.group_chunk ? r.group_chunk : kGroupChunk;
+  blocks_per_sm = static_cast<int>(r.blocks_per_sm);
+  p.group_chunk = group_chunk;
+  p.blocks_per_sm = r.blocks_per_sm;
   p.shards = r.shards ? r.shards : 64;
   p.block = kBlock;
   uint32_t visited = r.visited;
@@ -511,11 +685,11 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     if (visited == MGBFS2_VISITED_BITMAP) return MGBFS2_UNSUPPORTED;
     if (visited == MGBFS2_VISITED_AUTO) visited = inverse_closed ? MGBFS2_VISITED_HASH3 : MGBFS2_VISITED_HASH;
   }
-  const uint64_t bitmap_bytes = rank_ok ? ((rank_total + 63) / 64) * 8 : UINT64_MAX;
+  const uint64_t bitmap_bytes = rank_ok ? ((rank_domain() + 63) / 64) * 8 : UINT64_MAX;
   if (visited == MGBFS2_VISITED_AUTO) {
     // The bitmap costs total/8 bytes, an exact hash ~16 B per state: take the
     // bitmap when it is the smaller exact structure and fits comfortably.
-    const bool dense = state_bound && rank_total / 128 <= state_bound;
+    const bool dense = expected && rank_domain() / 128 <= expected;
     if (rank_ok && bitmap_bytes <= budget / 2 && (dense || bitmap_bytes <= (64ull << 20)))
       visited = MGBFS2_VISITED_BITMAP;
     else
@@ -532,7 +706,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     // generator), else owner-routed layers, whose shard slices fit in L2
     // whatever the generators.
     dedup = MGBFS2_DEDUP_ATOMIC;
-    if (visited == MGBFS2_VISITED_BITMAP && lehmer && bitmap_bytes > (64ull << 20) && elements <= 16) {
+    if (visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product && bitmap_bytes > (64ull << 20) && elements <= 16) {
       const uint32_t n = elements, K = n > 10 ? std::min<uint32_t>(3, n - 10) : 1;
       bool local = n <= 13;
       for (uint32_t k = 0; k < gens && local; ++k) {
@@ -546,8 +720,8 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
   const bool hash_routed = dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_HASH && packed;
-  if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) && !(visited == MGBFS2_VISITED_BITMAP && lehmer) &&
-      !hash_routed)
+  if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) &&
+      !(visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product) && !hash_routed)
     return MGBFS2_UNSUPPORTED;
   // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
   if (dedup == MGBFS2_DEDUP_SORT && (!packed || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
@@ -595,7 +769,8 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   p.parent_skip = parent_skip;
   p.bucket_prefix = bucket_prefix;
   p.history_layers = visited == MGBFS2_VISITED_HASH3 ? 3 : 1;
-  p.bitmap_bits = visited == MGBFS2_VISITED_BITMAP ? rank_total : 0;
+  p.bitmap_bits = visited == MGBFS2_VISITED_BITMAP ? rank_domain() : 0;
+  p.rank_components = visited == MGBFS2_VISITED_BITMAP ? (use_product ? product_domain.components : 1) : 0;
   // Frontier capacity: the orbit bound (or the caller's cap) within memory.
   uint64_t fixed = visited == MGBFS2_VISITED_BITMAP ? bitmap_bytes : 0;
   if (fixed >= budget) return MGBFS2_OUT_OF_MEMORY;
@@ -607,9 +782,30 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   cap = std::min(cap, (budget - fixed) / (per_state + hash_per_state));
   if (cap == 0) return MGBFS2_OUT_OF_MEMORY;
   p.capacity = cap;
+  hash_quotient = false;
   if (visited == MGBFS2_VISITED_HASH) {
-    const uint64_t want = state_bound ? state_bound : cap;
-    p.table_slots = std::max<uint64_t>(1024, next_pow2(2 * std::min(want, cap)));
+    // All-visited table: sized for the state bound (or the frontier cap) at
+    // the growth threshold.  Fused layers of one-word keys take 32-bit
+    // quotient slots when the key bits beyond the slot index leave at least
+    // 8 bits for the probe distance.
+    // The learned plan sizes it for the prediction plus a quarter.
+    const uint64_t predicted = learned ? expected + expected / 4 + 1024 : 0;
+    const uint64_t want = std::min(learned ? predicted : (state_bound ? state_bound : cap), cap);
+    const uint32_t key_bits = key_mask == ~0ull ? 64u : 64u - static_cast<uint32_t>(__builtin_clzll(key_mask));
+    const bool quotient_ok = packed && !hash_routed && (dedup == MGBFS2_DEDUP_ATOMIC) &&
+                             !(r.options & MGBFS2_OPTION_WIDE_SLOTS);
+    // Longer linear-probe chains, not table bytes, cost the most: a half-full
+    // threshold (S11: 2^27 slots, load 0.3) measured 1.6x faster than 3/4.
+    const uint32_t load = r.hash_load_percent ? std::min<uint32_t>(95, std::max<uint32_t>(10, r.hash_load_percent))
+                                              : 50u;
+    const uint64_t slots = std::max<uint64_t>(1024, next_pow2((want * 100 + load - 1) / load));
+    uint32_t s_bits = 0;
+    while ((1ull << s_bits) < slots) ++s_bits;
+    hash_quotient = quotient_ok && key_bits <= s_bits + 24;
+    hash_load = load;
+    p.table_slots = slots;
+    p.table_slot_bytes = hash_quotient ? 4 : 8;
+    p.hash_load_percent = load;
   }
   if (hash_routed) {
     // Hash-routed layers: shard = table region of a key's home slot, regions
@@ -622,7 +818,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
     bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
   }
-  p.device_bytes = fixed + (visited == MGBFS2_VISITED_HASH ? p.table_slots * 8 : 0);
+  p.device_bytes = fixed + (visited == MGBFS2_VISITED_HASH ? p.table_slots * p.table_slot_bytes : 0);
   if (!packed) {
     int rc = wide_plan(&p, budget);
     if (rc) return rc;
@@ -680,6 +876,8 @@ static ExpandFn pick_sorted(int visit, uint32_t n) {
       }
     case V_MULTISET:
       return expand_sorted<V_MULTISET, 0>;
+    case V_PRODUCT:
+      return expand_sorted<V_PRODUCT, 0>;
     case V_HASH:
       return expand_sorted<V_HASH, 0>;
     default:
@@ -693,8 +891,12 @@ static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
       return warp ? pick_lehmer<V_LEHMER, true>(n) : pick_lehmer<V_LEHMER, false>(n);
     case V_MULTISET:
       return warp ? expand_packed<V_MULTISET, 0, true> : expand_packed<V_MULTISET, 0, false>;
+    case V_PRODUCT:
+      return warp ? expand_packed<V_PRODUCT, 0, true> : expand_packed<V_PRODUCT, 0, false>;
     case V_HASH:
       return expand_packed<V_HASH, 0, false>;
+    case V_HASHQ:
+      return expand_packed<V_HASHQ, 0, false>;
     default:
       return expand_packed<V_HASH3, 0, false>;
   }
@@ -894,7 +1096,7 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   uint64_t run = 0;
   for (uint32_t j = 0; j < R; ++j) {
     ip[j] = run;
-    run += (rcnt[order[j]] + kGroupChunk - 1) / kGroupChunk;
+    run += (rcnt[order[j]] + group_chunk - 1) / group_chunk;
   }
   ip[R] = run;
   *items = run;
@@ -926,7 +1128,7 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
                                 static_cast<int>(*smem_total)));
   // Eight blocks per SM (the 164 KB configuration, 92 KB left as L1) for the
   // plain kernel; the transposition kernel's registers allow five.
-  const int blocks = set_carveout(reinterpret_cast<const void*>(f), *smem_total, kGroupBlocksPerSM);
+  const int blocks = set_carveout(reinterpret_cast<const void*>(f), *smem_total, want_blocks(kGroupBlocksPerSM));
   *grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(blocks) * sm_count, *items)));
   return MGBFS2_OK;
 }
@@ -1071,8 +1273,26 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
 }
 
 int Graph::visit_kind() const {
-  if (plan.visited == MGBFS2_VISITED_BITMAP) return (lehmer && elements >= 2) ? V_LEHMER : V_MULTISET;
-  return plan.visited == MGBFS2_VISITED_HASH ? V_HASH : V_HASH3;
+  if (plan.visited == MGBFS2_VISITED_BITMAP) {
+    if (use_product) return V_PRODUCT;
+    return (lehmer && elements >= 2) ? V_LEHMER : V_MULTISET;
+  }
+  if (plan.visited == MGBFS2_VISITED_HASH) return hash_quotient ? V_HASHQ : V_HASH;
+  return V_HASH3;
+}
+
+QuotientSlots Graph::quotient_slots(uint64_t slots) const {
+  QuotientSlots q{};
+  q.slots = static_cast<unsigned int*>(table.ptr);
+  q.mask = slots - 1;
+  q.s = 0;
+  while ((1ull << q.s) < slots) ++q.s;
+  q.bits = key_mask == ~0ull ? 64u : 64u - static_cast<uint32_t>(__builtin_clzll(key_mask));
+  const uint32_t rem = q.bits > q.s ? q.bits - q.s : 0u;
+  q.d = 32 - rem;
+  const uint64_t most = (q.d >= 32 ? (1ull << 32) : (1ull << q.d)) - 2;  // distance field holds j + 1 < 2^D
+  q.limit = static_cast<uint32_t>(std::min<uint64_t>(most, 1u << 20));
+  return q;
 }
 
 int size_carveout(const void* fn, size_t smem, int want, int threads) {
@@ -1168,10 +1388,23 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
   LoopState* ls = reinterpret_cast<LoopState*>(base);
   unsigned long long* layers = reinterpret_cast<unsigned long long*>(base + head);
   unsigned long long* stamps = layers + kEntries;
+  // The loop starts from the caller's state: the start (depth 0), or a
+  // resumed checkpoint's deepest layer.
+  const uint64_t count0 = *count, visited0 = *visited;
+  const uint32_t depth0 = *depth;
+  if (depth0 + 2 >= kEntries) {
+    *paused = true;  // too deep for the device loop's layer table: the host loop goes on
+    return MGBFS2_OK;
+  }
   LoopState h{};
-  h.count = 1;
-  h.visited = 1;
+  h.count = count0;
+  h.visited = visited0;
+  h.depth = depth0;
   h.capacity = cap;
+  h.gens = gens;
+  const int visit = visit_kind();
+  if ((visit == V_HASH || visit == V_HASHQ) && !(state_bound && table_slots * hash_load / 100 >= state_bound))
+    h.table_limit = table_slots * hash_load / 100;
   h.buf[0] = static_cast<unsigned long long*>(front.ptr);
   h.buf[1] = static_cast<unsigned long long*>(next.ptr);
   h.max_entries = kEntries;
@@ -1211,7 +1444,7 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
       void* args[] = {&q};
       e = cudaEventRecord(ev_kernel[0], stream);
       if (e == cudaSuccess) {
-        loop_start<<<1, 1, 0, stream>>>(stamps);
+        loop_start<<<1, 1, 0, stream>>>(stamps + depth0);
         e = cudaGetLastError();
       }
       if (e == cudaSuccess) {
@@ -1248,7 +1481,7 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
   if (!persistent_done && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
   if (!persistent_done && e == cudaSuccess) e = cudaEventRecord(ev_kernel[0], stream);
   if (!persistent_done && e == cudaSuccess) {
-    loop_start<<<1, 1, 0, stream>>>(stamps);
+    loop_start<<<1, 1, 0, stream>>>(stamps + depth0);
     e = cudaGetLastError();
   }
   if (!persistent_done && e == cudaSuccess) e = cudaGraphLaunch(exec, stream);
@@ -1267,19 +1500,20 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
   // Layers 1..out.depth were recorded; layers 0..out.depth were expanded
   // unless the table filled up (then layer out.depth is still to expand).
   const uint32_t D = out.depth;
-  const uint32_t expanded = out.stop == 3 ? D : D + 1;
-  for (uint32_t d = 1; d <= D; ++d) {
+  const uint32_t expanded = out.stop == 3 ? D : D + 1;  // layers depth0 .. expanded - 1 were expanded
+  auto size_at = [&](uint32_t d) { return d == depth0 ? count0 : sizes[d]; };
+  for (uint32_t d = depth0 + 1; d <= D; ++d) {
     layer_sizes.push_back(sizes[d]);
     layer_seconds.push_back(static_cast<double>(times[d] - times[d - 1]) * 1e-9);
   }
-  for (uint32_t d = 0; d < expanded; ++d) {
-    const uint64_t c = d ? sizes[d] : 1;
+  for (uint32_t d = depth0; d < expanded; ++d) {
+    const uint64_t c = size_at(d);
     st->successors += c * gens;
     st->visited_tests += c * gens - (parent_skip && d > 0 ? c : 0);
   }
-  launches += persistent_done ? 2 : 1 + 2 * expanded;
+  launches += persistent_done ? 2 : 1 + 2 * (expanded - depth0);
   if (out.parity) std::swap(front, next);
-  *count = D ? sizes[D] : 1;
+  *count = size_at(D);
   *visited = out.visited;
   *depth = D;
   *paused = out.stop == 3;
@@ -1291,13 +1525,13 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
   if (out.stop == 1) st->complete = 1;
   // The deepest layer sits in `front`; the layer before it is intact in `next`
   // (the last expansion appended nothing, or the loop paused before it).
-  if (D >= 2 && sizes[D - 1] < 1000) {
+  if (D >= depth0 + 2 && D >= 2 && sizes[D - 1] < 1000) {
     std::vector<uint64_t> words(sizes[D - 1]);
     MG_CHECK(cudaMemcpyAsync(words.data(), next.ptr, words.size() * 8, cudaMemcpyDeviceToHost, stream));
     MG_CHECK(cudaStreamSynchronize(stream));
     keep_small(D - 1, std::move(words));
   }
-  if (D >= 1 && sizes[D] < 1000) {
+  if (D >= depth0 + 1 && D >= 1 && sizes[D] < 1000) {
     std::vector<uint64_t> words(sizes[D]);
     MG_CHECK(cudaMemcpyAsync(words.data(), front.ptr, words.size() * 8, cudaMemcpyDeviceToHost, stream));
     MG_CHECK(cudaStreamSynchronize(stream));
@@ -1308,14 +1542,24 @@ int Graph::run_device_loop(const void* fn, ExpandParams* pp, size_t smem, uint64
 
 int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* user, mgbfs2_status* status) {
   if (!planned) return MGBFS2_STATE;
+  TraceRange range("mgbfs2.run");
   MG_CHECK(cudaSetDevice(device));
   if (!packed) return wide_run(limits, cb, user, status);
   mgbfs2_status st{};
-  layer_sizes.assign(1, 1);
-  layer_seconds.clear();
-  for (int i = 0; i < 2; ++i) {
-    small_layer[i].clear();
-    small_depth[i] = UINT32_MAX;
+  // A resumed run starts from the checkpoint's layer table, deepest layer
+  // (in `front`), visited structure and small-layer samples.
+  const bool resume = resume_pending;
+  resume_pending = false;
+  if (resume) {
+    layer_sizes = resume_layers;
+    layer_seconds.assign(layer_sizes.size() - 1, 0.0);
+  } else {
+    layer_sizes.assign(1, 1);
+    layer_seconds.clear();
+    for (int i = 0; i < 2; ++i) {
+      small_layer[i].clear();
+      small_depth[i] = UINT32_MAX;
+    }
   }
   launches = 0;
   const auto started = Clock::now();
@@ -1353,7 +1597,10 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   p.key_mask = key_mask;
   p.ppt = gens <= 4 ? 4 : 2;
   const size_t smem = terms.size() * sizeof(Term) + term_begin.size() * sizeof(uint32_t);
-  if (!sorted) set_carveout(reinterpret_cast<const void*>(fn), smem, kPackedBlocksPerSM);
+  if (!sorted)
+    set_carveout(reinterpret_cast<const void*>(fn), smem,
+                 want_blocks(visit == V_HASHQ ? kHashQBlocksPerSM : kPackedBlocksPerSM));
+  if (visit == V_PRODUCT) p.pd = product_domain;
   if (visit == V_MULTISET) {
     p.ms.n = elements;
     p.ms.bits = bits;
@@ -1364,15 +1611,27 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   int rc = MGBFS2_OK;
   double kernel_seconds = 0.0;
   MG_CHECK(cudaEventRecord(ev_run[0], stream));
-  // Initial state: visited structure cleared, start seeded, frontier = {start}.
+  // Initial state: visited structure cleared, start seeded, frontier = {start}
+  // (a resumed run keeps what the checkpoint restored).
   MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
-  if (visit == V_LEHMER || visit == V_MULTISET) {
-    MG_CHECK(cudaMemsetAsync(bitmap.ptr, 0, bitmap.bytes, stream));
+  if (visit == V_LEHMER || visit == V_MULTISET || visit == V_PRODUCT) {
+    if (!resume) MG_CHECK(cudaMemsetAsync(bitmap.ptr, 0, bitmap.bytes, stream));
     p.bitmap = static_cast<unsigned long long*>(bitmap.ptr);
   } else if (visit == V_HASH) {
-    table_slots = plan.table_slots;
-    if ((rc = table.ensure(table_slots * 8))) return rc;
-    MG_CHECK(cudaMemsetAsync(table.ptr, 0xff, table_slots * 8, stream));
+    if (!resume) {
+      table_slots = plan.table_slots;
+      if ((rc = table.ensure(table_slots * 8))) return rc;
+      MG_CHECK(cudaMemsetAsync(table.ptr, 0xff, table_slots * 8, stream));
+    }
+  } else if (visit == V_HASHQ) {
+    if (!resume) {
+      table_slots = plan.table_slots;
+      if ((rc = table.ensure(table_slots * 4))) return rc;
+      MG_CHECK(cudaMemsetAsync(table.ptr, 0, table_slots * 4, stream));
+    }
+    p.q = quotient_slots(table_slots);
+  } else if (resume) {
+    return MGBFS2_UNSUPPORTED;  // three-bank histories are not checkpointed
   } else {
     for (int b = 0; b < 3; ++b) bank_slots[b] = 0;
     bank_slots[0] = 1024;
@@ -1384,17 +1643,42 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   // no limits and no callback.
   const bool limited = limits && (limits->max_seconds > 0 || limits->max_layers || limits->cancel);
   const uint64_t loop_cap = std::max<uint64_t>(1, plan.capacity);
-  bool device_loop = !host_loop_only && !bucketed && !grouped_mode && !sorted && !limited && !cb &&
-                     (visit == V_LEHMER || visit == V_MULTISET || visit == V_HASH) &&
+  bool device_loop = !host_loop_only && !bucketed && !grouped_mode && !limited && !cb &&
+                     (visit == V_LEHMER || visit == V_MULTISET || visit == V_PRODUCT || visit == V_HASH ||
+                      visit == V_HASHQ) &&
                      2 * (loop_cap + 2) * 8 <= (16ull << 30);
-  if (device_loop && visit == V_HASH) device_loop = state_bound && plan.table_slots >= 2 * state_bound;
+  // The device loop never grows the table: it must hold every state below
+  // the growth threshold, or (a table sized by the learned planner) the loop
+  // pauses before the threshold could be passed and the host loop goes on.
+  if (device_loop && (visit == V_HASH || visit == V_HASHQ))
+    device_loop = plan.planner == MGBFS2_PLANNER_LEARNED ||
+                  (state_bound && table_slots * hash_load / 100 >= state_bound);
+  // A learned plan pre-sizes the host loop's frontier buffers for its
+  // predicted peak layer, so a correct prediction costs no buffer growth.
+  if (!device_loop && learned_peak) {
+    const uint64_t reserve = std::min<uint64_t>(plan.capacity, learned_peak + learned_peak / 4 + 1024);
+    if ((rc = front.ensure((reserve + 2) * 8)) || (rc = next.ensure((reserve + 2) * 8))) return rc;
+  }
   if (device_loop) {
+    // A resumed frontier is already in `front`: regrowing it must keep it.
+    if (resume && front.bytes < (loop_cap + 2) * 8) {
+      DeviceBuffer grown;
+      grown.stream = stream;
+      if ((rc = grown.ensure((loop_cap + 2) * 8))) return rc;
+      MG_CHECK(cudaMemcpyAsync(grown.ptr, front.ptr, last_count * 8, cudaMemcpyDeviceToDevice, stream));
+      front.free();
+      front = grown;
+      grown.ptr = nullptr;
+      grown.bytes = 0;
+    }
     if ((rc = front.ensure((loop_cap + 2) * 8))) return rc;
     if ((rc = next.ensure((loop_cap + 2) * 8))) return rc;
   }
-  if ((rc = front.ensure(16))) return rc;
-  MG_CHECK(cudaMemcpyAsync(front.ptr, &start_word, 8, cudaMemcpyHostToDevice, stream));
-  {
+  if (!resume) {
+    if ((rc = front.ensure(16))) return rc;
+    MG_CHECK(cudaMemcpyAsync(front.ptr, &start_word, 8, cudaMemcpyHostToDevice, stream));
+  }
+  if (!resume) {
     ExpandParams s = p;
     if (visit == V_HASH) {
       s.table = static_cast<unsigned long long*>(table.ptr);
@@ -1410,7 +1694,12 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   }
   uint64_t count = 1, visited = 1;
   uint32_t depth = 0;
-  if (count < 1000) {
+  if (resume) {
+    count = layer_sizes.back();
+    visited = 0;
+    for (uint64_t x : layer_sizes) visited += x;
+    depth = static_cast<uint32_t>(layer_sizes.size() - 1);
+  } else {
     keep_small(0, std::vector<uint64_t>(1, start_word));
   }
   uint64_t peak = plan.device_bytes;
@@ -1424,6 +1713,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     }
     p.probe_limit = 1u << 20;
     bool paused = false;
+    TraceRange loop_range(sorted ? "layers.device_loop.sorted" : "layers.device_loop.fused");
     rc = run_device_loop(reinterpret_cast<const void*>(fn), &p, smem, loop_cap, &st, &kernel_seconds, &count,
                          &visited, &depth, &paused);
     finished = rc != MGBFS2_OK || !paused;
@@ -1482,6 +1772,30 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       p.table = static_cast<unsigned long long*>(table.ptr);
       p.table_mask = table_slots - 1;
       p.tag = 0;
+    } else if (visit == V_HASHQ) {
+      // Grow (rehash) so the table stays below its threshold after this layer.
+      const uint64_t need = visited + bound;
+      if (need * 100 > table_slots * hash_load) {
+        const uint64_t slots = next_pow2((need * 100 + hash_load - 1) / hash_load);
+        DeviceBuffer grown;
+        grown.stream = stream;
+        if ((rc = grown.ensure(slots * 4))) break;
+        MG_CHECK(cudaMemsetAsync(grown.ptr, 0, slots * 4, stream));
+        const QuotientSlots from = quotient_slots(table_slots);
+        QuotientSlots to = quotient_slots(slots);
+        to.slots = static_cast<unsigned int*>(grown.ptr);
+        rehash_qtable<<<grid_for(reinterpret_cast<const void*>(rehash_qtable), 0, (table_slots + kBlock - 1) / kBlock),
+                        kBlock, 0, stream>>>(from, to, &p.control->error);
+        ++launches;
+        MG_CHECK(cudaGetLastError());
+        MG_CHECK(cudaStreamSynchronize(stream));
+        table.free();
+        table = grown;
+        grown.ptr = nullptr;
+        grown.bytes = 0;
+        table_slots = slots;
+      }
+      p.q = quotient_slots(table_slots);
     } else if (visit == V_HASH3) {
       const int ins = (depth + 1) % 3, cur = depth % 3, prev = (depth + 2) % 3;
       const uint64_t slots = std::max<uint64_t>(1024, next_pow2(2 * std::max<uint64_t>(bound, 1)));
@@ -1497,6 +1811,8 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     }
     const uint64_t work = count * gens;
     const bool routed = bucketed && work >= bucket_min_work;
+    TraceRange layer_range(routed ? "layer.bucket" : group_layer ? "layer.grouped" : sorted ? "layer.sorted"
+                                                                                         : "layer.fused");
     // One attempt; a routed layer whose shard buckets overflowed left the
     // bitmap untouched and is redone once with the exact shard counts.
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -1530,6 +1846,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         gp.next_cap = meta + 4 * R + 1;
         gp.next_count = meta + 5 * R + 1;
         gp.work = meta + 6 * R + 1;
+        gp.chunk = group_chunk;
         gp.control = p.control;
         gp.transp = static_cast<const uint32_t*>(transp_buf.ptr);
         reinterpret_cast<GroupedFn>(group_fn)<<<group_grid, kBlock, group_smem,
@@ -1674,10 +1991,6 @@ int Graph::sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* rows) {
 
 using mgbfs2::Graph;
 
-struct mgbfs2_graph {
-  Graph* impl;
-};
-
 extern "C" {
 
 int mgbfs2_graph_create(const mgbfs2_graph_desc* desc, int device, mgbfs2_graph** out, char* error,
@@ -1740,5 +2053,11 @@ void mgbfs2_destroy(mgbfs2_graph* graph) {
   delete graph->impl;
   delete graph;
 }
+
+int mgbfs2_trim_memory(int device) { return mgbfs2::device_cache_release(device); }
+
+void mgbfs2_trace_range_push(const char* label) { nvtxRangePushA(label ? label : "mgbfs2"); }
+
+void mgbfs2_trace_range_pop(void) { nvtxRangePop(); }
 
 }  // extern "C"

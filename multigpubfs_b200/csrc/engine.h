@@ -6,6 +6,8 @@
 #include <map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/mgbfs2.h"
 #include "device.cuh"
 
@@ -27,7 +29,22 @@ struct DeviceBuffer {
   cudaStream_t stream = nullptr;
   int ensure(size_t want, bool exact = false);  // exact: no geometric headroom
   void free();
+  // Hands the buffer to the process-wide device cache instead of the pool.
+  // Only when no work in flight on any stream uses it (its owner synchronised).
+  void release_to_cache(int device);
 };
+
+// Process-wide cache of device buffers given back by destroyed graph handles,
+// per device: a new handle's buffers are taken from it (smallest that fits)
+// before the stream-ordered pool is asked.  Creating and destroying a handle
+// per search then costs no pool allocation at all; allocating multi-GB
+// blocks from a pool whose free memory is split over blocks of other sizes
+// took 6-12 ms per allocation on a B200.
+bool device_cache_take(int device, size_t want, void** ptr, size_t* bytes);
+void device_cache_give(int device, void* ptr, size_t bytes);
+uint64_t device_cache_bytes(int device);
+void device_cache_drain(int device, cudaStream_t stream);
+int device_cache_release(int device);
 
 int retain_pool_memory(int device);
 // Pinned host buffers from a process-wide cache: creating and freeing page-
@@ -39,6 +56,22 @@ uint64_t pool_idle_bytes(int device);
 
 struct WideState;     // int64-key arena path (wide.cu)
 struct ExpandParams;  // packed_kernels.cuh
+
+// A named NVTX range for the lifetime of the object: a profiler's timeline
+// shows the library's phases (plan, run, each layer by kernel family, batch
+// waves, planner training) around the kernels.  NVTX v3 is header-only and
+// costs a pointer check when no tool is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+
+// The bitmap's product domain over the generators' position components of
+// packed codes (engine.cu); false when it cannot be represented.
+bool build_product_domain(uint32_t n, uint32_t bits, uint32_t distinct, const uint32_t* codes, uint32_t gens,
+                          const uint32_t* perms, ProductDomain* out);
 
 struct Graph {
   // Description.
@@ -58,6 +91,13 @@ struct Graph {
   std::vector<uint32_t> code_counts;
   uint64_t start_word = 0, key_mask = ~0ull;
   uint64_t rank_total = 0, state_bound = 0;
+  // Position components of the generators: when they split the positions
+  // and their product of multiset domains is smaller than the whole multiset
+  // domain, the bitmap ranks over the product (ProductDomain).
+  bool product = false;
+  ProductDomain product_domain{};
+  bool use_product = false;  // plan: rank over the product (not with the Lehmer-only routed / grouped layers)
+  uint64_t rank_domain() const { return use_product ? product_domain.total : rank_total; }
   std::vector<uint64_t> coxeter;   // certified layer sizes, empty if not Coxeter
   std::vector<Term> terms;
   std::vector<uint32_t> term_begin;  // gens + 1 term offsets, then inverse[gens]
@@ -72,6 +112,14 @@ struct Graph {
   int sm_count = 148;
   DeviceBuffer bitmap, front, next, table, bank[3], program, control_buf, scratch;
   uint64_t table_slots = 0, bank_slots[3] = {0, 0, 0};
+  // All-visited hash in 32-bit quotient slots (device.cuh QuotientSlots).
+  bool hash_quotient = false;
+  uint32_t hash_load = 50;  // growth threshold, percent
+  uint64_t learned_peak = 0;  // learned plan: predicted largest layer (pre-sizes the frontier buffers)
+  uint32_t group_chunk = 4096;  // plan shape: parents per grouped work item
+  int blocks_per_sm = 0;        // plan shape: resident layer-kernel blocks per SM, 0 = defaults
+  int want_blocks(int kernel_default) const { return blocks_per_sm ? blocks_per_sm : kernel_default; }
+  QuotientSlots quotient_slots(uint64_t slots) const;
   Control* host_control = nullptr;
   WideState* wide = nullptr;
 
@@ -116,6 +164,15 @@ struct Graph {
   int run_device_loop(const void* fn, ExpandParams* p, size_t smem, uint64_t cap, mgbfs2_status* st,
                       double* kernel_seconds, uint64_t* count, uint64_t* visited, uint32_t* depth, bool* paused);
 
+  // Checkpoint / resume (checkpoint.cu): read_checkpoint restores the visited
+  // structure, the deepest layer (in `front`) and the layer table, and the
+  // next run() goes on from there.
+  bool resume_pending = false;
+  std::vector<uint64_t> resume_layers;
+  int write_checkpoint(const char* path);
+  int read_checkpoint(const char* path);
+  int frontier_words(uint64_t* out, size_t capacity, size_t* count);
+
   // Results.
   std::vector<uint64_t> layer_sizes;
   std::vector<double> layer_seconds;
@@ -148,3 +205,8 @@ struct Graph {
 };
 
 }  // namespace mgbfs2
+
+// The C-ABI handle (mgbfs2.h) around a Graph.
+struct mgbfs2_graph {
+  mgbfs2::Graph* impl;
+};

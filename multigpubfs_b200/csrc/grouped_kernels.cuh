@@ -38,7 +38,7 @@ namespace mgbfs2 {
 constexpr uint32_t kGroupStage = 1024;  // staged winners per block (one pass of 256 x 4 parents)
 constexpr int kGroupBlocksPerSM = 8;    // resident blocks the shared-memory carveout is sized for
 constexpr uint32_t kMaxGroups = 1728;   // region tables: 13!/10! = 1716 groups at most
-constexpr uint32_t kGroupChunk = 4096;  // parents per work item
+constexpr uint32_t kGroupChunk = 4096;  // parents per work item unless the plan chooses another size
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
 static_assert(kGroupStage >= kBlock * 4, "a pass stages up to kBlock * ppt winners, ppt <= 4");
 
@@ -61,6 +61,7 @@ struct GroupedParams {
   const unsigned long long* next_cap;    // regions (spill last)
   unsigned long long* next_count;        // regions: winners reserved per region (may pass a group's cap)
   unsigned long long* work;              // work-item counter, zero at launch
+  uint32_t chunk;                        // parents per work item
   Control* control;
   // Incremental-rank path (every generator swaps positions t-1 and t): per
   // generator t and the weights of digits t-1 and t in the group part and in
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
   for (;;) {
     if (tid == 0) {
       // Claim a work item and locate it: a binary search over the region
-      // prefix (in visiting order), once per 4096 parents.
+      // prefix (in visiting order), once per work item.
       const unsigned long long item = atomicAdd(p.work, 1ull);
       sm.item = item;
       if (item < items) {
@@ -200,10 +201,10 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
           if (__ldg(&p.item_prefix[mid]) <= item) lo = mid;
           else hi = mid;
         }
-        const unsigned long long first = (item - __ldg(&p.item_prefix[lo])) * kGroupChunk;
+        const unsigned long long first = (item - __ldg(&p.item_prefix[lo])) * p.chunk;
         const uint32_t region = __ldg(&p.region_order[lo]);
         const unsigned long long avail = __ldg(&p.region_count[region]) - first;
-        sm.n = static_cast<uint32_t>(avail < kGroupChunk ? avail : kGroupChunk);
+        sm.n = static_cast<uint32_t>(avail < p.chunk ? avail : p.chunk);
         sm.src = __ldg(&p.region_begin[region]) + first;
       }
     }

@@ -166,6 +166,7 @@ int prepare_layer_program(uint32_t degree, uint32_t generators, const uint32_t* 
 int enqueue_layer(const LayerProgram& prog, uint32_t degree, uint32_t generators, const uint64_t* frontier,
                   uint64_t count, uint64_t* bitmap, uint64_t* next, uint64_t next_capacity, uint64_t* next_count,
                   uint32_t* error, unsigned char* scratch, const LayerLayout& l, int device, cudaStream_t stream) {
+  TraceRange range("layer_api.expand");
   Control* control = reinterpret_cast<Control*>(scratch + l.control);
   unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
   Term* program = reinterpret_cast<Term*>(scratch + l.program);

@@ -273,6 +273,7 @@ int mgbfs2_mlp_loss_grad(uint32_t inputs, const float* params, const float* x, c
                          float weight1, uint64_t batch, float* grad, float* loss, void* stream) {
   if (!inputs || inputs > kMaxIn || !params || !grad || (batch && (!x || !target))) return MGBFS2_INVALID_ARGUMENT;
   if (!batch) return MGBFS2_OK;
+  mgbfs2::TraceRange range("planner.loss_grad");
   const size_t smem = 2 * offsets(inputs).total * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(mlp_loss_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -311,6 +312,7 @@ int mgbfs2_mlp_infer_bf16(uint32_t inputs, const void* params_bf16, const float*
 int mgbfs2_mlp_rollout_bf16(const void* params_bf16, const float* x_mean, const float* x_scale, const float* statics,
                             const float* gens, uint32_t count, uint32_t max_depth, double* peak, double* total,
                             uint32_t* depth, void* stream) {
+  mgbfs2::TraceRange range("planner.rollout");
   if (!params_bf16 || !x_mean || !x_scale || (count && (!statics || !gens || !peak || !total || !depth)))
     return MGBFS2_INVALID_ARGUMENT;
   if (!count) return MGBFS2_OK;

@@ -13,9 +13,12 @@
 
 namespace mgbfs2 {
 
-enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3 };
 
 constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
+// The quotient-hash kernel stages half as many (16 KiB), so six blocks fit per
+// SM for more loads in flight on the random table reads.
+constexpr uint32_t kOutCapHashQ = 2048;
+constexpr int kHashQBlocksPerSM = 6;
 constexpr uint32_t kBlock = 256;
 constexpr int kPackedBlocksPerSM = 4;  // resident expand_packed blocks: the 164 KB configuration, 92 KB left as L1
 
@@ -30,6 +33,11 @@ struct LoopState {
   unsigned long long* layers;  // max_entries layer sizes
   unsigned long long* stamps;  // max_entries globaltimer readings (stamp d = end of layer d)
   uint32_t bar_count, bar_gen; // grid barrier of the persistent form (zero at launch)
+  // All-visited hash sized below the state bound (learned plan): the loop
+  // pauses (stop 3) before a layer that could take the table past this many
+  // states, and the host loop grows it.  0 = the table holds every state.
+  unsigned long long table_limit;
+  uint32_t gens, pad;
 };
 
 struct ExpandParams {
@@ -57,6 +65,8 @@ struct ExpandParams {
   const unsigned long long* look1;
   unsigned long long look1_mask;
   LoopState* loop;  // graph mode: count and buffers from here instead of frontier/count/next
+  QuotientSlots q;  // V_HASHQ table
+  ProductDomain pd;  // V_PRODUCT rank domain
 };
 
 // Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the
@@ -64,12 +74,15 @@ struct ExpandParams {
 // without a candidate.
 template <int V, int N, bool WARP>
 __device__ __forceinline__ bool claim(const ExpandParams& p, uint64_t c, bool valid) {
-  if constexpr (V == V_LEHMER || V == V_MULTISET) {
+  if constexpr (V == V_LEHMER || V == V_MULTISET || V == V_PRODUCT) {
     uint64_t r = 0;
     bool ok = valid;
     if (valid) {
       if constexpr (V == V_LEHMER) {
         r = lehmer_rank4<N>(c);
+      } else if constexpr (V == V_PRODUCT) {
+        ok = product_rank(c, p.pd, &r);
+        if (!ok) raise_error(&p.control->error, ERR_RANK_RANGE);
       } else {
         ok = multiset_rank(c, p.ms, &r);
         if (!ok) raise_error(&p.control->error, ERR_RANK_RANGE);
@@ -103,6 +116,11 @@ __device__ __forceinline__ bool claim(const ExpandParams& p, uint64_t c, bool va
   } else if constexpr (V == V_HASH) {
     if (!valid) return false;
     const int rc = hash_insert(p.table, p.table_mask, c, p.key_mask, p.tag, p.probe_limit);
+    if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+    return rc == 1;
+  } else if constexpr (V == V_HASHQ) {
+    if (!valid) return false;
+    const int rc = qhash_insert(p.q, c);
     if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
     return rc == 1;
   } else {
@@ -160,15 +178,17 @@ __device__ __forceinline__ uint32_t loop_step(LoopState* s, Control* c) {
     s->depth = d;
     c->next_count = 0;
     if (d + 1 >= s->max_entries) stop = 3;
+    if (s->table_limit && s->visited + produced * s->gens > s->table_limit) stop = 3;
   }
   s->stop = stop;
   return stop;
 }
 
 template <int V, int N, bool WARP>
-__global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
+__global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) expand_packed(ExpandParams p) {
+  constexpr uint32_t out_cap = V == V_HASHQ ? kOutCapHashQ : kOutCap;
   extern __shared__ __align__(16) unsigned char program_smem[];
-  __shared__ unsigned long long out[kOutCap];
+  __shared__ unsigned long long out[out_cap];
   __shared__ uint32_t out_count;
   __shared__ unsigned long long out_base;
   Term* terms = reinterpret_cast<Term*>(program_smem);
@@ -222,26 +242,59 @@ __global__ void __launch_bounds__(kBlock) expand_packed(ExpandParams p) {
       for (uint32_t g = 0; g < p.gens; ++g) {
         const uint32_t tb = begin[g], te = begin[g + 1];
         const unsigned long long gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
+        if constexpr (V == V_HASHQ) {
+          // The home-slot reads of all this thread's children of generator g
+          // are issued before any is resolved, so up to four table misses
+          // are in flight per thread instead of one.
+          uint64_t ch[4];
+          unsigned int first[4];
+          bool live[4];
   #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if (k >= static_cast<int>(p.ppt)) break;
-          const bool v = val[k] && g != skip[k];
-          const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
-          const bool won = claim<V, N, WARP>(p, c, v);
-          const unsigned m = __ballot_sync(kFullMask, won);
-          if (m) {
-            const int leader = __ffs(m) - 1;
-            uint32_t wb = 0;
-            if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
-            wb = __shfl_sync(kFullMask, wb, leader);
-            if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
+          for (int k = 0; k < 4; ++k) {
+            live[k] = k < static_cast<int>(p.ppt) && val[k] && g != skip[k];
+            ch[k] = live[k] ? apply_terms(par[k], terms, tb, te) : 0;
+            first[k] = live[k] ? qhash_first(p.q, ch[k]) : 0u;
+          }
+  #pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (k >= static_cast<int>(p.ppt)) break;
+            bool won = false;
+            if (live[k]) {
+              const int rc = qhash_resolve(p.q, ch[k], first[k]);
+              if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+              won = rc == 1;
+            }
+            const unsigned m = __ballot_sync(kFullMask, won);
+            if (m) {
+              const int leader = __ffs(m) - 1;
+              uint32_t wb = 0;
+              if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
+              wb = __shfl_sync(kFullMask, wb, leader);
+              if (won) out[wb + __popc(m & lanemask_lt())] = ch[k] | gtag;
+            }
+          }
+        } else {
+  #pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (k >= static_cast<int>(p.ppt)) break;
+            const bool v = val[k] && g != skip[k];
+            const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
+            const bool won = claim<V, N, WARP>(p, c, v);
+            const unsigned m = __ballot_sync(kFullMask, won);
+            if (m) {
+              const int leader = __ffs(m) - 1;
+              uint32_t wb = 0;
+              if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
+              wb = __shfl_sync(kFullMask, wb, leader);
+              if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
+            }
           }
         }
         if (g + 1 < p.gens) {
           __syncthreads();
           const uint32_t pending = out_count;
           __syncthreads();
-          if (pending + tile > kOutCap) flush_block(p, next, out, &out_count, &out_base);
+          if (pending + tile > out_cap) flush_block(p, next, out, &out_count, &out_base);
         }
       }
       flush_block(p, next, out, &out_count, &out_base);
@@ -282,7 +335,19 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
   const uint32_t per_tile = kSortTile / p.gens;  // parents per tile
   const unsigned long long state_mask = p.gen_shift ? (1ull << p.gen_shift) - 1ull : p.key_mask;
   const uint32_t key_bits = state_mask == ~0ull ? 64u : 64u - __clzll(static_cast<long long>(state_mask));
-  const unsigned long long tiles = (p.count + per_tile - 1) / per_tile;
+  for (;;) {
+  // The frontier, its size and the output: from the parameters, or (device
+  // loop) from the loop state of the layer in progress.
+  unsigned long long count = p.count;
+  const unsigned long long* frontier = p.frontier;
+  unsigned long long* next = p.next;
+  if (p.loop) {
+    count = p.loop->count;
+    const uint32_t parity = p.loop->parity;
+    frontier = p.loop->buf[parity];
+    next = p.loop->buf[parity ^ 1u];
+  }
+  const unsigned long long tiles = (count + per_tile - 1) / per_tile;
   for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
     const unsigned long long base = t * per_tile;
     for (uint32_t i = threadIdx.x; i < kSortTile; i += kSortThreads) s.keys[i] = kEmpty;
@@ -290,8 +355,8 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
     // Generation: child of local parent j by generator g goes to slot g * per_tile + j.
     for (uint32_t j = threadIdx.x; j < per_tile; j += kSortThreads) {
       const unsigned long long idx = base + j;
-      if (idx >= p.count) break;
-      const uint64_t par = p.frontier[idx];
+      if (idx >= count) break;
+      const uint64_t par = frontier[idx];
       const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par >> p.gen_shift) : 0u;
       const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
       for (uint32_t g = 0; g < p.gens; ++g) {
@@ -317,11 +382,20 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
     bool overflow = false;
     for (uint32_t i = threadIdx.x; i < winners; i += kSortThreads) {
       const unsigned long long pos = out_base + i;
-      if (pos < p.capacity) p.next[pos] = s.keys[i];
+      if (pos < p.capacity) next[pos] = s.keys[i];
       else overflow = true;
     }
     if (overflow) raise_error(&p.control->error, ERR_FRONTIER_OVERFLOW);
     __syncthreads();
+  }
+  // Persistent form, as in expand_packed: block 0 records the layer between
+  // two grid barriers and every block goes on unless the loop stops.
+  if (!p.persistent) return;
+  LoopState* ls = p.loop;
+  if (!grid_barrier(&ls->bar_count, &ls->bar_gen, &p.control->error)) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) loop_step(ls, p.control);
+  if (!grid_barrier(&ls->bar_count, &ls->bar_gen, &p.control->error)) return;
+  if (*reinterpret_cast<volatile uint32_t*>(&ls->stop)) return;
   }
 }
 
@@ -347,6 +421,11 @@ static __global__ void seed_packed(ExpandParams p, unsigned long long start, int
   } else if (kind == V_MULTISET) {
     if (multiset_rank(start, p.ms, &r)) atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
     else raise_error(&p.control->error, ERR_RANK_RANGE);
+  } else if (kind == V_PRODUCT) {
+    if (product_rank(start, p.pd, &r)) atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
+    else raise_error(&p.control->error, ERR_RANK_RANGE);
+  } else if (kind == V_HASHQ) {
+    if (qhash_insert(p.q, start) < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
   } else {
     if (hash_insert(p.table, p.table_mask, start, p.key_mask, p.tag, p.probe_limit) < 0)
       raise_error(&p.control->error, ERR_TABLE_FULL);
@@ -370,6 +449,29 @@ static __global__ void rehash_table(const unsigned long long* old_table, unsigne
         break;
       }
       slot = (slot + 1) & mask;
+    }
+    if (!placed) atomicOr(error, ERR_TABLE_FULL);
+  }
+}
+
+// Re-inserts every key of a quotient table into a larger one: the mixed
+// value of the key in slot t is (stored >> D) << s | (t - distance).
+static __global__ void rehash_qtable(QuotientSlots from, QuotientSlots to, unsigned int* error) {
+  const uint64_t slots = from.mask + 1;
+  for (unsigned long long t = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; t < slots;
+       t += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const unsigned int v = from.slots[t];
+    if (v == 0u) continue;
+    const uint64_t dist = (v & ((from.d >= 32 ? 0u : (1u << from.d)) - 1u)) - 1u;
+    const uint64_t x = ((static_cast<uint64_t>(v) >> from.d) << from.s) | ((t - dist) & from.mask);
+    const uint64_t home = x & to.mask, rem = x >> to.s;
+    bool placed = false;
+    for (uint32_t j = 0; j < to.limit; ++j) {
+      const unsigned int want = static_cast<unsigned int>((rem << to.d) | (j + 1));
+      if (atomicCAS(to.slots + ((home + j) & to.mask), 0u, want) == 0u) {
+        placed = true;
+        break;
+      }
     }
     if (!placed) atomicOr(error, ERR_TABLE_FULL);
   }

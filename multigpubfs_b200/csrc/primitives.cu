@@ -98,6 +98,17 @@ __global__ void rank_kernel(MultisetDomain d, int lehmer, const unsigned long lo
   }
 }
 
+__global__ void product_rank_kernel(ProductDomain d, const unsigned long long* words, unsigned long long count,
+                                    unsigned long long* ranks, unsigned int* error) {
+  for (unsigned long long i = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    uint64_t r = 0;
+    const bool ok = product_rank(words[i], d, &r);
+    ranks[i] = ok ? r : ~0ull;
+    if (!ok && error) atomicOr(error, ERR_RANK_RANGE);
+  }
+}
+
 __global__ void bitmap_claim_kernel(const unsigned long long* ranks, unsigned long long count,
                                     unsigned long long* bitmap, unsigned long long domain, uint8_t* won, int warp,
                                     unsigned int* error) {
@@ -285,6 +296,22 @@ int mgbfs2_rank_packed(uint32_t degree, uint32_t bits, uint32_t distinct, const 
   rank_kernel<<<blocks_for(count), kPrimBlock, 0, static_cast<cudaStream_t>(stream)>>>(
       d, lehmer, reinterpret_cast<const unsigned long long*>(words), count,
       reinterpret_cast<unsigned long long*>(ranks), error);
+  return cuda_status(cudaGetLastError());
+}
+
+int mgbfs2_rank_components(uint32_t degree, uint32_t bits, uint32_t distinct, const uint32_t* codes_host,
+                           uint32_t generators, const uint32_t* permutations_host, const uint64_t* words,
+                           uint64_t count, uint64_t* ranks, uint64_t* domain_size, uint32_t* error, void* stream) {
+  if (!degree || !codes_host || !generators || !permutations_host) return MGBFS2_INVALID_ARGUMENT;
+  mgbfs2::ProductDomain d{};
+  if (!mgbfs2::build_product_domain(degree, bits, distinct, codes_host, generators, permutations_host, &d))
+    return MGBFS2_INVALID_ARGUMENT;
+  if (domain_size) *domain_size = d.total;
+  if (!count) return MGBFS2_OK;
+  if (!words || !ranks) return MGBFS2_INVALID_ARGUMENT;
+  product_rank_kernel<<<blocks_for(count), kPrimBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+      d, reinterpret_cast<const unsigned long long*>(words), count, reinterpret_cast<unsigned long long*>(ranks),
+      error);
   return cuda_status(cudaGetLastError());
 }
 

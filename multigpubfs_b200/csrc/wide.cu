@@ -404,7 +404,9 @@ int Graph::wide_sample(uint32_t which, int64_t* out, size_t cap_rows, size_t* ro
 
 void Graph::wide_release() {
   if (!wide) return;
-  for (DeviceBuffer* b : {&wide->arena, &wide->table, &wide->perms, &wide->mats, &wide->mods, &wide->counters}) b->free();
+  // Called from release(), after the stream was synchronised.
+  for (DeviceBuffer* b : {&wide->arena, &wide->table, &wide->perms, &wide->mats, &wide->mods, &wide->counters})
+    b->release_to_cache(device);
   delete wide;
   wide = nullptr;
 }

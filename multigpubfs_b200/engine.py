@@ -92,10 +92,20 @@ class NativeGraph:
 
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
              planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True, host_loop=False,
-             full_rank=False) -> dict:
+             full_rank=False, wide_slots=False, hash_load_percent=None, predicted_states=None,
+             predicted_peak=None, group_chunk=None, blocks_per_sm=None) -> dict:
+        """Plans the run (mgbfs2_plan).  planner="learned" needs
+        `predicted_states` (and optionally `predicted_peak`), e.g. from
+        planner.predict_graph."""
         req = native.PlanRequest()
+        req.predicted_states = int(predicted_states or 0)
+        req.predicted_peak = int(predicted_peak or 0)
+        req.group_chunk = int(group_chunk or 0)
+        req.blocks_per_sm = int(blocks_per_sm or 0)
         req.options = ((0 if parent_skip else native.OPTION_NO_PARENT_SKIP) |
-                       (native.OPTION_HOST_LOOP if host_loop else 0) | (native.OPTION_FULL_RANK if full_rank else 0))
+                       (native.OPTION_HOST_LOOP if host_loop else 0) | (native.OPTION_FULL_RANK if full_rank else 0) |
+                       (native.OPTION_WIDE_SLOTS if wide_slots else 0))
+        req.hash_load_percent = hash_load_percent or 0
         req.bucket_margin = 0 if bucket_margin is None else (0xFFFFFFFF if bucket_margin == 0 else bucket_margin)
         req.bucket_min_work = bucket_min_work or 0
         req.visited = native.VISITED[visited]

@@ -133,6 +133,7 @@ def run_graph(graph, output, *, device=None, devices=None, capacity=None, max_se
     digest = graph.digest()
     setup_started = time.perf_counter()
     tuned = {"enabled": autotune, "source": None}
+    shapes = {}
     if autotune and visited == "auto" and dedup == "auto" and shards is None:
         # Only a plan the caller left open is tuned, within min(60, max_seconds // 3)
         # seconds that come off the run's deadline (multigpubfs/launch.py:277-290).
@@ -146,8 +147,17 @@ def run_graph(graph, output, *, device=None, devices=None, capacity=None, max_se
         visited = prof["plan"].get("visited", visited)
         dedup = prof["plan"].get("dedup", dedup)
         shards = prof["plan"].get("shards", shards)
+        shapes = {k: prof["plan"][k] for k in ("group_chunk", "blocks_per_sm", "bucket_margin", "hash_load_percent")
+                  if k in prof["plan"]}
+    learned = {}
+    if planner == "learned":
+        # The prediction sizes and chooses; mgbfs2_plan rejects the learned
+        # planner without one.
+        from .planner import choose_path
+        learned = choose_path(graph.to_dict(), device=dev)
     with NativeGraph(graph, dev) as engine:
-        plan = engine.plan(visited=visited, dedup=dedup, capacity=capacity, shards=shards, planner=planner)
+        plan = engine.plan(visited=visited, dedup=dedup, capacity=capacity, shards=shards, **shapes,
+                           **(learned or {"planner": planner}))
         setup_seconds = time.perf_counter() - setup_started
         result = engine.run(max_seconds=max_seconds, max_layers=max_layers, cancel_flag=cancel_flag)
         current = engine.sample(0, 1000)
@@ -173,6 +183,8 @@ def run_graph(graph, output, *, device=None, devices=None, capacity=None, max_se
         "states_per_second": result.states / bfs, "kernel_launches": result.kernel_launches,
         "redo_layers": result.redo_layers, "fatal_bits": result.fatal_names,
         "memory_backend": memory_backend, "segment_strategy": segment_strategy, "autotune": tuned,
+        "planner": {"name": planner, **({k: learned[k] for k in ("predicted_states", "predicted_peak")}
+                                        if learned else {})},
     }
     output.mkdir(parents=True)
     (output / "states.json").write_bytes(state_bytes)

@@ -50,12 +50,14 @@ class PlanRequest(C.Structure):
     _fields_ = [("visited", C.c_uint32), ("dedup", C.c_uint32), ("capacity", C.c_uint64),
                 ("reserve_bytes", C.c_uint64), ("shards", C.c_uint32), ("block", C.c_uint32),
                 ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64),
-                ("options", C.c_uint32), ("reserved", C.c_uint32)]
+                ("options", C.c_uint32), ("hash_load_percent", C.c_uint32), ("predicted_states", C.c_uint64),
+                ("predicted_peak", C.c_uint64), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
 
 
 OPTION_NO_PARENT_SKIP = 1
 OPTION_HOST_LOOP = 2
 OPTION_FULL_RANK = 4
+OPTION_WIDE_SLOTS = 8
 
 
 class PlanInfo(C.Structure):
@@ -64,10 +66,12 @@ class PlanInfo(C.Structure):
                 ("capacity", C.c_uint64), ("table_slots", C.c_uint64), ("bitmap_bits", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("state_bound", C.c_uint64), ("shards", C.c_uint32),
                 ("block", C.c_uint32), ("inverse_closed", C.c_uint32), ("planner", C.c_uint32),
-                ("parent_skip", C.c_uint32), ("bucket_prefix", C.c_uint32)]
+                ("parent_skip", C.c_uint32), ("bucket_prefix", C.c_uint32), ("table_slot_bytes", C.c_uint32),
+                ("hash_load_percent", C.c_uint32), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("rank_components", C.c_uint32), ("reserved", C.c_uint32)]
 
     def to_dict(self):
-        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
         d["visited"] = VISITED_NAMES.get(self.visited, self.visited)
         d["dedup"] = DEDUP_NAMES.get(self.dedup, self.dedup)
         d["planner"] = {0: "plain", 1: "learned"}.get(self.planner, self.planner)
@@ -88,7 +92,7 @@ class RunStatus(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("max_depth", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("host_loop", C.c_uint32),
-                ("reserved", C.c_uint32), ("memory_bytes", C.c_uint64), ("reserve_bytes", C.c_uint64),
+                ("tile_entries", C.c_uint32), ("memory_bytes", C.c_uint64), ("reserve_bytes", C.c_uint64),
                 ("predicted_capacity", C.POINTER(C.c_uint64))]
 
 
@@ -96,10 +100,11 @@ class BatchStatus(C.Structure):
     _fields_ = [("instances", C.c_uint32), ("complete_instances", C.c_uint32), ("waves", C.c_uint32),
                 ("redo_instances", C.c_uint32), ("graph_launches", C.c_uint32), ("kernel_launches", C.c_uint32),
                 ("layer_steps", C.c_uint32), ("fatal", C.c_uint32), ("states", C.c_uint64),
-                ("successors", C.c_uint64), ("seconds", C.c_double), ("device_seconds", C.c_double)]
+                ("successors", C.c_uint64), ("seconds", C.c_double), ("device_seconds", C.c_double),
+                ("redo_layers", C.c_uint32), ("reserved", C.c_uint32)]
 
     def to_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
 LAYER_CALLBACK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint64, C.c_double)
@@ -113,6 +118,16 @@ _SIGNATURES = {
     "mgbfs2_sample": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int64), C.c_size_t, C.POINTER(C.c_size_t)]),
     "mgbfs2_status_string": (C.c_char_p, [C.c_int]),
     "mgbfs2_destroy": (None, [C.c_void_p]),
+    "mgbfs2_trim_memory": (C.c_int, [C.c_int]),
+    "mgbfs2_checkpoint_write": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mgbfs2_checkpoint_resume": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mgbfs2_frontier_words": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "mgbfs2_trace_range_push": (None, [C.c_char_p]),
+    "mgbfs2_trace_range_pop": (None, []),
+    "mgbfs2_rank_components": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
+                                         C.POINTER(C.c_uint32), C.c_void_p, C.c_uint64, C.c_void_p,
+                                         C.POINTER(C.c_uint64), C.c_void_p, C.c_void_p]),
+    "mgbfs2_batch_layer_tables": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "mgbfs2_successors_i64": (C.c_int, [C.c_uint32] * 5 + [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
                                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mgbfs2_successors_packed": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
@@ -239,6 +254,12 @@ def require_device():
     if not torch.cuda.is_available():
         raise NativeUnavailable("no CUDA device: the native BFS has no CPU fallback")
     return lib
+
+
+def trim_memory(device: int = 0):
+    """Give the library's cached device buffers and the pool's unused memory
+    back to the device (mgbfs2_trim_memory)."""
+    check(require_device().mgbfs2_trim_memory(device), "mgbfs2_trim_memory")
 
 
 def check(code: int, where: str):

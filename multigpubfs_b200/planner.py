@@ -12,10 +12,11 @@ Targets: log1p |L_{d+1}| - log1p |L_d| (log growth) and the duplicate ratio
 1 - |L_{d+1}| / (g |L_d|).
 
 A rollout from |L_0| = 1 gives each instance's predicted layer profile; its
-peak times a margin sizes the instance's frontier in the batched sweep (an
-instance that overflows is rerun exactly with its orbit bound), and the
-profile picks the visited-set path of a single run.  Results never depend on
-the prediction.  There is no counterpart in the reference, which sizes
+peak times a margin sizes the instance's frontier in the batched sweep (a
+layer that outgrows it is redone in a larger segment), and for a single run
+the prediction (with |G| exact where the labels are distinct) chooses the
+bitmap or the hash and sizes the table and buffers through mgbfs2_plan.
+Results never depend on the prediction.  There is no counterpart in the reference, which sizes
 buffers from worst-case bounds and timed pilot runs
 (crates/mgbfs-runtime/src/generic_memory.rs:36-49, multigpubfs/autotune.py:276).
 """
@@ -327,21 +328,63 @@ def calibrate_margin(net: PlannerNet, graphs, tables, quantile=0.97, slack=1.1) 
     return max(1.0, q) * slack
 
 
-def choose_path(net: PlannerNet, graph: dict) -> dict:
-    """Visited set and dedup mode of a single run from the predicted profile:
-    the exact bitmap when the predicted orbit fills at least 1/128 of the rank
-    domain, else the hash (three layer banks when inverse-closed); bucketed
-    layers when the predicted peak layer reaches the bucketing threshold."""
-    prof = rollout(net, [graph])[0]
-    st = graph_statics(graph["action"]["generators"], graph["start"])
-    start = graph["start"]
-    counts = {}
-    for v in start:
-        counts[v] = counts.get(v, 0) + 1
-    rank_domain = math.exp(math.lgamma(len(start) + 1) - sum(math.lgamma(c + 1) for c in counts.values()))
-    total, peak = sum(prof), max(prof)
-    if total >= rank_domain / 128:
-        return {"visited": "bitmap", "dedup": "bucket" if peak * st.gens >= (1 << 22) else "atomic",
-                "predicted_states": total, "predicted_peak": peak}
-    return {"visited": "hash3" if st.inverse_closed else "hash", "dedup": "auto",
-            "predicted_states": total, "predicted_peak": peak}
+_DEFAULT = {}
+
+
+def default_planner(device: int = 0):
+    """(network, margin) trained by the library's kernels on layer tables the
+    batched engine computes for the 512-instance sweep (4/5 fitted, 1/5
+    calibrating the margin); made once per process and device, about two
+    seconds on a B200."""
+    if device not in _DEFAULT:
+        from . import workloads
+        from .batch import BatchSweep
+        graphs = workloads.sweep(512)
+        with BatchSweep(graphs, device) as sweep:
+            sweep.run()
+            tables = sweep.layer_tables()
+        fit = [i for i in range(len(graphs)) if i % 5]
+        cal = [i for i in range(len(graphs)) if i % 5 == 0]
+        net = PlannerNet(device, seed=0)
+        net.fit(*training_set([graphs[i] for i in fit], [tables[i] for i in fit]), steps=1500, lr=3e-3)
+        margin = calibrate_margin(net, [graphs[i] for i in cal], [tables[i] for i in cal])
+        _DEFAULT[device] = (net, margin)
+    return _DEFAULT[device]
+
+
+def predict_graph(graph: dict, net: PlannerNet | None = None, margin: float | None = None, device: int = 0) -> dict:
+    """The learned planner's prediction for one permutation graph, as the
+    keywords of NativeGraph.plan (mgbfs2_plan with MGBFS2_PLANNER_LEARNED):
+    the states the BFS settles -- exactly |<generators>| (host Schreier-Sims)
+    when the start's labels are distinct, else the network's predicted total
+    times the margin, capped by the multinomial bound -- and the predicted
+    peak layer times the margin.  The C planner chooses the bitmap or the hash
+    and sizes the hash table and frontier buffers from them; results never
+    depend on them.  Graphs outside the planner's features (matrix actions,
+    more than 20 points) raise ValueError("LEARNED_PLANNER_UNSUPPORTED")."""
+    a = graph["action"]
+    if a["kind"] != "permutation" or len(graph["start"]) > 20:
+        raise ValueError("LEARNED_PLANNER_UNSUPPORTED")
+    if net is None:
+        net, default_margin = default_planner(device)
+        margin = default_margin if margin is None else margin
+    margin = 1.5 if margin is None else margin
+    statics, states = batch_statics([graph])
+    peak, total, _ = rollout_device(net, [graph], statics=statics)
+    bound = int(states[0])
+    exact = len(set(graph["start"])) == len(graph["start"])
+    predicted = bound if exact else int(min(bound, max(1.0, float(total[0]) * margin)))
+    return {"planner": "learned", "predicted_states": max(1, predicted),
+            "predicted_peak": int(max(1, min(predicted, float(peak[0]) * margin + 1024))),
+            "exact_states": exact}
+
+
+def choose_path(graph: dict, net: PlannerNet | None = None, margin: float | None = None, device: int = 0) -> dict:
+    """The plan keywords of the learned planner for a single run: the
+    prediction of `predict_graph`, with which mgbfs2_plan takes the exact
+    bitmap when the predicted states fill at least 1/128 of the rank domain
+    (and the bitmap fits), else the hash (three layer banks when
+    inverse-closed), and sizes the table and buffers."""
+    kw = predict_graph(graph, net, margin, device)
+    kw.pop("exact_states")
+    return kw

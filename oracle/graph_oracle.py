@@ -176,6 +176,68 @@ def multiset_unrank(start, rank: int):
 
 
 # ---------------------------------------------------------------------------
+# Product of position components' multiset domains (PositionOrbitDomain,
+# crates/mgbfs-runtime/src/permutation_bitmap.rs:61-143).
+
+def position_components(n: int, generators):
+    """Classes of positions under i ~ g[i] for every generator, ordered by
+    their first position, each ascending (permutation_bitmap.rs:68-82)."""
+    parent = list(range(n))
+
+    def root(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+    for g in generators:
+        if len(g) != n or sorted(g) != list(range(n)):
+            raise ValueError("BITMAP_ORBIT_GENERATOR")
+        for i, j in enumerate(g):
+            parent[root(i)] = root(j)
+    classes = {}
+    for i in range(n):
+        classes.setdefault(root(i), []).append(i)
+    return sorted(classes.values(), key=lambda c: c[0])
+
+
+def product_domain(start, generators):
+    """[(positions, component start values, multiset size)] and the product."""
+    comps = []
+    size = 1
+    for pos in position_components(len(start), generators):
+        values = [start[i] for i in pos]
+        total = multiset_domain(values)[2]
+        comps.append((pos, values, total))
+        size *= total
+    return comps, size
+
+
+def product_rank(start, generators, state) -> int:
+    """Mixed-radix rank over the components in order, each digit the multiset
+    rank of the component's values in position order."""
+    comps, size = product_domain(start, generators)
+    rank = 0
+    for pos, values, total in comps:
+        digit = multiset_rank(values, [state[i] for i in pos])
+        rank = rank * total + digit
+    if rank >= size:
+        raise ValueError("BITMAP_RANK_RANGE")
+    return rank
+
+
+def product_unrank(start, generators, rank: int):
+    comps, size = product_domain(start, generators)
+    if not 0 <= rank < size:
+        raise ValueError("BITMAP_RANK_RANGE")
+    state = [None] * len(start)
+    for pos, values, total in reversed(comps):
+        rank, digit = divmod(rank, total)
+        for i, v in zip(pos, multiset_unrank(values, digit)):
+            state[i] = v
+    return state
+
+
+# ---------------------------------------------------------------------------
 # Generator families and certified layer tables.
 
 def lrx_generators(n: int):

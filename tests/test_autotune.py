@@ -54,3 +54,18 @@ def test_small_graphs_take_the_size_profile_without_pilots(tmp_path):
 def test_cache_path_override(monkeypatch, tmp_path):
     monkeypatch.setenv("MGBFS2_AUTOTUNE_CACHE", str(tmp_path / "x.json"))
     assert autotune.cache_path() == tmp_path / "x.json"
+
+
+def test_shape_candidates_vary_the_kept_path_only():
+    grouped = autotune.shape_candidates({"visited": "bitmap", "dedup": "grouped"},
+                                        {"visited": "bitmap", "dedup": "grouped"})
+    assert grouped[0] == {"visited": "bitmap", "dedup": "grouped"}
+    assert {"visited": "bitmap", "dedup": "grouped", "group_chunk": 2048, "blocks_per_sm": 6} in grouped
+    assert all(set(p) <= {"visited", "dedup", "group_chunk", "blocks_per_sm"} for p in grouped)
+    hashed = autotune.shape_candidates(dict(autotune.DEFAULT), {"visited": "hash", "dedup": "atomic"})
+    assert hashed[0] == autotune.DEFAULT and {"visited": "auto", "dedup": "auto", "hash_load_percent": 90} in hashed
+    bucket = autotune.shape_candidates({"visited": "bitmap", "dedup": "bucket", "shards": 1},
+                                       {"visited": "bitmap", "dedup": "bucket"})
+    assert [p.get("bucket_margin") for p in bucket] == [None, 1024, 16384]
+    assert autotune.shape_candidates(dict(autotune.DEFAULT), {"visited": "hash3", "dedup": "atomic"}) == \
+        [autotune.DEFAULT]

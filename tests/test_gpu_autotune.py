@@ -22,9 +22,14 @@ def test_pilots_compare_every_candidate_then_cache(tmp_path, lrx_layers):
     cache = tmp_path / "tune.json"
     got = autotune.choose_profile(g, 0, cache=cache)
     assert got["source"] == "pilot"
-    assert [t["plan"] for t in got["trials"]] == autotune.candidate_plans(g)
+    cands = autotune.candidate_plans(g)
+    # Stage 1: every path; stage 2: the shapes of the kept path, its default first.
+    plans = [t["plan"] for t in got["trials"]]
+    assert plans[:len(cands)] == cands and len(plans) > len(cands)
+    shapes = plans[len(cands):]
+    assert all({k: v for k, v in s.items() if k in ("visited", "dedup", "shards")} == shapes[0] for s in shapes)
     assert all(t["seconds"] is not None and t["seconds"] > 0 for t in got["trials"]), got["trials"]
-    assert got["plan"] in autotune.candidate_plans(g)
+    assert got["plan"] in plans
     again = autotune.choose_profile(g, 0, cache=cache)
     assert again["source"] == "cache" and again["plan"] == got["plan"]
     assert len(json.loads(cache.read_text())) == 1

@@ -41,7 +41,10 @@ VARIANTS = {
     "auto": {},
     "bitmap_atomic": dict(visited="bitmap", dedup="atomic"),
     "bitmap_warp": dict(visited="bitmap", dedup="warp"),
+    # one-word keys in 32-bit quotient slots where their bits allow, else 64-bit slots
     "hash": dict(visited="hash"),
+    "hash_wide": dict(visited="hash", wide_slots=True),
+    "hash_load95": dict(visited="hash", hash_load_percent=95),
     "hash3": dict(visited="hash3"),
     # every layer routed through the shard buckets
     "bitmap_bucket": dict(visited="bitmap", dedup="bucket", bucket_min_work=1),
@@ -66,6 +69,7 @@ VARIANTS = {
     # host-driven layer loop instead of the one-graph device loop
     "bitmap_atomic_hostloop": dict(visited="bitmap", dedup="atomic", host_loop=True),
     "hash_hostloop": dict(visited="hash", host_loop=True),
+    "hash_wide_hostloop": dict(visited="hash", wide_slots=True, host_loop=True),
 }
 
 
@@ -152,6 +156,18 @@ def test_lrx_small(lrx_layers, variant):
         redo += out[1].redo_layers
     if variant in ("bitmap_bucket_tight", "hash_bucket_tight"):
         assert redo > 0  # the exact redo path ran and changed nothing
+
+
+def test_s11_hash_plans_quotient_slots(lrx_layers):
+    """S11's 44-bit keys fit 32-bit quotient slots: 2^27 slots (512 MB) at the
+    default 50 % threshold instead of 2^27 64-bit slots (1 GB); same table."""
+    g = G.permutation_graph(G.lrx_generators(11), list(range(11)))
+    q = run(g, visited="hash")
+    w = run(g, visited="hash", wide_slots=True)
+    assert q[0]["table_slot_bytes"] == 4 and q[0]["table_slots"] == 1 << 27 and q[0]["hash_load_percent"] == 50
+    assert w[0]["table_slot_bytes"] == 8 and w[0]["table_slots"] == 1 << 27
+    assert q[1].layer_sizes == w[1].layer_sizes == lrx_layers[11]
+    assert q[2] == w[2] and q[3] == w[3]
 
 
 @pytest.mark.parametrize("variant", ["bitmap_warp", "bitmap_atomic", "bitmap_bucket_default", "bitmap_grouped_default"])

@@ -78,8 +78,90 @@ def test_learned_capacities_never_change_results():
     net.fit(*training_set(train, tables), steps=300)
     graphs = [G.sweep_instance(100 + i, True) for i in range(16)]
     expect = [P.packed_bfs(g["action"]["generators"], g["start"])[0] for g in graphs]
-    caps = predicted_capacities(net, graphs, margin=0.5, floor=0)  # deliberately tight: forces reruns
+    caps = predicted_capacities(net, graphs, margin=0.5, floor=0)  # deliberately tight: forces layer redos
     with BatchSweep(graphs) as sweep:
         st = sweep.run(capacities=caps)
         assert sweep.layer_tables() == expect
     assert st["complete_instances"] == 16
+
+
+# ---------------------------------------------------------------------------
+# The learned planner on single graphs (mgbfs2_plan with MGBFS2_PLANNER_LEARNED).
+
+def _projective_graph():
+    """PGL(2,13) on the 14 points of the projective line over Z/13 (x -> x+1,
+    x -> 2x, x -> -1/x; 13 stands for infinity): transitive, |G| = 2,184,
+    while the plain planner's worst-case bound is 14! and its rank domain a
+    10.9 GB bitmap."""
+    inf = 13
+
+    def inv(x):
+        return pow(x, 11, 13)  # x^(p-2) mod p
+    shift = [(x + 1) % 13 for x in range(13)] + [inf]
+    scale = [(2 * x) % 13 for x in range(13)] + [inf]
+    flip = [inf] + [(-inv(x)) % 13 for x in range(1, 13)] + [0]
+    return G.permutation_graph([shift, scale, flip], list(range(14)))
+
+
+def test_learned_plan_needs_a_prediction():
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    from multigpubfs_b200.native import NativeError
+    with NativeGraph(GraphDefinition.from_dict(_projective_graph())) as e:
+        with pytest.raises(NativeError) as info:
+            e.plan(planner="learned")
+        assert info.value.code == 1  # MGBFS2_INVALID_ARGUMENT: not a silent no-op
+
+
+def test_learned_plan_differs_from_plain_with_identical_tables():
+    from multigpubfs_b200 import GraphDefinition, native
+    from multigpubfs_b200.engine import NativeGraph
+    from multigpubfs_b200.planner import PlannerNet, predict_graph
+    g = _projective_graph()
+    assert native.group_order(g["action"]["generators"]) == 2184
+    expect, _, _ = P.packed_bfs(g["action"]["generators"], g["start"], use_bitmap=False, max_states=1 << 16)
+    net = PlannerNet(0, seed=1)  # the states are exact (|G|) whatever the network
+    kw = predict_graph(g, net, margin=1.5)
+    assert kw["predicted_states"] == 2184 and kw["exact_states"]
+    kw.pop("exact_states")
+    with NativeGraph(GraphDefinition.from_dict(g)) as e:
+        plain = e.plan()
+        r_plain = e.run()
+        learned = e.plan(**kw)
+        r_learned = e.run()
+        # An under-prediction: the table starts far too small, the device loop
+        # pauses before the threshold and the host loop grows it by rehash.
+        small = e.plan(planner="learned", predicted_states=40, predicted_peak=8)
+        r_small = e.run()
+    assert plain["visited"] == "bitmap" and plain["bitmap_bits"] == 87178291200
+    # 56-bit keys in a small table leave too few bits for quotient slots.
+    assert learned["planner"] == "learned" and learned["visited"] == "hash" and learned["table_slot_bytes"] == 8
+    assert learned["table_slots"] <= (1 << 13) and small["table_slots"] < learned["table_slots"]
+    assert r_plain.layer_sizes == r_learned.layer_sizes == r_small.layer_sizes == expect
+    assert r_plain.complete and r_learned.complete and r_small.complete
+
+
+def test_run_graph_learned_planner_reports_its_prediction(tmp_path):
+    import json
+    from multigpubfs_b200 import GraphDefinition, run_graph
+    g = GraphDefinition.from_dict(_projective_graph())
+    report = run_graph(g, tmp_path / "learned", planner="learned", autotune=False)
+    assert report["planner"]["name"] == "learned" and report["planner"]["predicted_states"] == 2184
+    assert report["plan"]["visited"] == "hash" and sum(report["layer_sizes"]) == 2184
+    plain = run_graph(g, tmp_path / "plain", autotune=False)
+    assert plain["layer_sizes"] == report["layer_sizes"] and plain["plan"]["visited"] == "bitmap"
+    assert json.loads((tmp_path / "learned" / "report.json").read_text())["status"] == "COMPLETE"
+
+
+def test_learned_underprediction_grows_the_quotient_table():
+    """S9 LRX (36-bit keys) with a prediction of 500 states: a 4096-slot
+    quotient table that the run grows by rehash, layer table unchanged."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    from tests.conftest import golden
+    g = GraphDefinition.from_dict(G.permutation_graph(G.lrx_generators(9), list(range(9))))
+    with NativeGraph(g) as e:
+        info = e.plan(visited="hash", planner="learned", predicted_states=500, predicted_peak=100)
+        r = e.run()
+    assert info["table_slot_bytes"] == 4 and info["table_slots"] == 4096
+    assert r.complete and r.layer_sizes == golden("lrx_layers.json")["layers"]["9"]

@@ -145,3 +145,39 @@ def test_domain_sizes():
     # permutation_bitmap.rs:204-293 domain sizes (full-multiset domains)
     assert G.multiset_domain([1, 1, 2, 3, 3])[2] == 30
     assert G.multiset_domain(list(range(10)))[2] == 3628800
+
+
+# ---------------------------------------------------------------------------
+# Position-component product domains: the reference's own known sizes
+# (crates/mgbfs-runtime/src/permutation_bitmap.rs:263-293) and rank bijections.
+
+PRODUCT_CASES = [
+    ([-7, 8, 10, 12, 90, 91], [[1, 0, 3, 2, 4, 5]], 4),
+    ([1, 1, 2, 3, 3], [[2, 1, 0, 4, 3], [1, 0, 2, 3, 4]], 3),
+    ([2, 0, 1], [[1, 0, 2], [0, 2, 1]], 6),
+]
+
+
+def test_product_domain_sizes_match_reference():
+    for start, gens, size in PRODUCT_CASES:
+        assert G.product_domain(start, gens)[1] == size
+        for r in range(size):
+            assert G.product_rank(start, gens, G.product_unrank(start, gens, r)) == r
+    # S10 acting on 10 of 14 points: the four fixed points shrink the domain to 10!.
+    start = list(range(14))
+    gens = []
+    for i in range(9):
+        g = list(range(14))
+        g[i], g[i + 1] = g[i + 1], g[i]
+        gens.append(g)
+    comps, size = G.product_domain(start, gens)
+    assert size == 3628800 and len(comps) == 5
+    for r in (0, 1, 1024, size - 1):
+        s = G.product_unrank(start, gens, r)
+        assert s[10:] == start[10:] and G.product_rank(start, gens, s) == r
+    bad = list(start)
+    bad[0], bad[13] = bad[13], bad[0]
+    with pytest.raises(ValueError):
+        G.product_rank(start, gens, bad)
+    with pytest.raises(ValueError):
+        G.position_components(3, [[0, 0, 1]])
