@@ -1,33 +1,41 @@
 #!/usr/bin/env python
-"""Benchmark: exact full BFS of S13 LRX on one B200 (one step = one whole BFS).
+"""Benchmark of the exact BFS engine on B200s.  Prints ONE JSON line (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference] [--workload NAME]
 
-Prints ONE JSON line (rank 0).  Workload (default ``s13-lrx``): the Cayley
-graph of S13 under L (cyclic left shift), R (cyclic right shift) and X (swap
-positions 0,1), from the identity: 13! = 6,227,020,800 states, 79 layers,
-18,681,062,400 successors per BFS, exact Lehmer-rank bitmap visited set.  Every
-timed BFS's layer table is checked against the reference's shipped table.
+Workloads (one step = one pass of the workload):
 
-* ``value``: successors/s over the K timed BFS runs, device-timed with CUDA
-  events bracketing the K runs (synchronised before and after), inputs
-  resident; with N GPUs (torchrun) each rank runs its own replica (the BFS does
-  not shard on one node in this build) and value = N * E / max-over-ranks time.
-* ``e2e``: the same metric through the C-ABI handle from host buffers:
-  create -> plan -> run -> layer table -> samples -> destroy, every step.
-* ``roofline``: algorithmic bytes B_alg = 16*N + 32*E (8-byte packed states
-  written once and read once; one 32-byte DRAM sector per visited test) over
-  the summed duration of the layer-expansion kernel launches, against the
-  measured HBM copy bandwidth.
-* ``cpu_baseline``: the C oracle (a CPU restatement of the reference's exact
-  BFS) on all host cores, over a bounded sample (the first 32 BFS layers of the
-  same graph).
+* ``s13-lrx`` (default, the headline): the Cayley graph of S13 under L (cyclic
+  left shift), R (cyclic right shift) and X (swap of positions 0, 1), full BFS
+  from the identity: 13! = 6,227,020,800 states, 79 layers, 18,681,062,400
+  successors, exact Lehmer-rank bitmap.  Every BFS's table is checked against
+  the reference's shipped table.
+* ``s13-coxeter``: S13 under the adjacent transpositions s1..s12 (inverse-closed),
+  checked against the Mahonian layer certificate.
+* ``s11-lrx-hash``: S11 LRX through the exact-key open-addressing hash of all
+  visited states, checked against the reference's packed-search table.
+* ``sweep512``: 512 seeded instances (n in {7..10}, 2-3 random generators,
+  directed and inverse-closed variants) in one batched run, every table
+  checked against the oracle's fixture.  With N GPUs the instances are split
+  between the ranks by exact work (g |G| per instance) and rank 0 checks the
+  gathered tables.
+* ``planner-s12``: learned vs plain planner on 128 S12 instances and on the
+  held-out sweep; tables checked against the oracle's fixtures.
+
+Keys of the line: ``value`` is successors/s with inputs resident, timed with
+CUDA events on the launching stream over the K steps; ``e2e`` is the same
+metric through the C ABI from host buffers (create -> plan -> run -> tables ->
+destroy, every step, wall clock); ``roofline`` divides algorithmic bytes
+B_alg = 16 N + 32 E p by the summed duration of the layer-expansion launches;
+``cpu_baseline`` is the C oracle (a CPU restatement of the reference's exact
+BFS) on all host cores over a bounded sample of the same workload.
 ``--impl reference`` times that CPU implementation alone (rank 0).
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -39,7 +47,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 HBM_FALLBACK_GBS = 6650.0
-CPU_SAMPLE_LAYERS = 32
+SWEEP_SEED = 20261203
+HELDOUT_SEED = SWEEP_SEED + 4096
 
 
 def lrx(n):
@@ -67,20 +76,29 @@ WORKLOADS = {
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
 }
+BATCHED = ("sweep512", "planner-s12")
+
+# Bounded CPU samples (about 10-30 s of C-oracle work on a 16-core host): the
+# layers run of each workload's sample; s11-lrx-hash runs whole, and sweep512
+# runs its first 128 instances whole.
+CPU_SAMPLE_LAYERS = {"s13-lrx": 32, "s13-coxeter": 20, "planner-s12": 17}
 
 
 def measured_peak():
-    path = ROOT / "MEASURED_PEAKS.json"
     try:
-        d = json.loads(path.read_text())
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return HBM_FALLBACK_GBS, "fallback"
 
 
+def golden(name):
+    return json.loads((ROOT / "tests" / "golden" / name).read_text())
+
+
 def expected_layers(name, n):
     if name == "s13-lrx":
-        return json.loads((ROOT / "tests/golden/lrx13_layers.json").read_text())["layers"]
+        return golden("lrx13_layers.json")["layers"]
     if name == "s13-coxeter":
         sizes = [1]
         for i in range(1, n + 1):
@@ -94,8 +112,24 @@ def expected_layers(name, n):
             sizes = out
         return sizes
     if name == "s11-lrx-hash":
-        return json.loads((ROOT / "tests/golden/lrx_layers.json").read_text())["layers"]["11"]
+        return golden("lrx_layers.json")["layers"]["11"]
     return None
+
+
+def generator_digest(graph):
+    import hashlib
+    text = json.dumps(graph["action"]["generators"], separators=(",", ":"))
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def sweep_fixture(key, graphs):
+    """The oracle's tables for `graphs` (tests/golden/sweep_tables.json), after
+    checking that the seeded generators are the ones the fixture was made from."""
+    fx = golden("sweep_tables.json")[key]
+    digests = [generator_digest(g) for g in graphs]
+    if digests != fx["generators_sha256"][:len(graphs)]:
+        raise RuntimeError(f"{key}: generated instances differ from the fixture's")
+    return fx["tables"]
 
 
 class ClockSampler:
@@ -152,34 +186,65 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(threads=None):
-    """The C oracle on the first CPU_SAMPLE_LAYERS layers of S13 LRX, all host cores."""
+# ---------------------------------------------------------------------------
+# CPU baseline: the C oracle on a bounded sample of the same workload.
+
+def cpu_sample(name, threads=None):
     from oracle import packed_oracle as P
+    from multigpubfs_b200 import workloads
     threads = threads or P.default_threads()
     P.library()
     t = time.perf_counter()
-    sizes, _, _ = P.packed_bfs(lrx(13), list(range(13)), use_bitmap=True, threads=threads,
-                               max_layers=CPU_SAMPLE_LAYERS, partial=True)
+    succ = states = 0
+    if name in WORKLOADS:
+        w = WORKLOADS[name]
+        layers = CPU_SAMPLE_LAYERS.get(name)
+        bitmap = w["visited"] == "bitmap"
+        sizes, _, _ = P.packed_bfs(w["gens"], list(range(w["n"])), use_bitmap=bitmap, threads=threads,
+                                   max_layers=layers or (1 << 16), partial=bool(layers))
+        states, succ = sum(sizes), len(w["gens"]) * sum(sizes)
+        what = (f"{name} layers 0-{len(sizes) - 1}" if layers else f"{name} full BFS") + \
+               f" ({'Lehmer bitmap' if bitmap else 'exact hash set'})"
+    elif name == "sweep512":
+        graphs = workloads.sweep(512)[:128]
+        for g in graphs:
+            sizes, _, _ = P.packed_bfs(g["action"]["generators"], g["start"], use_bitmap=True, threads=threads)
+            states += sum(sizes)
+            succ += len(g["action"]["generators"]) * sum(sizes)
+        what = "the first 128 of the 512 sweep instances, full BFS each (Lehmer bitmap)"
+    else:
+        g = workloads.planner_instance(0)
+        layers = CPU_SAMPLE_LAYERS[name]
+        sizes, _, _ = P.packed_bfs(g["action"]["generators"], g["start"], use_bitmap=True, threads=threads,
+                                   max_layers=layers, partial=True)
+        states, succ = sum(sizes), len(g["action"]["generators"]) * sum(sizes)
+        what = f"S12 planner instance 0, layers 0-{len(sizes) - 1} (Lehmer bitmap)"
     dt = time.perf_counter() - t
-    succ = 3 * sum(sizes)
     return {"value": succ / dt, "unit": "successors/s", "cores": threads, "kind": "port",
-            "sample": f"S13 LRX layers 0-{CPU_SAMPLE_LAYERS - 1} ({sum(sizes):,} states, {succ:,} successors), "
-                      f"C oracle (restated reference exact BFS), {dt:.2f} s"}
+            "sample": f"{what}: {states:,} states, {succ:,} successors, C oracle (restated reference exact BFS), "
+                      f"{dt:.2f} s"}
+
+
+def workload_desc(name):
+    if name in WORKLOADS:
+        return WORKLOADS[name]["desc"]
+    if name == "sweep512":
+        return ("batched sweep: 512 instances (256 seeds x directed / inverse-closed), n in {7,8,9,10}, 2-3 seeded "
+                "random generators, exact per-instance Lehmer bitmaps")
+    return "learned vs plain planner: 128 S12 instances (2-4 random generators plus inverses), whole device"
 
 
 def reference_arm(args, rank):
     if rank != 0:
         return 0
-    name = args.workload
     for _ in range(args.warmup):
-        cpu_baseline()
-    runs = [cpu_baseline() for _ in range(args.steps)]
+        cpu_sample(args.workload)
+    runs = [cpu_sample(args.workload) for _ in range(args.steps)]
     value = statistics.median(r["value"] for r in runs)
     line = {"metric": "successors/s", "value": value, "unit": "successors/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOADS.get(name, WORKLOADS["s13-lrx"])["desc"],
-                       "sample_layers": CPU_SAMPLE_LAYERS},
+            "config": {"workload": workload_desc(args.workload)},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "successors/s", "cores": runs[0]["cores"], "kind": "port",
                              "sample": runs[0]["sample"]},
@@ -188,34 +253,120 @@ def reference_arm(args, rank):
     return 0
 
 
-def bench_sweep(args, local):
-    """Batched sweep: 512 instances (256 seeds x {directed, inverse-closed}),
-    each wave one persistent cooperative launch."""
+def gpu_index(local):
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    return visible[local] if visible and visible[0] else str(local)
+
+
+def roofline(b_alg, seconds, kernel, traffic=None, traffic_source=None, **extra):
+    peak, peak_kind = measured_peak()
+    achieved = b_alg / seconds / 1e9
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "traffic": traffic, "peak_kind": peak_kind, "b_alg_bytes": b_alg, "kernel": kernel}
+    if traffic_source:
+        out["traffic_source"] = traffic_source
+    out.update(extra)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Batched sweep.
+
+def bench_sweep(args, rank, world, local):
+    """512 instances; with N ranks each runs a work-balanced share as its own
+    waves (no collective on the data path) and rank 0 checks the gathered
+    tables against the oracle's fixture."""
     import torch
-    from multigpubfs_b200 import workloads
+    import torch.distributed as dist
+    from datetime import timedelta
+    from multigpubfs_b200 import native, replicas, workloads
     from multigpubfs_b200.batch import BatchSweep
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
     graphs = workloads.sweep(512)
-    with BatchSweep(graphs, local) as sweep:
+    expect = sweep_fixture("sweep512", graphs)
+    _, order = native.graph_statics([(g["action"]["generators"], g["start"]) for g in graphs])
+    work = [len(g["action"]["generators"]) * int(s) for g, s in zip(graphs, order)]
+    owner = replicas.partition_instances(work, world)
+    ids = [i for i in range(len(graphs)) if owner[i] == rank]
+    mine = [graphs[i] for i in ids]
+    mine_expect = [expect[i] for i in ids]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with BatchSweep(mine, local) as sweep:
         for _ in range(args.warmup):
             sweep.run(host_loop=args.host_loop)
-        ref = sweep.layer_tables()
-        runs = [sweep.run(host_loop=args.host_loop) for _ in range(args.steps)]
-        assert sweep.layer_tables() == ref
-    dev = sum(r["device_seconds"] for r in runs) / len(runs)
-    succ, states = runs[0]["successors"], runs[0]["states"]
-    line = {"metric": "successors/s", "value": succ / dev, "unit": "successors/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "batched sweep: 512 instances (256 seeds x directed / inverse-closed), n in "
-                                   "{7,8,9,10}, 2-3 seeded random generators, exact per-instance Lehmer bitmaps, "
-                                   "each wave one persistent cooperative launch",
-                       "instances": len(graphs), "states_per_step": states, "successors_per_step": succ},
-            "settled_states_per_s": states / dev,
-            "wall_ms_per_step": sum(r["seconds"] for r in runs) / len(runs) * 1e3,
-            "waves": runs[0]["waves"], "launches_per_step": runs[0]["kernel_launches"],
-            "layer_steps": runs[0]["layer_steps"], "gpu_launches": sum(r["kernel_launches"] for r in runs)}
-    print(json.dumps(line), flush=True)
+        assert sweep.layer_tables() == mine_expect, "sweep tables differ from the oracle fixture (warm-up)"
+        barrier()
+        with ClockSampler(gpu_index(local)) as clocks:
+            runs = [sweep.run(host_loop=args.host_loop) for _ in range(args.steps)]
+        barrier()
+        tables = sweep.layer_tables()
+    assert tables == mine_expect, "sweep tables differ from the oracle fixture (timed runs)"
+    dev_s = sum(r["device_seconds"] for r in runs)
+    succ = runs[0]["successors"]
+    states = runs[0]["states"]
+    launches = sum(r["kernel_launches"] for r in runs)
+
+    # e2e: a fresh batch from host graph descriptions every step.
+    e2e = []
+    h2d = sum(8 * len(g["start"]) + 4 * len(g["start"]) * len(g["action"]["generators"]) for g in mine)
+    d2h = 0
+    for i in range(args.steps + 1):
+        barrier()
+        t0 = time.perf_counter()
+        with BatchSweep(mine, local) as sweep:
+            sweep.run(host_loop=args.host_loop)
+            got = sweep.layer_tables()
+        torch.cuda.synchronize()
+        if i:
+            e2e.append(time.perf_counter() - t0)
+        assert got == mine_expect
+        d2h = 8 * sum(len(t) for t in got)
+    e2e_s = sum(e2e) / len(e2e)
+
+    total_succ, dev_max, e2e_max = succ, dev_s, e2e_s
+    if world > 1:
+        # The job's time is the slowest rank's; its work is every rank's.
+        t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        n = torch.tensor([succ], dtype=torch.int64, device=dev)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        dev_max, e2e_max, total_succ = float(t[0].item()), float(t[1].item()), int(n.item())
+        gathered = replicas.gather_tables(ids, tables, len(graphs), device=dev)
+        if rank == 0:
+            assert gathered == expect, "gathered sweep tables differ from the oracle fixture"
+    if rank == 0:
+        all_states = sum(map(sum, expect))
+        line = {"metric": "successors/s", "value": total_succ * args.steps / dev_max, "unit": "successors/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": dev_max / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic",
+                "config": {"workload": workload_desc("sweep512"), "instances": len(graphs),
+                           "states_per_step": all_states, "successors_per_step": total_succ,
+                           "parallelism": f"instances split over {world} rank(s) by g|G|" if world > 1 else "1 GPU",
+                           "l2": "per-instance bitmaps and frontiers together exceed L2 (about 0.3 GB per step)"},
+                "settled_states_per_s": all_states * args.steps / dev_max,
+                "wall_ms_per_step": sum(r["seconds"] for r in runs) / len(runs) * 1e3,
+                "e2e": {"value": total_succ / e2e_max, "unit": "successors/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "roofline": roofline(16 * states + 32 * succ, dev_s / args.steps,
+                                     "batch_wave (one persistent cooperative launch per wave)", traffic=None),
+                "waves": runs[0]["waves"], "layer_steps": runs[0]["layer_steps"],
+                "gpu_launches": launches, "clocks": clocks.summary()}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_sample("sweep512")
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -223,27 +374,25 @@ def bench_planner(args, local):
     """Learned vs plain planner on batched sweeps.  The network is fitted by
     the library's kernels on 4/5 of the layer tables of the 512-instance sweep
     plus 32 S11 / S12 instances on other seeds, and its capacity margin is
-    calibrated on the other 1/5.  The plain run
-    reserves each instance's orbit bound n!, the learned run its predicted peak
-    times the margin (exact rerun on overflow); both must give identical
-    tables.  Scenarios: 128 S12 instances with the whole device, and a
-    held-out 512-instance sweep (other seeds) under a 1 GiB budget.  The
+    calibrated on the other 1/5.  The plain run reserves each instance's orbit
+    bound n!, the learned run its predicted peak times the margin (a layer
+    that outgrows it is redone in a larger segment); both must give the
+    oracle's tables.  Scenarios: 128 S12 instances with the whole device, and
+    the held-out 512-instance sweep under 1 GiB and 256 MiB budgets.  The
     learned wall time includes the prediction."""
-    import math
     import torch
-    from multigpubfs_b200 import workloads
+    from multigpubfs_b200 import native, workloads
     from multigpubfs_b200.batch import BatchSweep
     from multigpubfs_b200.planner import (PlannerNet, calibrate_margin, predicted_capacities, rollout_device,
                                           training_set)
     torch.cuda.set_device(local)
     t0 = time.perf_counter()
-    # Layer tables the BFS generates: the 512-instance sweep (n in 7..10) and
-    # 32 S11 / S12 instances on seeds disjoint from the scenarios' instances.
     train = workloads.sweep(512) + [workloads.planner_instance(i, n=n, seed_base=20261204 + 50000 + 100 * n)
                                     for n in (11, 12) for i in range(16)]
     with BatchSweep(train, local) as sw:
         sw.run()
         tables = sw.layer_tables()
+    assert tables[:512] == sweep_fixture("sweep512", train[:512]), "training tables differ from the oracle fixture"
     fit_ids = [i for i in range(len(train)) if i % 5]
     cal_ids = [i for i in range(len(train)) if i % 5 == 0]
     X, T = training_set([train[i] for i in fit_ids], [tables[i] for i in fit_ids])
@@ -251,15 +400,32 @@ def bench_planner(args, local):
     hist = net.fit(X, T, steps=2000, lr=3e-3)
     margin = calibrate_margin(net, [train[i] for i in cal_ids], [tables[i] for i in cal_ids])
     train_s = time.perf_counter() - t0
+    s12 = [workloads.planner_instance(i) for i in range(args.instances)]
+    heldout = workloads.sweep(512, seed_base=HELDOUT_SEED)
+    s12_fixture = golden("sweep_tables.json")["planner_s12"]
     scenarios = [
-        ("s12", f"{args.instances} S12 instances, 2-4 seeded random generators plus inverses, whole device",
-         [workloads.planner_instance(i) for i in range(args.instances)], None),
+        ("s12", f"{args.instances} S12 instances, 2-4 seeded random generators plus inverses, whole device", s12,
+         None),
         ("sweep_heldout_1gib", "512-instance sweep on held-out seeds, n in {7,8,9,10}, 1 GiB memory budget",
-         workloads.sweep(512, seed_base=20261203 + 4096), 1 << 30),
+         heldout, 1 << 30),
         ("sweep_heldout_256mib", "512-instance sweep on held-out seeds, n in {7,8,9,10}, 256 MiB memory budget",
-         workloads.sweep(512, seed_base=20261203 + 4096), 1 << 28),
+         heldout, 1 << 28),
     ]
-    keys = ("seconds", "device_seconds", "waves", "redo_instances", "states", "successors")
+
+    def check(name, graphs, got):
+        # Every table against the oracle: the fixture where it has one, and
+        # the exact state count |G| (host Schreier-Sims) for every instance.
+        if name == "s12":
+            for k, i in enumerate(s12_fixture["indices"]):
+                if i < len(graphs):
+                    assert generator_digest(graphs[i]) == s12_fixture["generators_sha256"][k]
+                    assert got[i] == s12_fixture["tables"][k], f"S12 instance {i} differs from the oracle fixture"
+            _, states = native.graph_statics([(g["action"]["generators"], g["start"]) for g in graphs])
+            assert [sum(t) for t in got] == [int(s) for s in states], "S12 state counts differ from |G|"
+        else:
+            assert got == sweep_fixture("sweep512_heldout", graphs), f"{name}: tables differ from the oracle fixture"
+
+    keys = ("seconds", "device_seconds", "waves", "redo_layers", "redo_instances", "states", "successors")
     report, same_all = {}, True
     for name, desc, graphs, budget in scenarios:
         t1 = time.perf_counter()
@@ -276,6 +442,7 @@ def bench_planner(args, local):
         out = {}
         for arm, rs in runs.items():
             assert all(r["layer_tables"] == rs[0]["layer_tables"] for r in rs)
+            check(name, graphs, rs[0]["layer_tables"])
             out[arm] = sorted(rs, key=lambda r: r["seconds"])[len(rs) // 2]
         same = out["plain"]["layer_tables"] == out["learned"]["layer_tables"]
         same_all &= same
@@ -285,6 +452,7 @@ def bench_planner(args, local):
         learned_wall = out["learned"]["seconds"] + predict_s
         report[name] = {
             "workload": desc, "instances": len(graphs), "memory_budget_bytes": budget, "identical_tables": same,
+            "oracle_checked": True,
             "plain": {k: out["plain"][k] for k in keys},
             "learned": dict({k: out["learned"][k] for k in keys}, predict_seconds=predict_s,
                             wall_with_prediction=learned_wall),
@@ -294,43 +462,31 @@ def bench_planner(args, local):
             "peak_log_true_over_predicted": {"median_abs": sorted(abs(x) for x in logr)[len(logr) // 2],
                                              "min": logr[0], "max": logr[-1]}}
     main_s = report["s12"]
-    line = {"metric": "successors/s", "value": main_s["learned"]["successors"] / main_s["learned"]["wall_with_prediction"],
+    learned = main_s["learned"]
+    line = {"metric": "successors/s", "value": learned["successors"] / learned["device_seconds"],
             "unit": "successors/s", "n_gpus": 1, "steps": max(1, args.steps), "warmup": 1,
-            "ms_per_step": main_s["learned"]["wall_with_prediction"] * 1e3, "higher_is_better": True,
+            "ms_per_step": learned["device_seconds"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "learned vs plain planner on batched sweeps (value: S12 scenario, learned)"},
+            "config": {"workload": "learned vs plain planner on batched sweeps (value: S12 scenario, learned, "
+                                   "device time; e2e: its wall time with the prediction)"},
+            "e2e": {"value": learned["successors"] / learned["wall_with_prediction"], "unit": "successors/s",
+                    "h2d_bytes_per_step": sum(8 * 12 + 4 * 12 * len(g["action"]["generators"]) for g in s12),
+                    "d2h_bytes_per_step": 8 * sum(len(t) for t in s12_fixture["tables"])},
+            "roofline": roofline(16 * learned["states"] + 32 * learned["successors"], learned["device_seconds"],
+                                 "batch_wave (S12 scenario, learned capacities)"),
             "identical_tables": same_all, "scenarios": report,
             "predictor": {"train_rows": int(len(X)), "loss_first": hist[0], "loss_last": hist[-1],
                           "train_seconds": train_s, "margin": margin}}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample("planner-s12")
     print(json.dumps(line), flush=True)
     return 0 if same_all else 1
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["native", "reference"], default="native")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["sweep512", "planner-s12"], default="s13-lrx")
-    ap.add_argument("--host-loop", action="store_true",
-                    help="layers as separate kernel launches with a host round trip each (for a profiler); "
-                         "by default a wave of the sweep, or a fused BFS, is one persistent launch")
-    ap.add_argument("--instances", type=int, default=128, help="planner-s12: number of S12 instances")
-    ap.add_argument("--dedup", default=None)
-    ap.add_argument("--visited", default=None)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return reference_arm(args, rank)
-    if args.workload == "sweep512":
-        return bench_sweep(args, local)
-    if args.workload == "planner-s12":
-        return bench_planner(args, local)
+# ---------------------------------------------------------------------------
+# Single-graph workloads.
 
+def bench_single(args, rank, world, local):
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -357,12 +513,10 @@ def main():
     for _ in range(args.warmup):
         r = eng.run()
         assert r.layer_sizes == expect, "layer table mismatch in warm-up"
-    visible = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
-    gpu_index = visible[local] if visible and visible[0] else str(local)
     results = []
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_index) as clocks:
+    with ClockSampler(gpu_index(local)) as clocks:
         start.record()
         wall0 = time.perf_counter()
         for _ in range(args.steps):
@@ -371,6 +525,10 @@ def main():
         barrier()
         wall = time.perf_counter() - wall0
     device_s = start.elapsed_time(stop) * 1e-3
+    # The engine runs on its own stream and each run() returns after its
+    # stream is done, so the torch events bracket the whole K runs; the
+    # engine's own CUDA-event time of each run is summed beside it.
+    engine_s = sum(r.device_seconds for r in results)
     for r in results:
         assert r.complete and r.layer_sizes == expect, "layer table mismatch in a timed run"
     device_max = device_s
@@ -382,6 +540,7 @@ def main():
         device_max = view["device_seconds_max"]
     succ = results[0].successors
     states = results[0].states
+    tests = results[0].visited_tests
     kernel_s = sum(r.kernel_seconds for r in results) / len(results)
     launches = sum(r.kernel_launches for r in results)
     eng.close()
@@ -409,14 +568,14 @@ def main():
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
 
     if rank == 0:
-        peak, peak_kind = measured_peak()
-        b_alg = 16 * states + 32 * succ
-        achieved = b_alg / kernel_s / 1e9
-        traffic = None
+        p_probe = 1
+        b_alg = 16 * states + 32 * succ * p_probe
+        traffic, source = None, None
         prof = ROOT / "profiles" / f"traffic_{args.workload}.json"
         if prof.exists():
             try:
                 traffic = json.loads(prof.read_text()).get(plan["dedup"], {}).get("dram_bytes_per_bfs")
+                source = f"ncu capture summarised in profiles/{prof.name}, not measured in this run"
             except Exception:
                 traffic = None
         kernel_names = {"grouped": "expand_grouped (grouped layers; small layers expand_packed)",
@@ -435,29 +594,62 @@ def main():
             "dtype": "u64",
             "data": "synthetic",
             "config": {"workload": w["desc"], "visited": plan["visited"], "dedup": plan["dedup"],
-                       "planner": plan["planner"], "parallelism": f"replicas{world}",
-                       "states_per_bfs": states, "successors_per_bfs": succ,
-                       "l2": "working set larger than L2 (bitmap %d MB, frontiers up to several GB)"
-                             % (plan["bitmap_bits"] // 8 // (1 << 20))},
+                       "planner": plan["planner"], "parallelism": f"replicas{world}" + (
+                           " (each GPU runs the whole BFS; the BFS itself is not split)" if world > 1 else ""),
+                       "states_per_bfs": states, "successors_per_bfs": succ, "visited_tests_per_bfs": tests,
+                       "l2": "working set larger than L2 (%s)" % (
+                           "bitmap %d MB, frontiers up to several GB" % (plan["bitmap_bits"] // 8 // (1 << 20))
+                           if plan["visited"] == "bitmap" else
+                           "table of %d slots = %d MB" % (plan["table_slots"], plan["table_slots"] * 8 >> 20))},
             "settled_states_per_s": world * states * args.steps / device_max,
             "wall_ms_per_step": wall / args.steps * 1e3,
+            "engine_ms_per_step": engine_s / args.steps * 1e3,
             "kernel_ms_per_step": kernel_s * 1e3,
             "e2e": {"value": world * succ / float(e2e_t.item()), "unit": "successors/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "b_alg_bytes": b_alg,
-                         "kernel": kernel_names.get(plan["dedup"], "expand_packed (fused layer expansion)")},
+            "roofline": roofline(b_alg, kernel_s,
+                                 kernel_names.get(plan["dedup"], "expand_packed (fused layer expansion)"),
+                                 traffic=traffic, traffic_source=source,
+                                 **({"probes_per_test": "1 (lower bound)"} if plan["visited"] != "bitmap" else {})),
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_sample(args.workload)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["native", "reference"], default="native")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + list(BATCHED), default="s13-lrx")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="layers as separate kernel launches with a host round trip each (for a profiler); "
+                         "by default a wave of the sweep, or a fused BFS, is one persistent launch")
+    ap.add_argument("--instances", type=int, default=128, help="planner-s12: number of S12 instances")
+    ap.add_argument("--dedup", default=None)
+    ap.add_argument("--visited", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+    if args.workload == "sweep512":
+        return bench_sweep(args, rank, world, local)
+    if args.workload == "planner-s12":
+        if world > 1 and rank != 0:
+            return 0
+        return bench_planner(args, local)
+    return bench_single(args, rank, world, local)
 
 
 if __name__ == "__main__":
