@@ -543,6 +543,9 @@ def bench_single(args, rank, world, local):
     tests = results[0].visited_tests
     kernel_s = sum(r.kernel_seconds for r in results) / len(results)
     launches = sum(r.kernel_launches for r in results)
+    # The hash's probes per visited test, measured on the final table: every
+    # stored key's distance from its home slot plus one (mgbfs2_table_probes).
+    probes = eng.table_probes()[0] if plan["visited"] == "hash" else 1.0
     eng.close()
 
     # ---- e2e: C-ABI handle from host buffers, every step ------------------------------
@@ -568,8 +571,7 @@ def bench_single(args, rank, world, local):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
 
     if rank == 0:
-        p_probe = 1
-        b_alg = 16 * states + 32 * succ * p_probe
+        b_alg = int(16 * states + 32 * succ * probes)
         traffic, source = None, None
         prof = ROOT / "profiles" / f"traffic_{args.workload}.json"
         if prof.exists():
@@ -600,7 +602,8 @@ def bench_single(args, rank, world, local):
                        "l2": "working set larger than L2 (%s)" % (
                            "bitmap %d MB, frontiers up to several GB" % (plan["bitmap_bits"] // 8 // (1 << 20))
                            if plan["visited"] == "bitmap" else
-                           "table of %d slots = %d MB" % (plan["table_slots"], plan["table_slots"] * 8 >> 20))},
+                           "table of %d slots = %d MB" % (plan["table_slots"],
+                                                          plan["table_slots"] * plan["table_slot_bytes"] >> 20))},
             "settled_states_per_s": world * states * args.steps / device_max,
             "wall_ms_per_step": wall / args.steps * 1e3,
             "engine_ms_per_step": engine_s / args.steps * 1e3,
@@ -610,7 +613,10 @@ def bench_single(args, rank, world, local):
             "roofline": roofline(b_alg, kernel_s,
                                  kernel_names.get(plan["dedup"], "expand_packed (fused layer expansion)"),
                                  traffic=traffic, traffic_source=source,
-                                 **({"probes_per_test": "1 (lower bound)"} if plan["visited"] != "bitmap" else {})),
+                                 **({"probes_per_test": round(probes, 4),
+                                     "probes_source": "mean over the final table's keys (mgbfs2_table_probes)",
+                                     "table_slot_bytes": plan["table_slot_bytes"]}
+                                    if plan["visited"] == "hash" else {})),
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

@@ -98,6 +98,9 @@ typedef struct {
    * memory allow).  They change speed only. */
   uint32_t group_chunk;
   uint32_t blocks_per_sm;
+  uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 4 up to
+                                  4 generators, else 2) */
+  uint32_t reserved;
 } mgbfs2_plan_request;
 
 /* Inverse-closed packed graphs tag every frontier state with the generator
@@ -142,7 +145,7 @@ typedef struct {
   uint32_t group_chunk;      /* parents per grouped work item */
   uint32_t blocks_per_sm;    /* requested resident blocks per SM, 0 = kernel defaults */
   uint32_t rank_components;  /* bitmap: position components of the rank domain (1 = the whole multiset) */
-  uint32_t reserved;
+  uint32_t parents_per_thread; /* fused layers' states per thread and tile */
 } mgbfs2_plan_info;
 
 typedef struct {
@@ -223,6 +226,13 @@ MGBFS2_API int mgbfs2_checkpoint_resume(mgbfs2_graph* graph, const char* path);
  * recorded), so a caller can archive every layer, as the reference's layer
  * archive does (scripts/bfs_tail_archive.py:96-131). */
 MGBFS2_API int mgbfs2_frontier_words(mgbfs2_graph* graph, uint64_t* out, size_t capacity, size_t* count);
+
+/* After a run on the all-visited hash: the mean number of slots an insert or
+ * a successful lookup of each stored key reads (its distance from its home
+ * slot plus one, over every key in the table) and the number of keys.  The
+ * measured probes per visited test of the roofline's algorithmic bytes.
+ * No reference counterpart. */
+MGBFS2_API int mgbfs2_table_probes(mgbfs2_graph* graph, double* mean_probes, uint64_t* keys);
 
 /* Static message for a status code (reference: native_fault.rs error markers). */
 MGBFS2_API const char* mgbfs2_status_string(int code);

@@ -24,6 +24,11 @@ margin of routed layers, the growth threshold of the hash table, and the
 resident blocks of the fused kernels; the stage-1 plan with default shapes is
 the default trial.  Results never depend on the choice: every path and shape
 is exact and only changes speed.
+
+A batched sweep is tuned the same way (`choose_sweep_shape`): its tile size and
+resident blocks per SM are timed on a spread sample of the sweep's instances,
+every trial's layer tables must equal the default's, and the keep-the-default
+rule and the cache apply.
 """
 from __future__ import annotations
 
@@ -88,10 +93,12 @@ def shape_candidates(plan: dict, resolved: dict) -> list[dict]:
     elif dedup == "bucket":
         out += [dict(plan, bucket_margin=m) for m in (1024, 16384)]
     elif visited == "hash":
-        out += [dict(plan, hash_load_percent=f) for f in (50, 90)]
+        out += [dict(plan, hash_load_percent=f) for f in (35, 70)]
+        out.append(dict(plan, parents_per_thread=4 if resolved.get("parents_per_thread") == 2 else 2))
         out += [dict(plan, blocks_per_sm=b) for b in (4, 8)]
     elif visited == "bitmap":
         out += [dict(plan, blocks_per_sm=b) for b in (3, 6)]
+        out.append(dict(plan, parents_per_thread=2 if resolved.get("parents_per_thread", 4) == 4 else 4))
     return out
 
 
@@ -203,3 +210,69 @@ def choose_profile(graph: GraphDefinition, device: int = 0, *, budget_seconds: f
         entries[key] = {"plan": choice, "trials": trials, "pilot_layers": depth}
         store_cache(path, entries)
     return {"plan": choice, "source": "pilot", "trials": trials, "pilot_layers": depth}
+
+
+SWEEP_SAMPLE = 64                  # instances a sweep pilot runs
+SWEEP_SHAPES = [{}, {"tile_entries": 512}, {"tile_entries": 256}, {"blocks_per_sm": 3}, {"blocks_per_sm": 2}]
+
+
+def sweep_sample(count: int, sample: int = SWEEP_SAMPLE) -> list[int]:
+    """Indices of the instances a sweep pilot runs: `sample` of them spread
+    evenly over the sweep (all of them for smaller sweeps)."""
+    if count <= sample:
+        return list(range(count))
+    return sorted({(k * count) // sample for k in range(sample)})
+
+
+def sweep_cache_key(graphs, device_name: str, build: str) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for g in graphs:
+        h.update(GraphDefinition.from_dict(g).digest().encode() if isinstance(g, dict) else g.digest().encode())
+    return f"sweep:{h.hexdigest()[:32]}|{device_name}|{build}"
+
+
+def choose_sweep_shape(graphs, device: int = 0, *, sample: int = SWEEP_SAMPLE, budget_seconds: float = 30.0,
+                       cache: Path | None = None, use_cache: bool = True) -> dict:
+    """The batched sweep's shape (keyword arguments of BatchSweep.run) for
+    `graphs` on `device`: from the cache, or by timing SWEEP_SHAPES on a
+    sample of the instances (each trial runs the sample twice and keeps the
+    second device time; a trial whose tables differ from the default's is
+    discarded).  Returns {"shape", "source", "trials", "sample"}."""
+    import torch
+    from . import native
+    from .batch import BatchSweep
+    graphs = list(graphs)
+    device_name = torch.cuda.get_device_name(device)
+    stamp = Path(native.LIBRARY).with_suffix(".stamp")
+    build = stamp.read_text().strip()[:16] if stamp.exists() else "unbuilt"
+    path = cache or cache_path()
+    key = sweep_cache_key(graphs, device_name, build)
+    entries = load_cache(path) if use_cache else {}
+    if key in entries:
+        return {"shape": entries[key]["shape"], "source": "cache", "trials": entries[key].get("trials", []),
+                "sample": entries[key].get("sample", [])}
+    picked = sweep_sample(len(graphs), sample)
+    started = time.perf_counter()
+    trials, expect = [], None
+    with BatchSweep([graphs[i] for i in picked], device) as sweep:
+        for shape in SWEEP_SHAPES:
+            if trials and time.perf_counter() - started > budget_seconds:
+                break
+            try:
+                sweep.run(**shape)
+                status = sweep.run(**shape)
+                tables = sweep.layer_tables()
+            except native.NativeError:
+                trials.append({"plan": shape, "seconds": None})
+                continue
+            if expect is None:
+                expect = tables
+            ok = status["complete_instances"] == status["instances"] and not status["fatal"] and tables == expect
+            trials.append({"plan": shape, "seconds": status["device_seconds"] if ok else None})
+    choice = pick(trials) if trials else {}
+    if use_cache:
+        entries = load_cache(path)
+        entries[key] = {"shape": choice, "trials": trials, "sample": picked}
+        store_cache(path, entries)
+    return {"shape": choice, "source": "pilot", "trials": trials, "sample": picked}

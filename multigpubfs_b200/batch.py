@@ -16,12 +16,21 @@ import csv
 import ctypes as C
 import hashlib
 import json
+from itertools import chain
 from pathlib import Path
 
 import numpy as np
 
 from . import native
 from .graph_definition import GraphDefinition
+
+
+_DESC_DTYPE = np.dtype({
+    "names": [name for name, _ in native.GraphDesc._fields_],
+    "formats": [np.uint64 if issubclass(t, C._Pointer) or t is C.c_uint64 else np.uint32
+                for _, t in native.GraphDesc._fields_],
+    "offsets": [getattr(native.GraphDesc, name).offset for name, _ in native.GraphDesc._fields_],
+    "itemsize": C.sizeof(native.GraphDesc)})
 
 
 class BatchSweep:
@@ -37,27 +46,25 @@ class BatchSweep:
             raise ValueError("BATCH_ARGUMENT: no instances")
         if any(g["action"]["kind"] != "permutation" for g in self.graphs):
             raise ValueError("BATCH_REQUIRES_PERMUTATION_ACTION")
-        degree = [len(g["start"]) for g in self.graphs]
-        gens = [len(g["action"]["generators"]) for g in self.graphs]
-        starts = np.ascontiguousarray(np.concatenate([np.asarray(g["start"], dtype=np.int64) for g in self.graphs]))
-        perms = np.ascontiguousarray(np.concatenate(
-            [np.asarray(g["action"]["generators"], dtype=np.int64).ravel() for g in self.graphs]))
+        degree = np.fromiter((len(g["start"]) for g in self.graphs), dtype=np.int64, count=n)
+        gens = np.fromiter((len(g["action"]["generators"]) for g in self.graphs), dtype=np.int64, count=n)
+        starts = np.fromiter(chain.from_iterable(g["start"] for g in self.graphs), dtype=np.int64,
+                             count=int(degree.sum()))
+        perms = np.fromiter(chain.from_iterable(chain.from_iterable(g["action"]["generators"]) for g in self.graphs),
+                            dtype=np.int64, count=int((degree * gens).sum()))
         if perms.size and (perms.min() < 0 or perms.max() > 0xFFFFFFFF):
             raise ValueError("GRAPH_PERMUTATION_GENERATOR")
         perms = perms.astype(np.uint32)
         self._keep = [starts, perms]
+        # The descriptor array is filled column-wise through a numpy view with
+        # the ctypes structure's field offsets.
         descs = (native.GraphDesc * n)()
-        s_off = p_off = 0
-        for k in range(n):
-            d = descs[k]
-            d.kind = 0
-            d.elements = d.rows = degree[k]
-            d.cols = 1
-            d.generators = gens[k]
-            d.permutations = C.cast(perms.ctypes.data + 4 * p_off, C.POINTER(C.c_uint32))
-            d.start = C.cast(starts.ctypes.data + 8 * s_off, C.POINTER(C.c_int64))
-            s_off += degree[k]
-            p_off += degree[k] * gens[k]
+        view = np.frombuffer(descs, dtype=_DESC_DTYPE, count=n)
+        view["elements"] = view["rows"] = degree
+        view["cols"] = 1
+        view["generators"] = gens
+        view["permutations"] = perms.ctypes.data + 4 * (np.cumsum(degree * gens) - degree * gens)
+        view["start"] = starts.ctypes.data + 8 * (np.cumsum(degree) - degree)
         handle = C.c_void_p()
         err = C.create_string_buffer(512)
         rc = self.lib.mgbfs2_batch_create(descs, n, device, C.byref(handle), err, len(err))
@@ -84,11 +91,13 @@ class BatchSweep:
         self.close()
 
     def run(self, *, capacities=None, memory_bytes=None, max_depth=None, host_loop=False, graph_loop=False,
-            blocks_per_sm=None) -> dict:
+            blocks_per_sm=None, tile_entries=None) -> dict:
         """Runs every instance to completion.  Each wave is one persistent
         cooperative launch by default; `host_loop` launches every layer step
         from the host (one sync per layer, e.g. for a profiler) and
-        `graph_loop` runs the steps as a CUDA-graph WHILE loop."""
+        `graph_loop` runs the steps as a CUDA-graph WHILE loop.
+        `blocks_per_sm` and `tile_entries` (256, 512 or 1024 frontier entries
+        per tile) are speed-only shapes; autotune.choose_sweep_shape picks them."""
         if host_loop and graph_loop:
             raise ValueError("host_loop and graph_loop are exclusive")
         opts = native.BatchOptions()
@@ -96,6 +105,7 @@ class BatchSweep:
         opts.host_loop = 1 if host_loop else (2 if graph_loop else 0)
         opts.memory_bytes = memory_bytes or 0
         opts.blocks_per_sm = blocks_per_sm or 0
+        opts.tile_entries = tile_entries or 0
         keep = None
         if capacities is not None:
             if len(capacities) != self.count:

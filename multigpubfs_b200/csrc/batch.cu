@@ -656,20 +656,27 @@ static int validate_instance(const mgbfs2_graph_desc& d, Batch::Instance* out, s
   in.gens = d.generators;
   in.orbit = factorial(n);
   in.begin.assign(1, 0);
-  std::map<std::vector<uint32_t>, uint32_t> index;
+  // A generator of at most 15 points is one 60-bit word (4 bits per image), so
+  // finding a generator's inverse among them is a word comparison.
+  std::vector<uint64_t> words(in.gens);
   for (uint32_t k = 0; k < in.gens; ++k) {
-    std::vector<uint32_t> g(d.permutations + static_cast<size_t>(k) * n, d.permutations + static_cast<size_t>(k + 1) * n);
-    std::vector<uint8_t> seen(n, 0);
-    for (uint32_t v : g) {
-      if (v >= n || seen[v]) { *why = "GRAPH_PERMUTATION_GENERATOR"; return MGBFS2_INVALID_ARGUMENT; }
-      seen[v] = 1;
+    const uint32_t* g = d.permutations + static_cast<size_t>(k) * n;
+    uint32_t seen = 0;
+    uint64_t w = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t v = g[i];
+      if (v >= n || (seen >> v) & 1u) { *why = "GRAPH_PERMUTATION_GENERATOR"; return MGBFS2_INVALID_ARGUMENT; }
+      seen |= 1u << v;
+      w |= static_cast<uint64_t>(v) << (4 * i);
     }
-    if (!index.count(g)) index[g] = k;
-    std::map<int, uint64_t> groups;
-    for (uint32_t i = 0; i < n; ++i) groups[static_cast<int>(g[i]) - static_cast<int>(i)] |= 15ull << (4 * i);
-    for (auto& kv : groups) {
-      const int shift = kv.first * 4;
-      in.terms.push_back(Term{kv.second, shift > 0 ? static_cast<uint32_t>(shift) : 0u,
+    words[k] = w;
+    // One term per displacement g[i] - i, in ascending displacement order.
+    uint64_t masks[2 * 15 + 1] = {};
+    for (uint32_t i = 0; i < n; ++i) masks[static_cast<int>(g[i]) - static_cast<int>(i) + 15] |= 15ull << (4 * i);
+    for (int disp = -15; disp <= 15; ++disp) {
+      if (!masks[disp + 15]) continue;
+      const int shift = disp * 4;
+      in.terms.push_back(Term{masks[disp + 15], shift > 0 ? static_cast<uint32_t>(shift) : 0u,
                               shift < 0 ? static_cast<uint32_t>(-shift) : 0u});
     }
     in.begin.push_back(static_cast<uint32_t>(in.terms.size()));
@@ -697,11 +704,14 @@ static int validate_instance(const mgbfs2_graph_desc& d, Batch::Instance* out, s
   in.inverse_closed = true;
   in.inverse.assign(in.gens, 0xffffffffu);
   for (uint32_t k = 0; k < in.gens; ++k) {
-    std::vector<uint32_t> inv(n);
-    for (uint32_t i = 0; i < n; ++i) inv[d.permutations[static_cast<size_t>(k) * n + i]] = i;
-    auto it = index.find(inv);
-    if (it == index.end()) in.inverse_closed = false;
-    else in.inverse[k] = it->second;
+    uint64_t inv = 0;
+    for (uint32_t i = 0; i < n; ++i)
+      inv |= static_cast<uint64_t>(i) << (4 * d.permutations[static_cast<size_t>(k) * n + i]);
+    // The first generator equal to the inverse, as the index lookup did.
+    uint32_t h = 0;
+    while (h < in.gens && words[h] != inv) ++h;
+    if (h == in.gens) in.inverse_closed = false;
+    else in.inverse[k] = h;
   }
   if (!in.inverse_closed) std::fill(in.inverse.begin(), in.inverse.end(), 0xffffffffu);
   *out = in;
@@ -742,7 +752,7 @@ static int batch_create(const mgbfs2_graph_desc* graphs, uint32_t count, int dev
 // Runs one wave (the instances in `ids`, with segment capacities `caps`, and
 // `pool` spare entries in each frontier buffer for layer redos).
 static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vector<uint64_t>& caps, uint64_t pool,
-                    uint32_t max_depth, uint32_t ppt, uint32_t tile_ppt, uint32_t loop, mgbfs2_batch_status* st,
+                    uint32_t max_depth, uint32_t blocks_per_sm, uint32_t tile_ppt, uint32_t loop, mgbfs2_batch_status* st,
                     double* kernel_seconds) {
   TraceRange range("batch.wave");
   const uint32_t W = static_cast<uint32_t>(ids.size());
@@ -837,10 +847,10 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   p.ctl = reinterpret_cast<BatchCtl*>(base + o_ctl);
   batch_seed<<<std::max<uint32_t>(1, (W + 255) / 256), 256, 0, b->stream>>>(p);
   ++st->kernel_launches;
-  // `ppt` here is the tuned blocks-per-SM of batch_expand (0 = the default);
-  // the carveout is sized for that many and the rest left as L1.
-  const int per_sm = size_carveout(reinterpret_cast<const void*>(batch_expand), 0,
-                                   ppt ? static_cast<int>(ppt) : kBatchBlocksPerSM, kBatchBlock);
+  // The carveout is sized for the tuned resident blocks of batch_expand (0 =
+  // the default) and the rest left as L1.
+  const int want = blocks_per_sm ? static_cast<int>(blocks_per_sm) : kBatchBlocksPerSM;
+  const int per_sm = size_carveout(reinterpret_cast<const void*>(batch_expand), 0, want, kBatchBlock);
   const uint32_t grid = static_cast<uint32_t>(per_sm * b->sm_count);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -850,7 +860,6 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   if (loop == kLoopPersistent) {
     // One cooperative launch; its grid must be co-resident, so it is sized by
     // the occupancy of batch_wave itself under the carveout set above.
-    const int want = ppt ? static_cast<int>(ppt) : kBatchBlocksPerSM;
     int wave_sm = size_carveout(reinterpret_cast<const void*>(batch_wave), 0, want, kBatchBlock);
     int resident = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, batch_wave, kBatchBlock, 0) != cudaSuccess) {
@@ -916,17 +925,24 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
   *kernel_seconds += ms * 1e-3;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  // Results.
+  // Results.  The instance records come first: their deepest layer bounds
+  // the columns of the layer and step tables that are read back (a strided
+  // copy of depth + 1 columns instead of max_depth).
   std::vector<BatchInst> done(W);
-  std::vector<unsigned long long> layers(static_cast<size_t>(W) * max_depth);
   BatchCtl hc{};
   MG_CHECK_BATCH(cudaMemcpyAsync(done.data(), p.inst, W * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream));
-  MG_CHECK_BATCH(cudaMemcpyAsync(layers.data(), p.layers, layers.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaMemcpyAsync(&hc, p.ctl, sizeof(hc), cudaMemcpyDeviceToHost, b->stream));
   std::vector<unsigned long long> stamps(static_cast<size_t>(max_steps) + 1, 0);
   MG_CHECK_BATCH(cudaMemcpyAsync(stamps.data(), p.stamps, stamps.size() * 8, cudaMemcpyDeviceToHost, b->stream));
-  std::vector<uint32_t> steps(static_cast<size_t>(W) * max_depth);
-  MG_CHECK_BATCH(cudaMemcpyAsync(steps.data(), p.layer_step, steps.size() * 4, cudaMemcpyDeviceToHost, b->stream));
+  MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
+  uint32_t cols = 1;
+  for (uint32_t k = 0; k < W; ++k) cols = std::max(cols, std::min(done[k].depth + 1, max_depth));
+  std::vector<unsigned long long> layers(static_cast<size_t>(W) * cols);
+  std::vector<uint32_t> steps(static_cast<size_t>(W) * cols);
+  MG_CHECK_BATCH(cudaMemcpy2DAsync(layers.data(), cols * 8ull, p.layers, max_depth * 8ull, cols * 8ull, W,
+                                   cudaMemcpyDeviceToHost, b->stream));
+  MG_CHECK_BATCH(cudaMemcpy2DAsync(steps.data(), cols * 4ull, p.layer_step, max_depth * 4ull, cols * 4ull, W,
+                                   cudaMemcpyDeviceToHost, b->stream));
   MG_CHECK_BATCH(cudaStreamSynchronize(b->stream));
   if (loop == kLoopGraph) st->kernel_launches += 3 * hc.step;
   st->layer_steps += hc.step;
@@ -938,13 +954,13 @@ static int run_wave(Batch* b, const std::vector<uint32_t>& ids, const std::vecto
     in.layers.clear();
     in.layer_seconds.clear();
     if (in.status == INST_DONE) {
-      for (uint32_t d = 0; d < max_depth && layers[static_cast<size_t>(k) * max_depth + d]; ++d) {
-        in.layers.push_back(layers[static_cast<size_t>(k) * max_depth + d]);
+      for (uint32_t d = 0; d < cols && layers[static_cast<size_t>(k) * cols + d]; ++d) {
+        in.layers.push_back(layers[static_cast<size_t>(k) * cols + d]);
         // Layer d >= 1 came from the wave's step t (shared by the wave's
         // instances, stamped at its end); depth 0 is the seed.
         double dt = 0.0;
         if (d) {
-          const uint32_t t = steps[static_cast<size_t>(k) * max_depth + d];
+          const uint32_t t = steps[static_cast<size_t>(k) * cols + d];
           if (t < max_steps && stamps[t + 1] > stamps[t]) dt = (stamps[t + 1] - stamps[t]) * 1e-9;
         }
         in.layer_seconds.push_back(dt);
@@ -983,7 +999,7 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
   mgbfs2_batch_options o{};
   if (options) o = *options;
   const uint32_t max_depth = o.max_depth ? o.max_depth : 1024;
-  const uint32_t ppt = o.blocks_per_sm;
+  const uint32_t blocks_per_sm = o.blocks_per_sm;
   const uint32_t loop = o.host_loop;
   if (loop > kLoopGraph) return MGBFS2_INVALID_ARGUMENT;
   const uint32_t tile = o.tile_entries ? o.tile_entries : kBatchTile;
@@ -1044,7 +1060,7 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
     // released its bit counts again), so its redo segments rarely sum to more
     // than twice its orbit; a pool that runs out falls back to the rerun.
     const uint64_t pool = predicted && short_by && budget > used ? std::min((budget - used) / 16, 2 * orbits) : 0;
-    rc = run_wave(b, wave, caps, pool, max_depth, ppt, tile_ppt, loop, &st, &kernel_seconds);
+    rc = run_wave(b, wave, caps, pool, max_depth, blocks_per_sm, tile_ppt, loop, &st, &kernel_seconds);
     ++st.waves;
     for (uint32_t i : wave) {
       if (b->inst[i].status == INST_OVERFLOW) {

@@ -118,6 +118,7 @@ struct Graph {
   uint64_t learned_peak = 0;  // learned plan: predicted largest layer (pre-sizes the frontier buffers)
   uint32_t group_chunk = 4096;  // plan shape: parents per grouped work item
   int blocks_per_sm = 0;        // plan shape: resident layer-kernel blocks per SM, 0 = defaults
+  uint32_t parents_per_thread = 0;  // plan shape: fused layers' states per thread, 0 = by generators
   int want_blocks(int kernel_default) const { return blocks_per_sm ? blocks_per_sm : kernel_default; }
   QuotientSlots quotient_slots(uint64_t slots) const;
   Control* host_control = nullptr;
@@ -172,6 +173,7 @@ struct Graph {
   int write_checkpoint(const char* path);
   int read_checkpoint(const char* path);
   int frontier_words(uint64_t* out, size_t capacity, size_t* count);
+  int table_probe_mean(double* mean, uint64_t* keys);
 
   // Results.
   std::vector<uint64_t> layer_sizes;

@@ -15,8 +15,10 @@ namespace mgbfs2 {
 
 
 constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
-// The quotient-hash kernel stages half as many (16 KiB), so six blocks fit per
-// SM for more loads in flight on the random table reads.
+// The quotient-hash kernel runs six blocks per SM (its registers allow six)
+// with a 16 KB stage, so that 6 x 17 KB stays in the 132 KB shared-memory
+// configuration and leaves about 100 KB of L1 (a 32 KB stage pushed it to the
+// 228 KB configuration, and the BFS ran 1.3x slower).
 constexpr uint32_t kOutCapHashQ = 2048;
 constexpr int kHashQBlocksPerSM = 6;
 constexpr uint32_t kBlock = 256;
@@ -212,6 +214,10 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
     const uint32_t lane = lane_id();
     const uint32_t tile = blockDim.x * p.ppt;
     const unsigned long long tiles = (count + tile - 1) / tile;
+    // When a whole tile's winners fit the stage (tile x generators), the
+    // block flushes once per tile and skips the room check (two barriers)
+    // after every generator.
+    const bool one_flush = tile * p.gens <= out_cap;
     for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
       const unsigned long long base = t * tile;
       uint64_t par[4];
@@ -290,7 +296,7 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
             }
           }
         }
-        if (g + 1 < p.gens) {
+        if (g + 1 < p.gens && !one_flush) {
           __syncthreads();
           const uint32_t pending = out_count;
           __syncthreads();

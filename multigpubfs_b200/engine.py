@@ -93,7 +93,7 @@ class NativeGraph:
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
              planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True, host_loop=False,
              full_rank=False, wide_slots=False, hash_load_percent=None, predicted_states=None,
-             predicted_peak=None, group_chunk=None, blocks_per_sm=None) -> dict:
+             predicted_peak=None, group_chunk=None, blocks_per_sm=None, parents_per_thread=None) -> dict:
         """Plans the run (mgbfs2_plan).  planner="learned" needs
         `predicted_states` (and optionally `predicted_peak`), e.g. from
         planner.predict_graph."""
@@ -102,6 +102,7 @@ class NativeGraph:
         req.predicted_peak = int(predicted_peak or 0)
         req.group_chunk = int(group_chunk or 0)
         req.blocks_per_sm = int(blocks_per_sm or 0)
+        req.parents_per_thread = int(parents_per_thread or 0)
         req.options = ((0 if parent_skip else native.OPTION_NO_PARENT_SKIP) |
                        (native.OPTION_HOST_LOOP if host_loop else 0) | (native.OPTION_FULL_RANK if full_rank else 0) |
                        (native.OPTION_WIDE_SLOTS if wide_slots else 0))
@@ -141,6 +142,31 @@ class NativeGraph:
                          sizes, seconds, status.states, status.successors, status.bfs_seconds,
                          status.kernel_launches, status.redo_layers, status.peak_device_bytes,
                          status.device_seconds, status.kernel_seconds, status.visited_tests, names)
+
+    def table_probes(self):
+        """(mean probes per stored key, keys) of the all-visited hash after a run."""
+        mean, keys = C.c_double(), C.c_uint64()
+        native.check(self.lib.mgbfs2_table_probes(self.handle, C.byref(mean), C.byref(keys)), "mgbfs2_table_probes")
+        return float(mean.value), int(keys.value)
+
+    def checkpoint(self, path):
+        """Writes the BFS state after run() (mgbfs2_checkpoint_write)."""
+        native.check(self.lib.mgbfs2_checkpoint_write(self.handle, str(path).encode()), "mgbfs2_checkpoint_write")
+
+    def resume(self, path):
+        """Loads a checkpoint into this planned handle; the next run() goes on
+        from its depth (mgbfs2_checkpoint_resume)."""
+        native.check(self.lib.mgbfs2_checkpoint_resume(self.handle, str(path).encode()), "mgbfs2_checkpoint_resume")
+
+    def frontier_words(self):
+        """The deepest layer's packed states (numpy uint64), tags removed."""
+        import numpy as np
+        count = C.c_size_t()
+        native.check(self.lib.mgbfs2_frontier_words(self.handle, None, 0, C.byref(count)), "mgbfs2_frontier_words")
+        out = np.zeros(max(count.value, 1), dtype=np.uint64)
+        native.check(self.lib.mgbfs2_frontier_words(self.handle, out.ctypes.data, out.size, C.byref(count)),
+                     "mgbfs2_frontier_words")
+        return out[:count.value]
 
     def layer_table(self):
         count = C.c_size_t()

@@ -51,7 +51,8 @@ class PlanRequest(C.Structure):
                 ("reserve_bytes", C.c_uint64), ("shards", C.c_uint32), ("block", C.c_uint32),
                 ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64),
                 ("options", C.c_uint32), ("hash_load_percent", C.c_uint32), ("predicted_states", C.c_uint64),
-                ("predicted_peak", C.c_uint64), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+                ("predicted_peak", C.c_uint64), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("parents_per_thread", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 OPTION_NO_PARENT_SKIP = 1
@@ -68,10 +69,10 @@ class PlanInfo(C.Structure):
                 ("block", C.c_uint32), ("inverse_closed", C.c_uint32), ("planner", C.c_uint32),
                 ("parent_skip", C.c_uint32), ("bucket_prefix", C.c_uint32), ("table_slot_bytes", C.c_uint32),
                 ("hash_load_percent", C.c_uint32), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("rank_components", C.c_uint32), ("reserved", C.c_uint32)]
+                ("rank_components", C.c_uint32), ("parents_per_thread", C.c_uint32)]
 
     def to_dict(self):
-        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
         d["visited"] = VISITED_NAMES.get(self.visited, self.visited)
         d["dedup"] = DEDUP_NAMES.get(self.dedup, self.dedup)
         d["planner"] = {0: "plain", 1: "learned"}.get(self.planner, self.planner)
@@ -119,6 +120,7 @@ _SIGNATURES = {
     "mgbfs2_status_string": (C.c_char_p, [C.c_int]),
     "mgbfs2_destroy": (None, [C.c_void_p]),
     "mgbfs2_trim_memory": (C.c_int, [C.c_int]),
+    "mgbfs2_table_probes": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "mgbfs2_checkpoint_write": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mgbfs2_checkpoint_resume": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mgbfs2_frontier_words": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),

@@ -63,9 +63,30 @@ def test_shape_candidates_vary_the_kept_path_only():
     assert {"visited": "bitmap", "dedup": "grouped", "group_chunk": 2048, "blocks_per_sm": 6} in grouped
     assert all(set(p) <= {"visited", "dedup", "group_chunk", "blocks_per_sm"} for p in grouped)
     hashed = autotune.shape_candidates(dict(autotune.DEFAULT), {"visited": "hash", "dedup": "atomic"})
-    assert hashed[0] == autotune.DEFAULT and {"visited": "auto", "dedup": "auto", "hash_load_percent": 90} in hashed
+    assert hashed[0] == autotune.DEFAULT and {"visited": "auto", "dedup": "auto", "hash_load_percent": 70} in hashed
+    assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 2} in hashed
+    quotient = autotune.shape_candidates(dict(autotune.DEFAULT),
+                                         {"visited": "hash", "dedup": "atomic", "parents_per_thread": 2})
+    assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 4} in quotient
     bucket = autotune.shape_candidates({"visited": "bitmap", "dedup": "bucket", "shards": 1},
                                        {"visited": "bitmap", "dedup": "bucket"})
     assert [p.get("bucket_margin") for p in bucket] == [None, 1024, 16384]
     assert autotune.shape_candidates(dict(autotune.DEFAULT), {"visited": "hash3", "dedup": "atomic"}) == \
         [autotune.DEFAULT]
+
+
+def test_sweep_sample_spreads_over_the_sweep():
+    assert autotune.sweep_sample(10) == list(range(10))
+    picked = autotune.sweep_sample(512, 64)
+    assert len(picked) == 64 and picked[0] == 0 and picked[-1] == 504
+    assert all(b - a == 8 for a, b in zip(picked, picked[1:]))
+    assert autotune.SWEEP_SHAPES[0] == {}   # the default shape is the first trial
+
+
+def test_sweep_cache_key_depends_on_every_instance():
+    from oracle import graph_oracle as G
+    a = [G.sweep_instance(i, False) for i in range(4)]
+    b = a[:3] + [G.sweep_instance(9, False)]
+    assert autotune.sweep_cache_key(a, "B200", "x") == autotune.sweep_cache_key(list(a), "B200", "x")
+    assert autotune.sweep_cache_key(a, "B200", "x") != autotune.sweep_cache_key(b, "B200", "x")
+    assert autotune.sweep_cache_key(a, "B200", "x").startswith("sweep:")

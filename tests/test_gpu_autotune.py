@@ -48,3 +48,23 @@ def test_run_graph_with_autotune_is_exact(tmp_path, monkeypatch, lrx_layers):
     assert report2["autotune"]["source"] == "cache" and report2["layer_sizes"] == lrx_layers[11]
     small = run_graph(_lrx(8), tmp_path / "out3", autotune=True)
     assert small["autotune"]["source"] == "size" and small["layer_sizes"] == lrx_layers[8]
+
+
+def test_sweep_shape_pilots_stay_exact_then_cache(tmp_path):
+    from multigpubfs_b200 import autotune, workloads
+    from multigpubfs_b200.batch import BatchSweep
+    graphs = workloads.sweep(48)
+    cache = tmp_path / "tune.json"
+    got = autotune.choose_sweep_shape(graphs, 0, sample=16, cache=cache)
+    assert got["source"] == "pilot" and len(got["sample"]) == 16
+    assert [t["plan"] for t in got["trials"]] == autotune.SWEEP_SHAPES
+    assert all(t["seconds"] is not None and t["seconds"] > 0 for t in got["trials"]), got["trials"]
+    assert got["shape"] in autotune.SWEEP_SHAPES
+    again = autotune.choose_sweep_shape(graphs, 0, sample=16, cache=cache)
+    assert again["source"] == "cache" and again["shape"] == got["shape"]
+    with BatchSweep(graphs, 0) as sweep:
+        sweep.run()
+        plain = sweep.layer_tables()
+        for shape in autotune.SWEEP_SHAPES[1:]:
+            sweep.run(**shape)
+            assert sweep.layer_tables() == plain, shape
