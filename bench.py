@@ -21,6 +21,9 @@ Workloads (one step = one pass of the workload):
   gathered tables.
 * ``planner-s12``: learned vs plain planner on 128 S12 instances and on the
   held-out sweep; tables checked against the oracle's fixtures.
+* ``s13-lrx-sharded``: the S13 LRX BFS split over the ranks by state ownership
+  (an NCCL all-to-all of routed children per layer chunk; strong scaling),
+  checked against the reference's table.
 
 Keys of the line: ``value`` is successors/s with inputs resident, timed with
 CUDA events on the launching stream over the K steps; ``e2e`` is the same
@@ -76,7 +79,7 @@ WORKLOADS = {
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
 }
-BATCHED = ("sweep512", "planner-s12")
+BATCHED = ("sweep512", "planner-s12", "s13-lrx-sharded")
 
 # Bounded CPU samples (about 10-30 s of C-oracle work on a 16-core host): the
 # layers run of each workload's sample; s11-lrx-hash runs whole, and sweep512
@@ -194,6 +197,8 @@ def cpu_sample(name, threads=None):
     from multigpubfs_b200 import workloads
     threads = threads or P.default_threads()
     P.library()
+    if name == "s13-lrx-sharded":
+        name = "s13-lrx"  # the same BFS, split or not
     t = time.perf_counter()
     succ = states = 0
     if name in WORKLOADS:
@@ -231,6 +236,8 @@ def workload_desc(name):
     if name == "sweep512":
         return ("batched sweep: 512 instances (256 seeds x directed / inverse-closed), n in {7,8,9,10}, 2-3 seeded "
                 "random generators, exact per-instance Lehmer bitmaps")
+    if name == "s13-lrx-sharded":
+        return "S13 LRX full BFS (6,227,020,800 states) split over the ranks by state ownership"
     return "learned vs plain planner: 128 S12 instances (2-4 random generators plus inverses), whole device"
 
 
@@ -629,6 +636,103 @@ def bench_single(args, rank, world, local):
     return 0
 
 
+def bench_sharded(args, rank, world, local):
+    """One S13 LRX BFS split over the ranks by state ownership
+    (multigpubfs_b200.sharded): each rank owns a slice of the bitmap, children
+    are routed to their owners and exchanged with an NCCL all-to-all per layer
+    chunk.  One rank (no torchrun) runs the same loop over a one-rank NCCL
+    group.  Strong scaling: the total work is one BFS whatever N is."""
+    import socket
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from multigpubfs_b200 import GraphDefinition, sharded
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world == 1 and "MASTER_ADDR" not in os.environ:
+        with socket.socket() as sock:
+            sock.bind(("127.0.0.1", 0))
+            port = sock.getsockname()[1]
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK="0", WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    n, gens = 13, lrx(13)
+    graph = GraphDefinition.permutation(gens, list(range(n)))
+    expect = expected_layers("s13-lrx", n)
+    chunk = 1 << 26
+
+    def barrier():
+        dist.barrier()
+        torch.cuda.synchronize()
+
+    shard = sharded.DeviceShard(graph, rank, world, dev, chunk_parents=chunk)
+    bfs = sharded.ShardedBfs([shard], sharded.DistExchange(None, dev))
+    for _ in range(args.warmup):
+        shard.reset()
+        assert bfs.run() == expect, "layer table mismatch in warm-up"
+    barrier()
+    shard.launches = 0
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tables = []
+    with ClockSampler(gpu_index(local)) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            shard.reset()
+            tables.append(bfs.run())
+        stop.record()
+        barrier()
+    device_s = start.elapsed_time(stop) * 1e-3
+    launches = shard.launches
+    assert all(t == expect for t in tables), "layer table mismatch in a timed run"
+    del bfs, shard
+    torch.cuda.empty_cache()
+
+    # e2e: shards built from the host graph every step.
+    e2e = []
+    for i in range(args.steps + 1):
+        barrier()
+        t0 = time.perf_counter()
+        s = sharded.DeviceShard(graph, rank, world, dev, chunk_parents=chunk)
+        got = sharded.ShardedBfs([s], sharded.DistExchange(None, dev)).run()
+        del s
+        torch.cuda.synchronize()
+        if i:
+            e2e.append(time.perf_counter() - t0)
+        assert got == expect
+    t = torch.tensor([device_s, sum(e2e) / len(e2e)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device_max, e2e_max = float(t[0].item()), float(t[1].item())
+    if rank == 0:
+        states = sum(expect)
+        succ = len(gens) * states
+        geo = sharded.geometry(n, world)
+        line = {
+            "metric": "successors/s", "value": succ * args.steps / device_max, "unit": "successors/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": device_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "S13 LRX full BFS (6,227,020,800 states) split over the ranks by state "
+                                   "ownership: prefix blocks of two Lehmer digits, block s on rank s mod N",
+                       "parallelism": f"owner-partitioned bitmap over {world} rank(s), NCCL all-to-all per chunk",
+                       "slice_bits_per_rank": geo.slice_bits, "chunk_parents": chunk,
+                       "states_per_bfs": states, "successors_per_bfs": succ,
+                       "l2": "bitmap slices and frontiers larger than L2 at N <= 4"},
+            "settled_states_per_s": states * args.steps / device_max,
+            "e2e": {"value": succ / e2e_max, "unit": "successors/s", "h2d_bytes_per_step": 8 * n + 4 * n * 3,
+                    "d2h_bytes_per_step": 8 * len(expect)},
+            "roofline": roofline(16 * states + 32 * succ, device_max / args.steps,
+                                 "count_lehmer + route_lehmer + accept_lehmer (owner-partitioned), timed as the "
+                                 "whole step including the exchange"),
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_sample("s13-lrx")
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -655,6 +759,8 @@ def main():
         if world > 1 and rank != 0:
             return 0
         return bench_planner(args, local)
+    if args.workload == "s13-lrx-sharded":
+        return bench_sharded(args, rank, world, local)
     return bench_single(args, rank, world, local)
 
 

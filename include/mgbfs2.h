@@ -334,6 +334,8 @@ MGBFS2_API int mgbfs2_bucket_keys(const uint64_t* keys, uint64_t count, uint32_t
  * receives their exact number (bit 0 of *error when it exceeds the capacity).
  * All temporaries live in `scratch` (device, >= mgbfs2_expand_layer_scratch_bytes
  * bytes, 256-byte aligned); asynchronous on `stream`; allocates nothing.
+ * `frontier` must be 16-byte aligned (MGBFS2_INVALID_ARGUMENT otherwise):
+ * parents are read two at a time.
  * Replaces the route + accept pair mgbfs_bitmap_route / mgbfs_bitmap_accept,
  * cuda/permutation_bitmap.cu:27-48 and :105-133. */
 MGBFS2_API int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
@@ -362,6 +364,58 @@ MGBFS2_API int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t gener
                                                  uint64_t count, uint64_t* bitmap, uint64_t* next,
                                                  uint64_t next_capacity, uint64_t* next_count, uint32_t* error,
                                                  void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Owner-partitioned layers: one BFS over several ranks (one per GPU).      */
+/* Replaces the reference's owner route / exchange / accept split
+ * (cuda/permutation_bitmap.cu:27-48 and :105-205 with world/owner arguments,
+ * the grouped send/recv of crates/mgbfs-runtime/src/generic_distributed_native.rs:199-285).
+ * The partition differs from the reference's rank mod world: prefix block s
+ * (the states whose first `prefix` Lehmer digits give s; (degree-prefix)!
+ * consecutive ranks) belongs to rank s mod world, which stores it as local
+ * block s / world, so a rank's slice is blocks_per_owner * (degree-prefix)!
+ * bits and the owner of a child costs `prefix` digit steps, not a full rank.
+ * Packed states of `degree` <= 16 distinct 4-bit codes, as in the layer call
+ * above.  When the generator set holds inverse pairs and the bits fit
+ * (4 * degree + bits of the generator count <= 64), every routed child carries
+ * the number g + 1 of its generator in the bits from 4 * degree up, and route
+ * skips each parent's edge back to its own parent; the tags travel with the
+ * words and are ignored by the claim. */
+
+/* The partition of `degree`-symbol states over `world` ranks: prefix digits,
+ * blocks per owner and bits per slice.  MGBFS2_UNSUPPORTED when
+ * world * blocks_per_owner exceeds 256 buckets.  Host only. */
+MGBFS2_API int mgbfs2_shard_geometry(uint32_t degree, uint32_t world, uint32_t* prefix, uint32_t* blocks_per_owner,
+                                     uint64_t* slice_bits);
+
+/* Device scratch bytes each of the two calls below needs (256-byte aligned). */
+MGBFS2_API uint64_t mgbfs2_shard_scratch_bytes(void);
+
+/* Sending side of a layer: expands `frontier` and writes every child (packed
+ * word) to out[], owner-major and block-minor, sized exactly by a counting pass;
+ * out_capacity >= count * generators (MGBFS2_CAPACITY otherwise).
+ * bucket_counts (device, world * blocks_per_owner u64) receives the count per
+ * (owner, local block): owner w's words are the contiguous run of its
+ * blocks_per_owner buckets, ready for an all-to-all with these split sizes.
+ * `frontier` must be 16-byte aligned (a chunk of a frontier starts at an even
+ * entry).  Asynchronous on `stream`. */
+MGBFS2_API int mgbfs2_shard_route(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                                  const uint64_t* frontier, uint64_t count, uint32_t world, uint64_t* out,
+                                  uint64_t out_capacity, uint64_t* bucket_counts, uint32_t* error, void* scratch,
+                                  uint64_t scratch_bytes, void* stream);
+
+/* Receiving side: `incoming` holds the words every source rank sent to
+ * `owner`, in source order; incoming_counts (device, world * blocks_per_owner
+ * u64, source-major) holds each source's bucket_counts row for this owner.
+ * Each word is claimed in this rank's slice (bit = local block *
+ * (degree-prefix)! + rank within the block); winners go to next[], *next_count
+ * (device) receives their number.  A word whose prefix block this rank does not
+ * own is not claimed and raises bit 7 (BAD_REFERENCE) of *error.
+ * Asynchronous on `stream`. */
+MGBFS2_API int mgbfs2_shard_accept(uint32_t degree, uint32_t world, uint32_t owner, const uint64_t* incoming,
+                                   const uint64_t* incoming_counts, uint64_t* bitmap_slice, uint64_t* next,
+                                   uint64_t next_capacity, uint64_t* next_count, uint32_t* error, void* scratch,
+                                   uint64_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched sweep: many BFS instances, each wave one persistent launch.       */

@@ -40,6 +40,9 @@ constexpr uint32_t kMaxEntries = 12;                 // staged successors per th
 constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kStageCap = kBlock * kMaxEntries;  // 3072
 constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per accept work item
+constexpr unsigned long long kFactorial[17] = {1ull, 1ull, 2ull, 6ull, 24ull, 120ull, 720ull, 5040ull, 40320ull,
+                                               362880ull, 3628800ull, 39916800ull, 479001600ull, 6227020800ull,
+                                               87178291200ull, 1307674368000ull, 20922789888000ull};
 
 struct RouteParams {
   const unsigned long long* frontier;
@@ -58,6 +61,10 @@ struct RouteParams {
   // slot, (mix64(key) & table_mask) >> region_shift.
   unsigned long long table_mask, key_mask;
   uint32_t region_shift, pad1;
+  // Owner routing across ranks (owners > 1): prefix block s belongs to rank
+  // s mod owners and goes to bucket (s mod owners) * owner_blocks + s / owners,
+  // so each rank's buckets are contiguous (owner-major, block-minor).
+  uint32_t owners, owner_blocks;
 };
 
 struct AcceptParams {
@@ -74,6 +81,10 @@ struct AcceptParams {
   unsigned long long* table;
   unsigned long long table_mask, key_mask;
   uint32_t probe_limit, pad1;
+  // Owner slices (owners > 1): bucket b holds states of this rank's local
+  // block b / owners, i.e. of prefix block (b / owners) * owners + owner, and
+  // `bitmap` is the rank's slice: bit = local block * (N-K)! + rank in block.
+  uint32_t owners, owner;
 };
 
 // Shard of a successor: its rank range for the Lehmer bitmap, or (N = 0) the
@@ -110,7 +121,8 @@ __device__ __forceinline__ uint32_t route_shard(const RouteParams& p, uint64_t c
   if constexpr (N == 0) {
     return static_cast<uint32_t>((mix64(c & p.key_mask) & p.table_mask) >> p.region_shift);
   } else {
-    return prefix_shard<N, K>(c);
+    const uint32_t s = prefix_shard<N, K>(c);
+    return p.owners > 1 ? (s % p.owners) * p.owner_blocks + s / p.owners : s;
   }
 }
 
@@ -292,7 +304,7 @@ __global__ void __launch_bounds__(kBlock) count_lehmer(RouteParams p) {
     const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(w >> p.gen_shift) : 0u;
     const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
     for (uint32_t g = 0; g < p.gens; ++g)
-      if (g != skip) atomicAdd(&hist[prefix_shard<N, K>(apply_terms(w, terms, tbegin[g], tbegin[g + 1]))], 1u);
+      if (g != skip) atomicAdd(&hist[route_shard<N, K>(p, apply_terms(w, terms, tbegin[g], tbegin[g + 1]))], 1u);
   }
   __syncthreads();
   for (uint32_t s = threadIdx.x; s < p.shards; s += blockDim.x)
@@ -337,6 +349,13 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
     const unsigned long long first = (item - item_prefix[s]) * kAcceptChunk;
     const uint32_t n = static_cast<uint32_t>(min(static_cast<unsigned long long>(kAcceptChunk), p.shard_count[s] - first));
     const unsigned long long* src = p.buckets + p.shard_begin[s] + first;
+    // Prefix block of the bucket's states and the offset of its bits: on one
+    // GPU the bucket is the block and its bits are its ranks; on an owner
+    // slice, local block j = s / owners holds prefix block j * owners + owner.
+    const bool sliced = p.owners > 1;
+    const uint32_t local = sliced ? s / p.owners : s;
+    const uint32_t block = sliced ? local * p.owners + p.owner : s;
+    const uint64_t shift = static_cast<uint64_t>(block - local) * kFactorial[N - K];
     for (uint32_t round = 0; round < n; round += 8 * kBlock) {
       unsigned long long w[8], old[8];
       uint64_t r[8];
@@ -345,12 +364,17 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
         const uint32_t i = round + k * kBlock + tid;
         w[k] = i < n ? src[i] : 0ull;
       }
+      bool bad = false;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = round + k * kBlock + tid;
-        r[k] = lehmer_rank4_in_shard<N, K>(w[k], s);
-        old[k] = i < n ? atomicOr(&p.bitmap[r[k] >> 6], 1ull << (r[k] & 63)) : ~0ull;
+        // A state routed to a rank that does not own it is never claimed.
+        const bool mine = !sliced || prefix_shard<N, K>(w[k]) == block;
+        bad = bad || (i < n && !mine);
+        r[k] = lehmer_rank4_in_shard<N, K>(w[k], block) - shift;
+        old[k] = i < n && mine ? atomicOr(&p.bitmap[r[k] >> 6], 1ull << (r[k] & 63)) : ~0ull;
       }
+      if (bad) raise_error(&p.control->error, ERR_BAD_REFERENCE);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const bool won = !(old[k] & (1ull << (r[k] & 63)));

@@ -23,6 +23,7 @@ enum : uint32_t {
   ERR_WAIT_LIMIT = 1u << 4,         // a bounded wait gave up
   ERR_ARENA_OVERFLOW = 1u << 5,     // wide-key arena capacity exceeded
   ERR_BAD_STATE = 1u << 6,          // malformed input state
+  ERR_BAD_REFERENCE = 1u << 7,      // a routed state reached a rank that does not own it
 };
 
 constexpr uint32_t kFullMask = 0xffffffffu;

@@ -135,11 +135,14 @@ uint32_t occupancy_grid(const void* fn, size_t smem, int device) {
 // the bucket region is 8 bytes per successor.
 constexpr uint64_t kMaxLayerSuccessors = (UINT64_MAX / 2) / sizeof(unsigned long long);
 
+// The route kernels read two parents at a time as one 16-byte load.
+bool frontier_aligned(const uint64_t* frontier) { return reinterpret_cast<uintptr_t>(frontier) % 16 == 0; }
+
 bool layer_arguments_ok(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
                         const uint64_t* frontier, uint64_t count, const uint64_t* bitmap, const uint64_t* next,
                         const uint64_t* next_count) {
   return degree >= 2 && degree <= 16 && generators && generators <= kLayerMaxGens && permutations_host && bitmap &&
-         next_count && (!count || (frontier && next));
+         next_count && (!count || (frontier && next && frontier_aligned(frontier)));
 }
 
 // The generator program of one layer call, as the kernels read it from scratch.
@@ -252,6 +255,208 @@ int expand_layer_into(uint32_t degree, uint32_t generators, const uint32_t* perm
 
 uint64_t expand_layer_scratch_bytes(uint64_t count, uint32_t generators) {
   return layer_layout(count * generators).total;
+}
+
+// ---------------------------------------------------------------------------
+// Owner-partitioned layers: one BFS whose Lehmer bitmap is split over `world`
+// ranks (one per GPU).  Prefix block s (the ranks sharing the first `prefix`
+// Lehmer digits, (n - prefix)! of them) belongs to rank s mod world, which
+// keeps it as its local block s / world: bit = (s / world) * (n - prefix)! +
+// the rank within the block.  A layer is route (every child to its owner's
+// buckets) -> an all-to-all of the buckets between the ranks (the caller's,
+// over NCCL) -> accept (each rank claims what it received in its slice).
+namespace {
+
+struct ShardGeometry {
+  uint32_t prefix = 0, blocks_per_owner = 0;
+  uint64_t blocks = 0, block_bits = 0, slice_bits = 0;
+};
+
+int shard_geometry(uint32_t degree, uint32_t world, ShardGeometry* g) {
+  if (degree < 2 || degree > 16 || world < 1) return MGBFS2_INVALID_ARGUMENT;
+  g->prefix = degree >= 4 ? 2u : 1u;
+  g->blocks = 1;
+  for (uint32_t i = degree - g->prefix + 1; i <= degree; ++i) g->blocks *= i;
+  g->blocks_per_owner = static_cast<uint32_t>((g->blocks + world - 1) / world);
+  // Buckets are owner-major, block-minor: world * blocks_per_owner of them,
+  // each an 8-bit bucket index in the route kernel.
+  if (static_cast<uint64_t>(world) * g->blocks_per_owner > kMaxShards) return MGBFS2_UNSUPPORTED;
+  g->block_bits = 1;
+  for (uint32_t i = 2; i <= degree - g->prefix; ++i) g->block_bits *= i;
+  g->slice_bits = g->blocks_per_owner * g->block_bits;
+  return MGBFS2_OK;
+}
+
+// Copies the route's exact bucket counts out and raises the caller's error bits.
+__global__ void publish_route(const Control* control, const unsigned long long* meta, uint32_t buckets,
+                              unsigned long long* bucket_counts, unsigned int* error) {
+  for (uint32_t b = threadIdx.x; b < buckets; b += blockDim.x) bucket_counts[b] = meta[2 * kMaxShards + b];
+  if (threadIdx.x == 0 && error && control->error) atomicOr(error, control->error);
+}
+
+// Receiving side: the incoming words are the sources' segments back to back
+// (source rank order); source r's segment holds its local blocks j in order,
+// counts[r * blocks + j] words each.  Accept bucket j * world + r (block-major,
+// so the resident blocks claim in one local block at a time) gets its range.
+__global__ void layout_incoming(const unsigned long long* counts, uint32_t world, uint32_t blocks,
+                                unsigned long long* meta) {
+  if (threadIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint32_t r = 0; r < world; ++r) {
+      for (uint32_t j = 0; j < blocks; ++j) {
+        const uint32_t b = j * world + r;
+        const unsigned long long c = counts[static_cast<size_t>(r) * blocks + j];
+        meta[b] = run;
+        meta[kMaxShards + b] = c;
+        meta[2 * kMaxShards + b] = c;
+        run += c;
+      }
+    }
+    meta[3 * kMaxShards] = 0;
+  }
+}
+
+// Parent-edge tags of the owner-partitioned path: a child carries the number
+// (g + 1) of the generator that produced it in the bits above its 4 * degree
+// code bits, and route skips, for each parent, the generator equal to the
+// inverse of its tag's, whose child is the parent's own parent (visited in an
+// earlier layer).  Replaces the term program's trailing "no skip" table and
+// returns the tag shift (0 = no tags: no inverse pairs, or no spare bits).
+uint32_t tag_parent_edges(uint32_t degree, uint32_t gens, const uint32_t* perms, std::vector<uint32_t>* begin) {
+  const uint32_t tag_bits = 32 - __builtin_clz(gens);
+  if (4 * degree + tag_bits > 64) return 0;
+  std::vector<uint32_t> inverse(gens, 0xffffffffu);
+  bool any = false;
+  std::vector<uint32_t> inv(degree);
+  for (uint32_t k = 0; k < gens; ++k) {
+    for (uint32_t i = 0; i < degree; ++i) inv[perms[static_cast<size_t>(k) * degree + i]] = i;
+    for (uint32_t h = 0; h < gens && inverse[k] == 0xffffffffu; ++h)
+      if (std::equal(inv.begin(), inv.end(), perms + static_cast<size_t>(h) * degree)) inverse[k] = h;
+    any = any || inverse[k] != 0xffffffffu;
+  }
+  if (!any) return 0;
+  std::copy(inverse.begin(), inverse.end(), begin->end() - gens);
+  return 4 * degree;
+}
+
+int stage_program(const LayerProgram& prog, unsigned char* scratch, const LayerLayout& l, cudaStream_t stream) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(scratch + l.control, 0, sizeof(Control), stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(scratch + l.meta, 0, (3 * kMaxShards + 1) * sizeof(unsigned long long), stream)) !=
+          cudaSuccess)
+    return cuda_status(e);
+  if (prog.terms.empty()) return MGBFS2_OK;
+  unsigned char* program = scratch + l.program;
+  if ((e = cudaMemcpyAsync(program, prog.terms.data(), prog.terms.size() * sizeof(Term), cudaMemcpyHostToDevice,
+                           stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(program + prog.terms.size() * sizeof(Term), prog.begin.data(),
+                           prog.begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+    return cuda_status(e);
+  return MGBFS2_OK;
+}
+
+}  // namespace
+
+int shard_route(uint32_t degree, uint32_t generators, const uint32_t* permutations_host, const uint64_t* frontier,
+                uint64_t count, uint32_t world, uint64_t* out, uint64_t out_capacity, uint64_t* bucket_counts,
+                uint32_t* error, unsigned char* scratch, uint64_t scratch_bytes, cudaStream_t stream) {
+  TraceRange range("shard.route");
+  ShardGeometry g;
+  if (int rc = shard_geometry(degree, world, &g)) return rc;
+  if (!generators || generators > kLayerMaxGens || !permutations_host || !bucket_counts || !scratch ||
+      (count && (!frontier || !out || !frontier_aligned(frontier))))
+    return MGBFS2_INVALID_ARGUMENT;
+  if (count > kMaxLayerSuccessors / generators) return MGBFS2_CAPACITY;
+  if (out_capacity < count * generators) return MGBFS2_CAPACITY;
+  const LayerLayout l = layer_layout(0);
+  if (scratch_bytes < l.total) return MGBFS2_CAPACITY;
+  LayerProgram prog;
+  if (!build_layer_program(degree, generators, permutations_host, &prog.terms, &prog.begin))
+    return MGBFS2_INVALID_ARGUMENT;
+  const uint32_t gen_shift = tag_parent_edges(degree, generators, permutations_host, &prog.begin);
+  prog.prefix = g.prefix;
+  if (!pick_layer_kernels(degree, g.prefix, &prog.kernels)) return MGBFS2_UNSUPPORTED;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (int rc = stage_program(prog, scratch, l, stream)) return rc;
+  Control* control = reinterpret_cast<Control*>(scratch + l.control);
+  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  Term* program = reinterpret_cast<Term*>(scratch + l.program);
+  const uint32_t buckets = world * g.blocks_per_owner;
+  if (count) {
+    RouteParams rp{};
+    rp.frontier = reinterpret_cast<const unsigned long long*>(frontier);
+    rp.count = count;
+    rp.terms = program;
+    rp.term_begin = reinterpret_cast<const uint32_t*>(program + prog.terms.size());
+    rp.gens = generators;
+    rp.total_terms = static_cast<uint32_t>(prog.terms.size());
+    rp.ppt = generators <= 3 ? 4 : (generators <= 6 ? 2 : 1);
+    rp.group = kMaxEntries / rp.ppt;
+    rp.gen_shift = gen_shift;
+    rp.shards = buckets;
+    rp.prefix = g.prefix;
+    rp.owners = world;
+    rp.owner_blocks = g.blocks_per_owner;
+    rp.buckets = reinterpret_cast<unsigned long long*>(out);
+    rp.shard_begin = meta;
+    rp.shard_cap = meta + kMaxShards;
+    rp.shard_count = meta + 2 * kMaxShards;
+    rp.control = control;
+    const LayerKernels& k = prog.kernels;
+    const size_t count_smem = kMaxShards * sizeof(uint32_t) + prog.bytes();
+    k.count<<<occupancy_grid(reinterpret_cast<const void*>(k.count), count_smem, device), kBlock, count_smem,
+              stream>>>(rp);
+    layout_shards<<<1, 32, 0, stream>>>(meta, buckets);
+    const size_t route_smem = sizeof(RouteSmem) + prog.bytes();
+    if ((e = cudaFuncSetAttribute(reinterpret_cast<const void*>(k.route), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(route_smem))) != cudaSuccess)
+      return cuda_status(e);
+    k.route<<<occupancy_grid(reinterpret_cast<const void*>(k.route), route_smem, device), kBlock, route_smem,
+              stream>>>(rp);
+  }
+  publish_route<<<1, kBlock, 0, stream>>>(control, meta, buckets, reinterpret_cast<unsigned long long*>(bucket_counts),
+                                          error);
+  return cuda_status(cudaGetLastError());
+}
+
+int shard_accept(uint32_t degree, uint32_t world, uint32_t owner, const uint64_t* incoming,
+                 const uint64_t* incoming_counts, uint64_t* bitmap_slice, uint64_t* next, uint64_t next_capacity,
+                 uint64_t* next_count, uint32_t* error, unsigned char* scratch, uint64_t scratch_bytes,
+                 cudaStream_t stream) {
+  TraceRange range("shard.accept");
+  ShardGeometry g;
+  if (int rc = shard_geometry(degree, world, &g)) return rc;
+  if (owner >= world || !incoming_counts || !bitmap_slice || !next_count || !scratch || !incoming || !next)
+    return MGBFS2_INVALID_ARGUMENT;
+  const LayerLayout l = layer_layout(0);
+  if (scratch_bytes < l.total) return MGBFS2_CAPACITY;
+  LayerKernels k{};
+  if (!pick_layer_kernels(degree, g.prefix, &k)) return MGBFS2_UNSUPPORTED;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (int rc = stage_program(LayerProgram{}, scratch, l, stream)) return rc;
+  Control* control = reinterpret_cast<Control*>(scratch + l.control);
+  unsigned long long* meta = reinterpret_cast<unsigned long long*>(scratch + l.meta);
+  layout_incoming<<<1, 32, 0, stream>>>(reinterpret_cast<const unsigned long long*>(incoming_counts), world,
+                                        g.blocks_per_owner, meta);
+  AcceptParams ap{};
+  ap.buckets = reinterpret_cast<const unsigned long long*>(incoming);
+  ap.shard_begin = meta;
+  ap.shard_count = meta + 2 * kMaxShards;
+  ap.shards = world * g.blocks_per_owner;
+  ap.bitmap = reinterpret_cast<unsigned long long*>(bitmap_slice);
+  ap.next = reinterpret_cast<unsigned long long*>(next);
+  ap.capacity = next_capacity;
+  ap.work = meta + 3 * kMaxShards;
+  ap.control = control;
+  ap.owners = world;
+  ap.owner = owner;
+  k.accept<<<occupancy_grid(reinterpret_cast<const void*>(k.accept), 0, device), kBlock, 0, stream>>>(ap);
+  publish_layer<<<1, 32, 0, stream>>>(control, reinterpret_cast<unsigned long long*>(next_count), error);
+  return cuda_status(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------
@@ -377,6 +582,35 @@ int mgbfs2_expand_layer_bitmap(uint32_t degree, uint32_t generators, const uint3
 }  // extern "C"
 
 extern "C" {
+
+int mgbfs2_shard_geometry(uint32_t degree, uint32_t world, uint32_t* prefix, uint32_t* blocks_per_owner,
+                          uint64_t* slice_bits) {
+  mgbfs2::ShardGeometry g;
+  if (int rc = mgbfs2::shard_geometry(degree, world, &g)) return rc;
+  if (prefix) *prefix = g.prefix;
+  if (blocks_per_owner) *blocks_per_owner = g.blocks_per_owner;
+  if (slice_bits) *slice_bits = g.slice_bits;
+  return MGBFS2_OK;
+}
+
+uint64_t mgbfs2_shard_scratch_bytes(void) { return mgbfs2::layer_layout(0).total; }
+
+int mgbfs2_shard_route(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
+                       const uint64_t* frontier, uint64_t count, uint32_t world, uint64_t* out, uint64_t out_capacity,
+                       uint64_t* bucket_counts, uint32_t* error, void* scratch, uint64_t scratch_bytes, void* stream) {
+  return mgbfs2::shard_route(degree, generators, permutations_host, frontier, count, world, out, out_capacity,
+                             bucket_counts, error, static_cast<unsigned char*>(scratch), scratch_bytes,
+                             static_cast<cudaStream_t>(stream));
+}
+
+int mgbfs2_shard_accept(uint32_t degree, uint32_t world, uint32_t owner, const uint64_t* incoming,
+                        const uint64_t* incoming_counts, uint64_t* bitmap_slice, uint64_t* next,
+                        uint64_t next_capacity, uint64_t* next_count, uint32_t* error, void* scratch,
+                        uint64_t scratch_bytes, void* stream) {
+  return mgbfs2::shard_accept(degree, world, owner, incoming, incoming_counts, bitmap_slice, next, next_capacity,
+                              next_count, error, static_cast<unsigned char*>(scratch), scratch_bytes,
+                              static_cast<cudaStream_t>(stream));
+}
 
 int mgbfs2_expand_layer_bitmap_static(uint32_t degree, uint32_t generators, const uint32_t* permutations_host,
                                       const uint64_t* frontier, uint64_t count, uint64_t* bitmap, uint64_t* next,

@@ -23,7 +23,7 @@ DEDUP_NAMES = {v: k for k, v in DEDUP.items()}
 PLANNER = {"plain": 0, "learned": 1}
 REASONS = {0: "FRONTIER_EXHAUSTED", 1: "DEADLINE", 2: "CANCELLED", 3: "RESOURCE", 4: "PROFILE_LAYER_LIMIT"}
 ERROR_BITS = {1: "FRONTIER_OVERFLOW", 2: "TABLE_FULL", 4: "RANK_RANGE", 8: "BUCKET_OVERFLOW", 16: "WAIT_LIMIT",
-              32: "ARENA_OVERFLOW", 64: "BAD_STATE"}
+              32: "ARENA_OVERFLOW", 64: "BAD_STATE", 128: "BAD_REFERENCE"}
 
 
 class NativeUnavailable(RuntimeError):
@@ -151,6 +151,15 @@ _SIGNATURES = {
     "mgbfs2_expand_layer_bitmap_static": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p,
                                                     C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                                     C.c_void_p, C.c_void_p]),
+    "mgbfs2_shard_geometry": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint64)]),
+    "mgbfs2_shard_scratch_bytes": (C.c_uint64, []),
+    "mgbfs2_shard_route": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p, C.c_uint64,
+                                     C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_uint64, C.c_void_p]),
+    "mgbfs2_shard_accept": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                      C.c_void_p]),
     "mgbfs2_batch_create": (C.c_int, [C.POINTER(GraphDesc), C.c_uint32, C.c_int, C.POINTER(C.c_void_p), C.c_char_p,
                                       C.c_size_t]),
     "mgbfs2_batch_run": (C.c_int, [C.c_void_p, C.POINTER(BatchOptions), C.POINTER(BatchStatus)]),

@@ -6,10 +6,11 @@ between the ranks by work and whose tables are gathered to rank 0.
 The reference splits ONE search across GPUs by state ownership
 (multigpubfs/launch.py:350-378, one `graph-rank` process per GPU) and, after
 the run, requires every rank to report the same layer table
-(multigpubfs/launch.py:398-405).  This engine's path does not shard one
-search (a layer's visited test needs the whole bitmap or table), so `--gpus N`
-runs N independent replicas; what the ranks still share is that check and the
-timing rule: the job's time is the slowest rank's device time.
+(multigpubfs/launch.py:398-405).  The owner-partitioned split of one search
+is multigpubfs_b200.sharded (the bench's `s13-lrx-sharded`); the single-graph
+workloads here run N independent replicas of the fused engine, and what the
+ranks share is that table check and the timing rule: the job's time is the
+slowest rank's device time.
 
 Everything here is host logic over `torch.distributed`; it runs on NCCL with
 CUDA tensors in the benchmark and on gloo with CPU tensors in the tests.
