@@ -25,8 +25,13 @@ namespace {
 constexpr unsigned long long kPending = 1ull << 63;
 constexpr unsigned long long kRowMask = (1ull << 40) - 1;
 constexpr unsigned long long kFailedRow = kRowMask - 1;
+// Row field of a pending claim.  It must not be kRowMask: with an all-ones
+// fingerprint that claim would equal kEmpty, a second thread would take the
+// still "empty" slot for the same key, and the state would be stored twice.
+constexpr unsigned long long kClaimRow = kRowMask - 2;
 constexpr uint32_t kFpShift = 40;
 constexpr unsigned long long kFpMask = (1ull << 23) - 1;
+static_assert((kPending | (kFpMask << kFpShift) | kClaimRow) != kEmpty, "a pending claim must never read as empty");
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr uint32_t kWideBlock = 256;
 
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(kWideBlock) wide_expand(WideParams p) {
     for (unsigned long long probe = 0; probe <= p.mask; ++probe, slot = (slot + 1) & p.mask) {
       unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&p.table[slot]);
       if (cur == kEmpty) {
-        const unsigned long long claim = kPending | (fp << kFpShift) | kRowMask;
+        const unsigned long long claim = kPending | (fp << kFpShift) | kClaimRow;
         const unsigned long long prev = atomicCAS(&p.table[slot], kEmpty, claim);
         if (prev == kEmpty) {
           const unsigned long long row = atomicAdd(p.arena_count, 1ull);
@@ -198,7 +203,7 @@ int Graph::wide_plan(mgbfs2_plan_info* p, uint64_t budget) {
   const uint64_t per_state = row_bytes + 16;  // arena row + table slots at load <= 1/2
   uint64_t cap = state_bound ? state_bound : UINT64_MAX;
   cap = std::min<uint64_t>(cap, budget / per_state);
-  cap = std::min<uint64_t>(cap, kRowMask - 2);
+  cap = std::min<uint64_t>(cap, kClaimRow);  // rows stay below kClaimRow and kFailedRow
   if (!cap) return MGBFS2_OUT_OF_MEMORY;
   p->capacity = std::min(p->capacity, cap);
   p->table_slots = std::max<uint64_t>(1024, next_pow2_u64(2 * std::min<uint64_t>(cap, 1ull << 20)));

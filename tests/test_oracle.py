@@ -181,3 +181,10 @@ def test_product_domain_sizes_match_reference():
         G.product_rank(start, gens, bad)
     with pytest.raises(ValueError):
         G.position_components(3, [[0, 0, 1]])
+
+
+def test_matrix_oracle_matches_the_reference_sl2_table():
+    from tests.conftest import golden
+    fx = golden("matrix_groups.json")["cases"]["sl2_mod31"]
+    assert G.layer_sizes(fx["graph"]) == fx["layers"]
+    assert sum(fx["layers"]) == 31 * (31 * 31 - 1)
