@@ -55,12 +55,14 @@ uint64_t program_digest(const Graph& g) {
   };
   mix(g.perms.data(), g.perms.size() * sizeof(uint32_t));
   mix(g.codes.data(), g.codes.size() * sizeof(uint32_t));
+  mix(g.matrices.data(), g.matrices.size() * sizeof(int64_t));
+  mix(g.moduli.data(), g.moduli.size() * sizeof(uint32_t));
   mix(&g.bits, sizeof(g.bits));
   return h;
 }
 
 bool checkpointable(int visit) {
-  return visit == V_LEHMER || visit == V_MULTISET || visit == V_PRODUCT || visit == V_HASH || visit == V_HASHQ;
+  return bitmap_kind(visit) || visit == V_HASH || visit == V_HASHQ;
 }
 
 // Device bytes <-> file through a pinned staging buffer.

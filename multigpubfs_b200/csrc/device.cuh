@@ -296,7 +296,53 @@ constexpr uint32_t kMaxComponents = 16;
 // The visited structure of a packed plan.  V_HASHQ: the all-visited set as
 // a quotient table of 32-bit slots.  V_PRODUCT: a bitmap over the product of
 // the position components' multiset domains.
-enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3, V_HASHQ = 4, V_PRODUCT = 5 };
+enum VisitKind : int { V_LEHMER = 0, V_MULTISET = 1, V_HASH = 2, V_HASH3 = 3, V_HASHQ = 4, V_PRODUCT = 5, V_RADIX = 6 };
+
+// Visited kinds kept as a bitmap over a rank domain.
+__host__ __device__ constexpr bool bitmap_kind(int v) {
+  return v == V_LEHMER || v == V_MULTISET || v == V_PRODUCT || v == V_RADIX;
+}
+
+// ---------------------------------------------------------------------------
+// Packed modular matrices: a rows x cols state of entries in [0, mod), entry
+// j = i * cols + c in bits [bits * j, bits * (j + 1)) of one word.  Generator g
+// is a rows x rows integer matrix (its coefficients are the masks of program
+// terms g * rows^2 ..); the child is (M_g . S) mod mod entry by entry.  The
+// host packs a graph only when no partial sum can leave int64, so the result
+// equals the reference's wrap-then-modulus (graph_definition.py:77-83).
+// The bitmap rank is the mixed-radix number of the entries, sum e_j * mod^j,
+// over the whole canonical entry space (the reference's certified bound,
+// workload_geometry.py:21-36).
+struct MatrixAction {
+  uint32_t rows, cols, bits, mod;  // mod = 0: permutation terms instead
+};
+
+__device__ __forceinline__ uint64_t apply_matrix(const MatrixAction& a, uint64_t s, const Term* coef) {
+  const uint64_t field = (1ull << a.bits) - 1;
+  uint64_t child = 0;
+  for (uint32_t i = 0; i < a.rows; ++i) {
+    for (uint32_t c = 0; c < a.cols; ++c) {
+      long long acc = 0;
+      for (uint32_t k = 0; k < a.rows; ++k)
+        acc += static_cast<long long>(coef[i * a.rows + k].mask) *
+               static_cast<long long>((s >> (a.bits * (k * a.cols + c))) & field);
+      // Most sums of small coefficients stay in [0, 2^32): a 32-bit remainder.
+      long long v = (acc >= 0 && acc < (1ll << 32)) ? static_cast<long long>(static_cast<uint32_t>(acc) % a.mod)
+                                                   : acc % static_cast<long long>(a.mod);
+      if (v < 0) v += a.mod;
+      child |= static_cast<uint64_t>(v) << (a.bits * (i * a.cols + c));
+    }
+  }
+  return child;
+}
+
+__device__ __forceinline__ uint64_t radix_rank(uint64_t s, const MatrixAction& a) {
+  const uint64_t field = (1ull << a.bits) - 1;
+  const uint32_t n = a.rows * a.cols;
+  uint64_t r = 0;
+  for (uint32_t j = n; j-- > 0;) r = r * a.mod + ((s >> (a.bits * j)) & field);
+  return r;
+}
 
 struct ProductDomain {
   uint32_t components, bits, distinct, pad;

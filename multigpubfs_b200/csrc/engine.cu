@@ -296,18 +296,44 @@ void Graph::analyse() {
       }
     }
   } else {
-    packed = false;
+    packed = packed_matrix = false;
     state_bound = orbit_bound;
     // Canonical same-modulus entries bound the orbit (workload_geometry.py:21-36).
     bool same = !moduli.empty();
     for (uint32_t m : moduli) same = same && m == moduli[0];
     if (same && moduli[0]) {
+      const uint32_t m = moduli[0];
       bool canonical = true;
-      for (int64_t v : start) canonical = canonical && v >= 0 && v < static_cast<int64_t>(moduli[0]);
+      for (int64_t v : start) canonical = canonical && v >= 0 && v < static_cast<int64_t>(m);
       uint64_t b = 1;
-      for (size_t i = 0; i < start.size(); ++i) b = sat_mul(b, moduli[0]);
+      for (size_t i = 0; i < start.size(); ++i) b = sat_mul(b, m);
       if (!canonical) b = b == UINT64_MAX ? b : b + 1;
       state_bound = state_bound ? std::min(state_bound, b) : b;
+      // Packing: entries of ceil(log2 m) bits, the word's top bit left clear
+      // (so no state equals the empty marker), and every partial sum of a row
+      // of |coefficients| times (m - 1) inside int64.
+      uint32_t eb = 1;
+      while ((1ull << eb) < m) ++eb;
+      bool fits = canonical && static_cast<uint64_t>(n) * eb < 64;
+      for (uint32_t k = 0; k < gens && fits; ++k)
+        for (uint32_t i = 0; i < rows && fits; ++i) {
+          unsigned __int128 sum = 0;
+          for (uint32_t j = 0; j < rows; ++j) {
+            const int64_t v = matrices[static_cast<size_t>(k) * rows * rows + i * rows + j];
+            const unsigned __int128 a = v < 0 ? static_cast<unsigned __int128>(-(v + 1)) + 1 : v;
+            sum += a * (m - 1);
+          }
+          fits = sum <= static_cast<unsigned __int128>(INT64_MAX);
+        }
+      if (fits) {
+        packed = packed_matrix = true;
+        bits = eb;
+        key_mask = (1ull << (n * eb)) - 1;
+        start_word = 0;
+        for (uint32_t i = 0; i < n; ++i) start_word |= static_cast<uint64_t>(start[i]) << (eb * i);
+        rank_total = b;  // m^entries, the radix-rank domain
+        rank_ok = rank_total != UINT64_MAX;
+      }
     }
     inverse_closed = matrix_inverse_closed();
   }
@@ -318,6 +344,10 @@ void Graph::analyse() {
 void Graph::build_program() {
   term_begin.assign(1, 0);
   terms.clear();
+  if (packed_matrix) {
+    build_matrix_program();
+    return;
+  }
   if (!packed) return;
   const uint32_t n = elements;
   for (uint32_t k = 0; k < gens; ++k) {
@@ -353,6 +383,44 @@ void Graph::build_program() {
     const uint32_t key_bits = n * bits, tag_bits = 32 - __builtin_clz(gens);
     if (key_bits + tag_bits <= 64) gen_shift = key_bits;
   }
+  term_begin.insert(term_begin.end(), inverse.begin(), inverse.end());
+}
+
+static std::vector<int64_t> mat_mul_mod(const std::vector<int64_t>& a, const std::vector<int64_t>& b, uint32_t n,
+                                        uint32_t m, uint32_t mod);
+
+// Program of packed modular matrices: generator g's rows x rows coefficients
+// as term masks g * rows^2 .., then the parent-edge table: inverse[g] = the
+// first generator h with M_h . M_g = I (mod m), whose child of a child of g
+// is the parent itself.
+void Graph::build_matrix_program() {
+  const uint32_t r = rows, m = moduli[0];
+  for (uint32_t k = 0; k < gens; ++k) {
+    for (uint32_t j = 0; j < r * r; ++j)
+      terms.push_back(Term{static_cast<unsigned long long>(matrices[static_cast<size_t>(k) * r * r + j]), 0u, 0u});
+    term_begin.push_back(static_cast<uint32_t>(terms.size()));
+  }
+  std::vector<int64_t> eye(static_cast<size_t>(r) * r, 0);
+  for (uint32_t i = 0; i < r; ++i) eye[i * r + i] = 1;
+  auto reduced = [&](uint32_t k) {
+    std::vector<int64_t> a(matrices.begin() + static_cast<size_t>(k) * r * r,
+                           matrices.begin() + static_cast<size_t>(k + 1) * r * r);
+    for (auto& v : a) {
+      v %= static_cast<int64_t>(m);
+      if (v < 0) v += m;
+    }
+    return a;
+  };
+  std::vector<uint32_t> inverse(gens, 0xffffffffu);
+  bool any = false;
+  for (uint32_t k = 0; k < gens; ++k) {
+    for (uint32_t h = 0; h < gens && inverse[k] == 0xffffffffu; ++h)
+      if (mat_mul_mod(reduced(h), reduced(k), r, r, m) == eye) inverse[k] = h;
+    any = any || inverse[k] != 0xffffffffu;
+  }
+  gen_shift = 0;
+  const uint32_t key_bits = elements * bits, tag_bits = 32 - __builtin_clz(gens);
+  if (any && key_bits + tag_bits <= 64) gen_shift = key_bits;
   term_begin.insert(term_begin.end(), inverse.begin(), inverse.end());
 }
 
@@ -723,12 +791,13 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     }
   }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
-  const bool hash_routed = dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_HASH && packed;
+  const bool hash_routed =
+      dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_HASH && packed && !packed_matrix;
   if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) &&
       !(visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product) && !hash_routed)
     return MGBFS2_UNSUPPORTED;
   // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
-  if (dedup == MGBFS2_DEDUP_SORT && (!packed || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
+  if (dedup == MGBFS2_DEDUP_SORT && (!packed || packed_matrix || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
   if (dedup == MGBFS2_DEDUP_BUCKET && !hash_routed) {
     // Shards = states sharing their first K symbols: N!/(N-K)! shards whose
     // bitmap slices hold (N-K)! bits.  Default: the smallest K (1 or 2) whose
@@ -901,6 +970,8 @@ static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
       return warp ? expand_packed<V_MULTISET, 0, true> : expand_packed<V_MULTISET, 0, false>;
     case V_PRODUCT:
       return warp ? expand_packed<V_PRODUCT, 0, true> : expand_packed<V_PRODUCT, 0, false>;
+    case V_RADIX:
+      return warp ? expand_packed<V_RADIX, 0, true> : expand_packed<V_RADIX, 0, false>;
     case V_HASH:
       return expand_packed<V_HASH, 0, false>;
     case V_HASHQ:
@@ -1282,6 +1353,7 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
 
 int Graph::visit_kind() const {
   if (plan.visited == MGBFS2_VISITED_BITMAP) {
+    if (packed_matrix) return V_RADIX;
     if (use_product) return V_PRODUCT;
     return (lehmer && elements >= 2) ? V_LEHMER : V_MULTISET;
   }
@@ -1609,6 +1681,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     set_carveout(reinterpret_cast<const void*>(fn), smem,
                  want_blocks(visit == V_HASHQ ? kHashQBlocksPerSM : kPackedBlocksPerSM));
   if (visit == V_PRODUCT) p.pd = product_domain;
+  p.mat = matrix_action();
   if (visit == V_MULTISET) {
     p.ms.n = elements;
     p.ms.bits = bits;
@@ -1622,7 +1695,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   // Initial state: visited structure cleared, start seeded, frontier = {start}
   // (a resumed run keeps what the checkpoint restored).
   MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
-  if (visit == V_LEHMER || visit == V_MULTISET || visit == V_PRODUCT) {
+  if (bitmap_kind(visit)) {
     if (!resume) MG_CHECK(cudaMemsetAsync(bitmap.ptr, 0, bitmap.bytes, stream));
     p.bitmap = static_cast<unsigned long long*>(bitmap.ptr);
   } else if (visit == V_HASH) {
@@ -1652,8 +1725,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   const bool limited = limits && (limits->max_seconds > 0 || limits->max_layers || limits->cancel);
   const uint64_t loop_cap = std::max<uint64_t>(1, plan.capacity);
   bool device_loop = !host_loop_only && !bucketed && !grouped_mode && !limited && !cb &&
-                     (visit == V_LEHMER || visit == V_MULTISET || visit == V_PRODUCT || visit == V_HASH ||
-                      visit == V_HASHQ) &&
+                     (bitmap_kind(visit) || visit == V_HASH || visit == V_HASHQ) &&
                      2 * (loop_cap + 2) * 8 <= (16ull << 30);
   // The device loop never grows the table: it must hold every state below
   // the growth threshold, or (a table sized by the learned planner) the loop
@@ -1959,7 +2031,10 @@ void Graph::keep_small(uint32_t depth, std::vector<uint64_t>&& words) {
 std::vector<int64_t> Graph::decode(uint64_t w) const {
   std::vector<int64_t> row(elements);
   const uint64_t mask = bits == 64 ? ~0ull : ((1ull << bits) - 1);
-  for (uint32_t i = 0; i < elements; ++i) row[i] = labels[(w >> (bits * i)) & mask];
+  for (uint32_t i = 0; i < elements; ++i) {
+    const uint64_t f = (w >> (bits * i)) & mask;
+    row[i] = packed_matrix ? static_cast<int64_t>(f) : labels[f];
+  }
   return row;
 }
 

@@ -85,6 +85,13 @@ struct Graph {
 
   // Analysis.
   bool packed = false, inverse_closed = false, lehmer = false, rank_ok = false;
+  // Modular matrices with one modulus, canonical start entries and no int64
+  // overflow in any product: packed into one word of `bits`-bit entries and
+  // expanded by the fused kernels (MatrixAction); others take the wide path.
+  bool packed_matrix = false;
+  MatrixAction matrix_action() const {
+    return packed_matrix ? MatrixAction{rows, cols, bits, moduli[0]} : MatrixAction{0, 0, 0, 0};
+  }
   uint32_t bits = 4, distinct = 0;
   std::vector<int64_t> labels;     // code -> label
   std::vector<uint32_t> codes;     // start codes
@@ -188,6 +195,7 @@ struct Graph {
   ~Graph();
   void analyse();
   void build_program();
+  void build_matrix_program();
   bool matrix_inverse_closed() const;
   void release();
   int make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out);

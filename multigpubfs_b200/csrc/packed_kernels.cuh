@@ -69,19 +69,29 @@ struct ExpandParams {
   LoopState* loop;  // graph mode: count and buffers from here instead of frontier/count/next
   QuotientSlots q;  // V_HASHQ table
   ProductDomain pd;  // V_PRODUCT rank domain
+  MatrixAction mat;  // packed modular matrices (mat.mod != 0); V_RADIX rank domain
 };
+
+// The child of packed state s under generator g (terms [tb, te) of the
+// program): permutation displacement terms, or a modular matrix product.
+__device__ __forceinline__ uint64_t apply_action(const ExpandParams& p, uint64_t s, const Term* terms, uint32_t tb,
+                                                 uint32_t te) {
+  return p.mat.mod ? apply_matrix(p.mat, s, terms + tb) : apply_terms(s, terms, tb, te);
+}
 
 // Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the
 // warp-aggregated bitmap path uses warp collectives); `valid` masks lanes
 // without a candidate.
 template <int V, int N, bool WARP>
 __device__ __forceinline__ bool claim(const ExpandParams& p, uint64_t c, bool valid) {
-  if constexpr (V == V_LEHMER || V == V_MULTISET || V == V_PRODUCT) {
+  if constexpr (bitmap_kind(V)) {
     uint64_t r = 0;
     bool ok = valid;
     if (valid) {
       if constexpr (V == V_LEHMER) {
         r = lehmer_rank4<N>(c);
+      } else if constexpr (V == V_RADIX) {
+        r = radix_rank(c, p.mat);
       } else if constexpr (V == V_PRODUCT) {
         ok = product_rank(c, p.pd, &r);
         if (!ok) raise_error(&p.control->error, ERR_RANK_RANGE);
@@ -258,7 +268,7 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
   #pragma unroll
           for (int k = 0; k < 4; ++k) {
             live[k] = k < static_cast<int>(p.ppt) && val[k] && g != skip[k];
-            ch[k] = live[k] ? apply_terms(par[k], terms, tb, te) : 0;
+            ch[k] = live[k] ? apply_action(p, par[k], terms, tb, te) : 0;
             first[k] = live[k] ? qhash_first(p.q, ch[k]) : 0u;
           }
   #pragma unroll
@@ -284,7 +294,7 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
           for (int k = 0; k < 4; ++k) {
             if (k >= static_cast<int>(p.ppt)) break;
             const bool v = val[k] && g != skip[k];
-            const uint64_t c = v ? apply_terms(par[k], terms, tb, te) : 0;
+            const uint64_t c = v ? apply_action(p, par[k], terms, tb, te) : 0;
             const bool won = claim<V, N, WARP>(p, c, v);
             const unsigned m = __ballot_sync(kFullMask, won);
             if (m) {
@@ -367,7 +377,7 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
       const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
       for (uint32_t g = 0; g < p.gens; ++g) {
         if (g == skip) continue;
-        const uint64_t c = apply_terms(par, terms, begin[g], begin[g + 1]);
+        const uint64_t c = apply_action(p, par, terms, begin[g], begin[g + 1]);
         s.keys[g * per_tile + j] = c | (p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull);
       }
     }
@@ -430,6 +440,9 @@ static __global__ void seed_packed(ExpandParams p, unsigned long long start, int
   } else if (kind == V_PRODUCT) {
     if (product_rank(start, p.pd, &r)) atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
     else raise_error(&p.control->error, ERR_RANK_RANGE);
+  } else if (kind == V_RADIX) {
+    r = radix_rank(start, p.mat);
+    atomicOr(&p.bitmap[r >> 6], 1ull << (r & 63));
   } else if (kind == V_HASHQ) {
     if (qhash_insert(p.q, start) < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
   } else {

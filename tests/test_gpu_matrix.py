@@ -36,3 +36,70 @@ def test_sl2_orbit_is_the_group_order(p):
         for _ in range(3):
             r = e.run()
             assert r.complete and r.states == p * (p * p - 1)
+
+
+def _gl2(p):
+    from multigpubfs_b200 import GraphDefinition
+    g = next(r for r in range(2, p) if all(pow(r, (p - 1) // q, p) != 1
+                                           for q in range(2, p) if (p - 1) % q == 0 and
+                                           all(q % d for d in range(2, int(q ** 0.5) + 1))))
+    gi = pow(g, p - 2, p)
+    gens = [[1, 1, 0, 1], [1, 0, 1, 1], [1, p - 1, 0, 1], [1, 0, p - 1, 1], [g, 0, 0, 1], [gi, 0, 0, 1]]
+    return GraphDefinition.matrix(2, 2, [(m, p) for m in gens], [1, 0, 0, 1])
+
+
+@pytest.mark.parametrize("visited", ["bitmap", "hash", "auto"])
+def test_packed_matrices_match_the_reference_on_every_visited_set(visited):
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    from oracle import graph_oracle as G
+    fx = golden("matrix_groups.json")["cases"]["sl2_mod31"]
+    g = GraphDefinition.from_dict(fx["graph"])
+    with NativeGraph(g) as e:
+        info = e.plan(visited=visited)
+        r = e.run()
+        last = e.sample(0, 1000)
+    assert info["packed"] == 1 and info["bits_per_symbol"] == 5 and info["parent_skip"] == 1
+    if info["visited"] == "bitmap":
+        assert info["bitmap_bits"] == 31 ** 4
+    assert r.layer_sizes == fx["layers"]
+    expect_last = sorted(tuple(s) for s in G.exact_layers(fx["graph"], 1 << 20)[-1])
+    assert [tuple(s) for s in last] == expect_last
+
+
+@pytest.mark.parametrize("p", [31, 101])
+def test_gl2_orbit_is_the_group_order(p):
+    from multigpubfs_b200.engine import NativeGraph
+    with NativeGraph(_gl2(p)) as e:
+        info = e.plan()
+        r = e.run()
+    assert info["packed"] == 1 and info["visited"] == "bitmap"
+    assert r.complete and r.states == (p * p - 1) * (p * p - p)
+
+
+def test_unpackable_matrices_stay_on_the_wide_path():
+    """Coefficients whose products could leave int64 are not packed; the wide
+    path keeps the reference's wrap-then-modulus."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    from oracle import graph_oracle as G
+    big = 1 << 45
+    gens = [([1, big, 0, 1], 1 << 20), ([1, 0, 1, 1], 1 << 20)]
+    g = GraphDefinition.matrix(2, 1, gens, [1, 2])
+    with NativeGraph(g) as e:
+        info = e.plan()
+        r = e.run(max_layers=6)
+    assert info["packed"] == 0
+    graph = G.matrix_graph(2, 1, gens, [1, 2])
+    seen, layer, expect = {(1, 2)}, [(1, 2)], [1]
+    while len(expect) < 6:
+        nxt = []
+        for s in layer:
+            for k in range(len(gens)):
+                c = tuple(G.successor(graph, list(s), k))
+                if c not in seen:
+                    seen.add(c)
+                    nxt.append(c)
+        layer = nxt
+        expect.append(len(nxt))
+    assert r.layer_sizes == expect
