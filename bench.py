@@ -62,6 +62,16 @@ def lrx(n):
     return [left, right, x]
 
 
+def gl2_generators(p):
+    """GL(2, p) from the identity: the elementary transvections, diag(g, 1) for
+    a primitive root g, and their inverses (orbit (p^2 - 1)(p^2 - p))."""
+    fac = [q for q in range(2, p) if (p - 1) % q == 0 and all(q % d for d in range(2, int(q ** 0.5) + 1))]
+    g = next(r for r in range(2, p) if all(pow(r, (p - 1) // q, p) != 1 for q in fac))
+    gi = pow(g, p - 2, p)
+    return [([1, 1, 0, 1], p), ([1, 0, 1, 1], p), ([1, p - 1, 0, 1], p), ([1, 0, p - 1, 1], p),
+            ([g, 0, 0, 1], p), ([gi, 0, 0, 1], p)]
+
+
 def coxeter(n):
     out = []
     for i in range(n - 1):
@@ -78,6 +88,10 @@ WORKLOADS = {
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
+    "gl2-211-matrix": dict(matrix_p=211, visited="bitmap", dedup="atomic",
+                           desc="GL(2,211) on 2x2 int64 matrices mod 211 from the identity, 6 generators: "
+                                "1,972,681,200 states, 99.5 % of the certified entry-space bound 211^4; packed "
+                                "8-bit entries, mixed-radix bitmap"),
 }
 BATCHED = ("sweep512", "planner-s12", "s13-lrx-sharded")
 
@@ -117,6 +131,37 @@ def expected_layers(name, n):
     if name == "s11-lrx-hash":
         return golden("lrx_layers.json")["layers"]["11"]
     return None
+
+
+def workload_graph(name):
+    from multigpubfs_b200 import GraphDefinition
+    w = WORKLOADS[name]
+    if "matrix_p" in w:
+        return GraphDefinition.matrix(2, 2, gl2_generators(w["matrix_p"]), [1, 0, 0, 1])
+    return GraphDefinition.permutation(w["gens"], list(range(w["n"])))
+
+
+def matrix_sample(p, states=300_000):
+    """The oracle's level BFS of GL(2, p) (oracle.graph_oracle.successor, one
+    core) until the settled states pass `states`: (layer sizes, seconds)."""
+    from oracle import graph_oracle as G
+    graph = G.matrix_graph(2, 2, gl2_generators(p), [1, 0, 0, 1])
+    gens = len(graph["action"]["generators"])
+    t = time.perf_counter()
+    start = (1, 0, 0, 1)
+    seen, layer, sizes = {start}, [start], [1]
+    while layer and sum(sizes) < states:
+        nxt = []
+        for s in layer:
+            for k in range(gens):
+                c = tuple(G.successor(graph, list(s), k))
+                if c not in seen:
+                    seen.add(c)
+                    nxt.append(c)
+        layer = nxt
+        if nxt:
+            sizes.append(len(nxt))
+    return sizes, time.perf_counter() - t
 
 
 def generator_digest(graph):
@@ -201,7 +246,15 @@ def cpu_sample(name, threads=None):
         name = "s13-lrx"  # the same BFS, split or not
     t = time.perf_counter()
     succ = states = 0
-    if name in WORKLOADS:
+    engine = "C oracle (restated reference exact BFS)"
+    if name in WORKLOADS and "matrix_p" in WORKLOADS[name]:
+        p = WORKLOADS[name]["matrix_p"]
+        sizes, _ = matrix_sample(p)
+        threads = 1
+        states, succ = sum(sizes), 6 * sum(sizes)
+        what = f"GL(2,{p}) layers 0-{len(sizes) - 1}"
+        engine = "Python oracle level BFS (restated reference exact_layers, one core)"
+    elif name in WORKLOADS:
         w = WORKLOADS[name]
         layers = CPU_SAMPLE_LAYERS.get(name)
         bitmap = w["visited"] == "bitmap"
@@ -226,8 +279,7 @@ def cpu_sample(name, threads=None):
         what = f"S12 planner instance 0, layers 0-{len(sizes) - 1} (Lehmer bitmap)"
     dt = time.perf_counter() - t
     return {"value": succ / dt, "unit": "successors/s", "cores": threads, "kind": "port",
-            "sample": f"{what}: {states:,} states, {succ:,} successors, C oracle (restated reference exact BFS), "
-                      f"{dt:.2f} s"}
+            "sample": f"{what}: {states:,} states, {succ:,} successors, {engine}, {dt:.2f} s"}
 
 
 def workload_desc(name):
@@ -506,8 +558,19 @@ def bench_single(args, rank, world, local):
     w = WORKLOADS[args.workload]
     visited = args.visited or w["visited"]
     dedup = args.dedup or w["dedup"]
-    graph = GraphDefinition.permutation(w["gens"], list(range(w["n"])))
-    expect = expected_layers(args.workload, w["n"])
+    graph = workload_graph(args.workload)
+    expect = expected_layers(args.workload, w.get("n"))
+    if expect is None:
+        # GL(2, p): the group order, and the oracle's first layers.
+        p = w["matrix_p"]
+        order = (p * p - 1) * (p * p - p)
+        prefix, _ = matrix_sample(p, 50_000)
+
+        def table_ok(sizes):
+            return sum(sizes) == order and sizes[:len(prefix) - 1] == prefix[:-1]
+    else:
+        def table_ok(sizes):
+            return sizes == expect
 
     def barrier():
         if world > 1:
@@ -519,7 +582,7 @@ def bench_single(args, rank, world, local):
     plan = eng.plan(visited=visited, dedup=dedup, host_loop=args.host_loop)
     for _ in range(args.warmup):
         r = eng.run()
-        assert r.layer_sizes == expect, "layer table mismatch in warm-up"
+        assert table_ok(r.layer_sizes), "layer table mismatch in warm-up"
     results = []
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -537,7 +600,7 @@ def bench_single(args, rank, world, local):
     # engine's own CUDA-event time of each run is summed beside it.
     engine_s = sum(r.device_seconds for r in results)
     for r in results:
-        assert r.complete and r.layer_sizes == expect, "layer table mismatch in a timed run"
+        assert r.complete and table_ok(r.layer_sizes), "layer table mismatch in a timed run"
     device_max = device_s
     if world > 1:
         # Replicas: every rank must hold the same table; the job time is the slowest rank's.
@@ -557,7 +620,10 @@ def bench_single(args, rank, world, local):
 
     # ---- e2e: C-ABI handle from host buffers, every step ------------------------------
     e2e_times = []
-    h2d = 8 * w["n"] + 4 * w["n"] * len(w["gens"]) + 8
+    if "matrix_p" in w:
+        h2d = 8 * 4 + 6 * (8 * 4 + 4) + 8
+    else:
+        h2d = 8 * w["n"] + 4 * w["n"] * len(w["gens"]) + 8
     d2h = 0
     for i in range(args.steps + 1):
         barrier()
@@ -571,8 +637,8 @@ def bench_single(args, rank, world, local):
         torch.cuda.synchronize()
         if i:
             e2e_times.append(time.perf_counter() - t0)
-        assert sizes == expect
-        d2h = 24 * len(sizes) + 16 * len(sizes) + 8 * w["n"] * (len(cur) + len(prev))
+        assert table_ok(sizes)
+        d2h = 24 * len(sizes) + 16 * len(sizes) + 8 * len(graph.start) * (len(cur) + len(prev))
     e2e_t = torch.tensor([sum(e2e_times) / len(e2e_times)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
