@@ -62,16 +62,6 @@ def lrx(n):
     return [left, right, x]
 
 
-def gl2_generators(p):
-    """GL(2, p) from the identity: the elementary transvections, diag(g, 1) for
-    a primitive root g, and their inverses (orbit (p^2 - 1)(p^2 - p))."""
-    fac = [q for q in range(2, p) if (p - 1) % q == 0 and all(q % d for d in range(2, int(q ** 0.5) + 1))]
-    g = next(r for r in range(2, p) if all(pow(r, (p - 1) // q, p) != 1 for q in fac))
-    gi = pow(g, p - 2, p)
-    return [([1, 1, 0, 1], p), ([1, 0, 1, 1], p), ([1, p - 1, 0, 1], p), ([1, 0, p - 1, 1], p),
-            ([g, 0, 0, 1], p), ([gi, 0, 0, 1], p)]
-
-
 def coxeter(n):
     out = []
     for i in range(n - 1):
@@ -137,7 +127,8 @@ def workload_graph(name):
     from multigpubfs_b200 import GraphDefinition
     w = WORKLOADS[name]
     if "matrix_p" in w:
-        return GraphDefinition.matrix(2, 2, gl2_generators(w["matrix_p"]), [1, 0, 0, 1])
+        from multigpubfs_b200.workloads import gl2_graph
+        return GraphDefinition.from_dict(gl2_graph(w["matrix_p"]))
     return GraphDefinition.permutation(w["gens"], list(range(w["n"])))
 
 
@@ -145,7 +136,8 @@ def matrix_sample(p, states=300_000):
     """The oracle's level BFS of GL(2, p) (oracle.graph_oracle.successor, one
     core) until the settled states pass `states`: (layer sizes, seconds)."""
     from oracle import graph_oracle as G
-    graph = G.matrix_graph(2, 2, gl2_generators(p), [1, 0, 0, 1])
+    from multigpubfs_b200.workloads import gl2_graph
+    graph = gl2_graph(p)
     gens = len(graph["action"]["generators"])
     t = time.perf_counter()
     start = (1, 0, 0, 1)

@@ -4,8 +4,9 @@
     python -m multigpubfs_b200.cli plan  <graph.json | family> [--visited ..] [--dedup ..]
     python -m multigpubfs_b200.cli run   <graph.json | family> [--max-layers N] [--repeat R] [--out DIR]
 
-``family`` is one of ``lrx:N`` (L, R, X on S_N) or ``coxeter:N`` (adjacent
-transpositions on S_N), started from the identity.  ``run`` prints one JSON
+``family`` is one of ``lrx:N`` (L, R, X on S_N), ``coxeter:N`` (adjacent
+transpositions on S_N), started from the identity, or ``gl2:P`` (GL(2, P) on
+2x2 matrices mod the prime P).  ``run`` prints one JSON
 line with the layer table and timings; with ``--out`` it writes the schema-2
 report.json / states.json through run_graph instead.
 """
@@ -38,7 +39,10 @@ def family(spec: str) -> GraphDefinition:
             g[i], g[i + 1] = g[i + 1], g[i]
             gens.append(g)
         return GraphDefinition.permutation(gens, list(range(n)), name=f"coxeter-{n}")
-    raise SystemExit(f"unknown graph {spec!r}: use a schema-2 JSON file, lrx:N or coxeter:N")
+    if kind == "gl2":
+        from .workloads import gl2_graph
+        return GraphDefinition.from_dict(gl2_graph(n))
+    raise SystemExit(f"unknown graph {spec!r}: use a schema-2 JSON file, lrx:N, coxeter:N or gl2:P")
 
 
 def main(argv=None) -> int:

@@ -40,9 +40,10 @@ constexpr uint32_t kMaxEntries = 12;                 // staged successors per th
 constexpr uint32_t kWarpsPerBlock = kBlock / 32;
 constexpr uint32_t kStageCap = kBlock * kMaxEntries;  // 3072
 constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per accept work item
-constexpr unsigned long long kFactorial[17] = {1ull, 1ull, 2ull, 6ull, 24ull, 120ull, 720ull, 5040ull, 40320ull,
-                                               362880ull, 3628800ull, 39916800ull, 479001600ull, 6227020800ull,
-                                               87178291200ull, 1307674368000ull, 20922789888000ull};
+// Template N of the route / accept kernels for packed modular matrices: shard
+// = the top entry (the most significant digit of the radix rank), so shard s
+// owns the rank range [s * m^(E-1), (s + 1) * m^(E-1)).
+constexpr int kRadixDomain = -1;
 
 struct RouteParams {
   const unsigned long long* frontier;
@@ -65,6 +66,7 @@ struct RouteParams {
   // s mod owners and goes to bucket (s mod owners) * owner_blocks + s / owners,
   // so each rank's buckets are contiguous (owner-major, block-minor).
   uint32_t owners, owner_blocks;
+  MatrixAction mat;  // packed modular matrices (route_lehmer<kRadixDomain, 1>)
 };
 
 struct AcceptParams {
@@ -85,6 +87,7 @@ struct AcceptParams {
   // block b / owners, i.e. of prefix block (b / owners) * owners + owner, and
   // `bitmap` is the rank's slice: bit = local block * (N-K)! + rank in block.
   uint32_t owners, owner;
+  MatrixAction mat;  // accept_lehmer<kRadixDomain, 1>: the radix rank's digits
 };
 
 // Shard of a successor: its rank range for the Lehmer bitmap, or (N = 0) the
@@ -118,7 +121,10 @@ __device__ __forceinline__ uint32_t prefix_shard(uint64_t w) {
 
 template <int N, int K>
 __device__ __forceinline__ uint32_t route_shard(const RouteParams& p, uint64_t c) {
-  if constexpr (N == 0) {
+  if constexpr (N == kRadixDomain) {
+    const uint32_t top = p.mat.rows * p.mat.cols - 1;
+    return static_cast<uint32_t>((c >> (p.mat.bits * top)) & ((1ull << p.mat.bits) - 1));
+  } else if constexpr (N == 0) {
     return static_cast<uint32_t>((mix64(c & p.key_mask) & p.table_mask) >> p.region_shift);
   } else {
     const uint32_t s = prefix_shard<N, K>(c);
@@ -184,7 +190,7 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
         for (int k = 0; k < 4; ++k) {
           if (k >= static_cast<int>(p.ppt)) break;
           if (val[k] && g != skip[k]) {
-            const uint64_t c = apply_terms(par[k], terms, tb, te);
+            const uint64_t c = p.mat.mod ? apply_matrix(p.mat, par[k], terms, tb, te) : apply_terms(par[k], terms, tb, te);
             const uint32_t s = route_shard<N, K>(p, c);
             const uint32_t slot = live * kBlock + tid;
             sm.state[slot] = c | gtag;
@@ -304,7 +310,11 @@ __global__ void __launch_bounds__(kBlock) count_lehmer(RouteParams p) {
     const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(w >> p.gen_shift) : 0u;
     const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
     for (uint32_t g = 0; g < p.gens; ++g)
-      if (g != skip) atomicAdd(&hist[route_shard<N, K>(p, apply_terms(w, terms, tbegin[g], tbegin[g + 1]))], 1u);
+      if (g != skip) {
+        const uint64_t c = p.mat.mod ? apply_matrix(p.mat, w, terms, tbegin[g], tbegin[g + 1])
+                                     : apply_terms(w, terms, tbegin[g], tbegin[g + 1]);
+        atomicAdd(&hist[route_shard<N, K>(p, c)], 1u);
+      }
   }
   __syncthreads();
   for (uint32_t s = threadIdx.x; s < p.shards; s += blockDim.x)
@@ -352,10 +362,14 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
     // Prefix block of the bucket's states and the offset of its bits: on one
     // GPU the bucket is the block and its bits are its ranks; on an owner
     // slice, local block j = s / owners holds prefix block j * owners + owner.
-    const bool sliced = p.owners > 1;
+    const bool sliced = N > 0 && p.owners > 1;
     const uint32_t local = sliced ? s / p.owners : s;
     const uint32_t block = sliced ? local * p.owners + p.owner : s;
-    const uint64_t shift = static_cast<uint64_t>(block - local) * kFactorial[N - K];
+    uint64_t shift = 0;
+    if constexpr (N > 0) {
+      constexpr uint64_t kBlockRanks = factorial_u64(N - K);
+      shift = static_cast<uint64_t>(block - local) * kBlockRanks;
+    }
     for (uint32_t round = 0; round < n; round += 8 * kBlock) {
       unsigned long long w[8], old[8];
       uint64_t r[8];
@@ -369,9 +383,14 @@ __global__ void __launch_bounds__(kBlock) accept_lehmer(AcceptParams p) {
       for (int k = 0; k < 8; ++k) {
         const uint32_t i = round + k * kBlock + tid;
         // A state routed to a rank that does not own it is never claimed.
-        const bool mine = !sliced || prefix_shard<N, K>(w[k]) == block;
+        bool mine = true;
+        if constexpr (N > 0) {
+          mine = !sliced || prefix_shard<N, K>(w[k]) == block;
+          r[k] = lehmer_rank4_in_shard<N, K>(w[k], block) - shift;
+        } else {
+          r[k] = radix_rank(w[k], p.mat);
+        }
         bad = bad || (i < n && !mine);
-        r[k] = lehmer_rank4_in_shard<N, K>(w[k], block) - shift;
         old[k] = i < n && mine ? atomicOr(&p.bitmap[r[k] >> 6], 1ull << (r[k] & 63)) : ~0ull;
       }
       if (bad) raise_error(&p.control->error, ERR_BAD_REFERENCE);

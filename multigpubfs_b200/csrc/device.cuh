@@ -27,6 +27,10 @@ enum : uint32_t {
 };
 
 constexpr uint32_t kFullMask = 0xffffffffu;
+
+__host__ __device__ constexpr uint64_t factorial_u64(int m) {
+  return m <= 1 ? 1ull : static_cast<uint64_t>(m) * factorial_u64(m - 1);
+}
 constexpr uint64_t kEmpty = ~0ull;  // never a packed state: code 0 always occurs
 
 // One displacement group of a generator: child |= ((p >> rshift) << lshift) & mask.
@@ -305,33 +309,65 @@ __host__ __device__ constexpr bool bitmap_kind(int v) {
 
 // ---------------------------------------------------------------------------
 // Packed modular matrices: a rows x cols state of entries in [0, mod), entry
-// j = i * cols + c in bits [bits * j, bits * (j + 1)) of one word.  Generator g
-// is a rows x rows integer matrix (its coefficients are the masks of program
-// terms g * rows^2 ..); the child is (M_g . S) mod mod entry by entry.  The
-// host packs a graph only when no partial sum can leave int64, so the result
-// equals the reference's wrap-then-modulus (graph_definition.py:77-83).
+// j = i * cols + c in bits [bits * j, bits * (j + 1)) of one word, so row i is
+// the contiguous field of cols * bits bits at i * cols * bits.  Generator g's
+// program (terms [tb, te)) lists, output row by output row, either one copy
+// term (the matrix row is a unit vector: the source row moves unchanged) or
+// the row's nonzero coefficients reduced mod m; rows with no term are zero.
+// Term fields: mask = coefficient, rshift = source row, lshift = output row
+// with kMatrixCopy set for a copy.  The host packs a graph only when no
+// partial sum can leave int64, so the result equals the reference's
+// wrap-then-modulus (graph_definition.py:77-83), and every coefficient being
+// reduced keeps the sums non-negative.
 // The bitmap rank is the mixed-radix number of the entries, sum e_j * mod^j,
 // over the whole canonical entry space (the reference's certified bound,
 // workload_geometry.py:21-36).
+constexpr uint32_t kMatrixCopy = 1u << 31;
+constexpr uint32_t kMatrixMaxCols = 8;
+
 struct MatrixAction {
   uint32_t rows, cols, bits, mod;  // mod = 0: permutation terms instead
+  uint32_t recip;                  // floor(2^32 / mod): Barrett reduction of 32-bit sums
+  uint32_t pad;
 };
 
-__device__ __forceinline__ uint64_t apply_matrix(const MatrixAction& a, uint64_t s, const Term* coef) {
+// x mod m.  Below 2^32 by Barrett's method (P. Barrett, CRYPTO 1986): with
+// R = floor(2^32 / m), q = floor(x * R / 2^32) is floor(x / m) or one less, so
+// one conditional subtraction finishes; larger sums take the 64-bit remainder.
+__device__ __forceinline__ uint64_t matrix_reduce(uint64_t x, const MatrixAction& a) {
+  if (x >> 32) return x % a.mod;
+  const uint32_t x32 = static_cast<uint32_t>(x);
+  uint32_t r = x32 - __umulhi(x32, a.recip) * a.mod;
+  if (r >= a.mod) r -= a.mod;
+  return r;
+}
+
+__device__ __forceinline__ uint64_t apply_matrix(const MatrixAction& a, uint64_t s, const Term* t, uint32_t tb,
+                                                 uint32_t te) {
+  const uint32_t row_bits = a.bits * a.cols;
+  const uint64_t row_mask = row_bits >= 64 ? ~0ull : ((1ull << row_bits) - 1);
   const uint64_t field = (1ull << a.bits) - 1;
   uint64_t child = 0;
-  for (uint32_t i = 0; i < a.rows; ++i) {
-    for (uint32_t c = 0; c < a.cols; ++c) {
-      long long acc = 0;
-      for (uint32_t k = 0; k < a.rows; ++k)
-        acc += static_cast<long long>(coef[i * a.rows + k].mask) *
-               static_cast<long long>((s >> (a.bits * (k * a.cols + c))) & field);
-      // Most sums of small coefficients stay in [0, 2^32): a 32-bit remainder.
-      long long v = (acc >= 0 && acc < (1ll << 32)) ? static_cast<long long>(static_cast<uint32_t>(acc) % a.mod)
-                                                   : acc % static_cast<long long>(a.mod);
-      if (v < 0) v += a.mod;
-      child |= static_cast<uint64_t>(v) << (a.bits * (i * a.cols + c));
+  for (uint32_t j = tb; j < te;) {
+    const uint32_t out = t[j].lshift;
+    if (out & kMatrixCopy) {
+      child |= ((s >> (row_bits * t[j].rshift)) & row_mask) << (row_bits * (out & ~kMatrixCopy));
+      ++j;
+      continue;
     }
+    uint64_t acc[kMatrixMaxCols];
+#pragma unroll
+    for (uint32_t c = 0; c < kMatrixMaxCols; ++c) acc[c] = 0;
+    for (; j < te && t[j].lshift == out; ++j) {
+      const uint64_t coef = t[j].mask;
+      const uint64_t src = s >> (row_bits * t[j].rshift);
+#pragma unroll
+      for (uint32_t c = 0; c < kMatrixMaxCols; ++c)
+        if (c < a.cols) acc[c] += coef * ((src >> (a.bits * c)) & field);
+    }
+#pragma unroll
+    for (uint32_t c = 0; c < kMatrixMaxCols; ++c)
+      if (c < a.cols) child |= matrix_reduce(acc[c], a) << (row_bits * out + a.bits * c);
   }
   return child;
 }

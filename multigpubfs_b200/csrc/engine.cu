@@ -314,7 +314,7 @@ void Graph::analyse() {
       // of |coefficients| times (m - 1) inside int64.
       uint32_t eb = 1;
       while ((1ull << eb) < m) ++eb;
-      bool fits = canonical && static_cast<uint64_t>(n) * eb < 64;
+      bool fits = canonical && static_cast<uint64_t>(n) * eb < 64 && cols <= kMatrixMaxCols;
       for (uint32_t k = 0; k < gens && fits; ++k)
         for (uint32_t i = 0; i < rows && fits; ++i) {
           unsigned __int128 sum = 0;
@@ -396,8 +396,19 @@ static std::vector<int64_t> mat_mul_mod(const std::vector<int64_t>& a, const std
 void Graph::build_matrix_program() {
   const uint32_t r = rows, m = moduli[0];
   for (uint32_t k = 0; k < gens; ++k) {
-    for (uint32_t j = 0; j < r * r; ++j)
-      terms.push_back(Term{static_cast<unsigned long long>(matrices[static_cast<size_t>(k) * r * r + j]), 0u, 0u});
+    for (uint32_t i = 0; i < r; ++i) {
+      std::vector<std::pair<uint32_t, uint64_t>> nz;
+      for (uint32_t j = 0; j < r; ++j) {
+        int64_t v = matrices[static_cast<size_t>(k) * r * r + i * r + j] % static_cast<int64_t>(m);
+        if (v < 0) v += m;
+        if (v) nz.emplace_back(j, static_cast<uint64_t>(v));
+      }
+      if (nz.size() == 1 && nz[0].second == 1) {
+        terms.push_back(Term{1ull, nz[0].first, i | kMatrixCopy});
+      } else {
+        for (auto& z : nz) terms.push_back(Term{z.second, z.first, i});
+      }
+    }
     term_begin.push_back(static_cast<uint32_t>(terms.size()));
   }
   std::vector<int64_t> eye(static_cast<size_t>(r) * r, 0);
@@ -789,16 +800,30 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
       if (local) dedup = MGBFS2_DEDUP_GROUPED;
       else if (n * (n - 1) <= kMaxShards) dedup = MGBFS2_DEDUP_BUCKET;
     }
+    // A radix bitmap larger than L2 routes by its top entry (m shards of
+    // m^(E-1) bits each).
+    if (visited == MGBFS2_VISITED_BITMAP && packed_matrix && bitmap_bytes > (64ull << 20) &&
+        moduli[0] <= kMaxShards)
+      dedup = MGBFS2_DEDUP_BUCKET;
   }
   if (visited != MGBFS2_VISITED_BITMAP && dedup == MGBFS2_DEDUP_WARP) dedup = MGBFS2_DEDUP_ATOMIC;
   const bool hash_routed =
       dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_HASH && packed && !packed_matrix;
+  const bool radix_routed = dedup == MGBFS2_DEDUP_BUCKET && visited == MGBFS2_VISITED_BITMAP && packed_matrix &&
+                            moduli[0] <= kMaxShards;
   if ((dedup == MGBFS2_DEDUP_BUCKET || dedup == MGBFS2_DEDUP_GROUPED) &&
-      !(visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product) && !hash_routed)
+      !(visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product) && !hash_routed && !radix_routed)
     return MGBFS2_UNSUPPORTED;
   // Sort-unique tiles hold kSortTile children: at least 16 parents per tile.
   if (dedup == MGBFS2_DEDUP_SORT && (!packed || packed_matrix || gens > kSortTile / 16)) return MGBFS2_UNSUPPORTED;
-  if (dedup == MGBFS2_DEDUP_BUCKET && !hash_routed) {
+  if (radix_routed) {
+    bucket_prefix = 1;
+    bucket_shards = moduli[0];
+    p.shards = bucket_shards;
+    bucket_margin = r.bucket_margin == 0 ? 4096 : (r.bucket_margin == UINT32_MAX ? 0 : r.bucket_margin);
+    bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
+  }
+  if (dedup == MGBFS2_DEDUP_BUCKET && !hash_routed && !radix_routed) {
     // Shards = states sharing their first K symbols: N!/(N-K)! shards whose
     // bitmap slices hold (N-K)! bits.  Default: the smallest K (1 or 2) whose
     // slice is at most 8 MiB, so the slices the resident accept blocks work
@@ -1315,6 +1340,7 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   rp.shard_cap = meta + kMaxShards;
   rp.shard_count = meta + 2 * kMaxShards;
   rp.control = p.control;
+  rp.mat = p.mat;
   if (visit_kind() == V_HASH) {
     uint32_t shift = 0;
     while ((1ull << shift) < table_slots) ++shift;
@@ -1345,6 +1371,7 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   ap.table_mask = p.table_mask;
   ap.key_mask = key_mask;
   ap.probe_limit = p.probe_limit;
+  ap.mat = p.mat;
   reinterpret_cast<AcceptFn>(const_cast<void*>(accept_fn))<<<grid_for(accept_fn, 0, UINT32_MAX), kBlock, 0, stream>>>(ap);
   ++launches;
   MG_CHECK(cudaGetLastError());
@@ -1649,13 +1676,17 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements);
   if (!fn) return MGBFS2_UNSUPPORTED;
   // Bucketed layers for large frontiers; small layers use the fused kernel.
-  const bool bucketed = plan.dedup == MGBFS2_DEDUP_BUCKET && (visit == V_LEHMER || visit == V_HASH);
+  const bool bucketed =
+      plan.dedup == MGBFS2_DEDUP_BUCKET && (visit == V_LEHMER || visit == V_HASH || visit == V_RADIX);
   RouteFn route_fn = nullptr;
   AcceptFn accept_fn = nullptr;
   if (bucketed) {
     if (visit == V_HASH) {
       route_fn = route_lehmer<0, 0>;
       accept_fn = accept_hash;
+    } else if (visit == V_RADIX) {
+      route_fn = route_lehmer<kRadixDomain, 1>;
+      accept_fn = accept_lehmer<kRadixDomain, 1>;
     } else {
       pick_bucket(elements, bucket_prefix, &route_fn, &accept_fn);
     }

@@ -90,7 +90,8 @@ struct Graph {
   // expanded by the fused kernels (MatrixAction); others take the wide path.
   bool packed_matrix = false;
   MatrixAction matrix_action() const {
-    return packed_matrix ? MatrixAction{rows, cols, bits, moduli[0]} : MatrixAction{0, 0, 0, 0};
+    if (!packed_matrix) return MatrixAction{0, 0, 0, 0, 0, 0};
+    return MatrixAction{rows, cols, bits, moduli[0], static_cast<uint32_t>((1ull << 32) / moduli[0]), 0};
   }
   uint32_t bits = 4, distinct = 0;
   std::vector<int64_t> labels;     // code -> label

@@ -42,7 +42,6 @@ constexpr uint32_t kGroupChunk = 4096;  // parents per work item unless the plan
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
 static_assert(kGroupStage >= kBlock * 4, "a pass stages up to kBlock * ppt winners, ppt <= 4");
 
-constexpr uint64_t factorial_u64(int m) { return m <= 1 ? 1ull : static_cast<uint64_t>(m) * factorial_u64(m - 1); }
 
 struct GroupedParams {
   const unsigned long long* frontier;

@@ -76,7 +76,7 @@ struct ExpandParams {
 // program): permutation displacement terms, or a modular matrix product.
 __device__ __forceinline__ uint64_t apply_action(const ExpandParams& p, uint64_t s, const Term* terms, uint32_t tb,
                                                  uint32_t te) {
-  return p.mat.mod ? apply_matrix(p.mat, s, terms + tb) : apply_terms(s, terms, tb, te);
+  return p.mat.mod ? apply_matrix(p.mat, s, terms, tb, te) : apply_terms(s, terms, tb, te);
 }
 
 // Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the

@@ -8,6 +8,10 @@
   inverse-closed variant adds every generator's inverse.
 * Planner instances: S12 with 2-4 seeded random generators plus inverses
   (default_rng(20261204 + i)).
+* GL(2, p): 2x2 int64 matrices mod a prime p from the identity under the
+  elementary transvections [[1,1],[0,1]], [[1,0],[1,1]], diag(g, 1) for the
+  least primitive root g, and their inverses; the orbit is the whole group,
+  (p^2 - 1)(p^2 - p) states, against the certified entry-space bound p^4.
 """
 from __future__ import annotations
 
@@ -72,3 +76,25 @@ def planner_instance(i, n=12, seed_base=20261204):
     k = int(rng.choice([2, 3, 4]))
     gens = with_inverses([[int(x) for x in rng.permutation(n)] for _ in range(k)])
     return permutation_graph(gens, list(range(n)), name=f"planner-{i}")
+
+
+def primitive_root(p):
+    """Least primitive root of the prime p."""
+    factors = [q for q in range(2, p) if (p - 1) % q == 0 and all(q % d for d in range(2, int(q ** 0.5) + 1))]
+    return next(r for r in range(2, p) if all(pow(r, (p - 1) // q, p) != 1 for q in factors))
+
+
+def gl2_generators(p):
+    """(matrix, modulus) pairs of GL(2, p) (row-major 2x2)."""
+    g = primitive_root(p)
+    gi = pow(g, p - 2, p)
+    mats = [[1, 1, 0, 1], [1, 0, 1, 1], [1, p - 1, 0, 1], [1, 0, p - 1, 1], [g, 0, 0, 1], [gi, 0, 0, 1]]
+    return [(m, p) for m in mats]
+
+
+def gl2_graph(p):
+    gens = gl2_generators(p)
+    return {"schema": 2, "name": f"gl2-{p}", "generator_names": [str(i) for i in range(len(gens))],
+            "action": {"kind": "matrix", "rows": 2, "cols": 2,
+                       "generators": [{"matrix": list(m), "modulo": mod} for m, mod in gens]},
+            "start": [1, 0, 0, 1], "expected_max_unique_states": None}

@@ -40,12 +40,8 @@ def test_sl2_orbit_is_the_group_order(p):
 
 def _gl2(p):
     from multigpubfs_b200 import GraphDefinition
-    g = next(r for r in range(2, p) if all(pow(r, (p - 1) // q, p) != 1
-                                           for q in range(2, p) if (p - 1) % q == 0 and
-                                           all(q % d for d in range(2, int(q ** 0.5) + 1))))
-    gi = pow(g, p - 2, p)
-    gens = [[1, 1, 0, 1], [1, 0, 1, 1], [1, p - 1, 0, 1], [1, 0, p - 1, 1], [g, 0, 0, 1], [gi, 0, 0, 1]]
-    return GraphDefinition.matrix(2, 2, [(m, p) for m in gens], [1, 0, 0, 1])
+    from multigpubfs_b200.workloads import gl2_graph
+    return GraphDefinition.from_dict(gl2_graph(p))
 
 
 @pytest.mark.parametrize("visited", ["bitmap", "hash", "auto"])
@@ -103,3 +99,29 @@ def test_unpackable_matrices_stay_on_the_wide_path():
         layer = nxt
         expect.append(len(nxt))
     assert r.layer_sizes == expect
+
+
+@pytest.mark.parametrize("case", ["sl2_mod31", "sl2_mod101"])
+def test_routed_radix_layers_match_the_reference(case):
+    """Every layer routed by the top entry (m shards of the radix bitmap),
+    then claimed shard by shard."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    fx = golden("matrix_groups.json")["cases"][case]
+    with NativeGraph(GraphDefinition.from_dict(fx["graph"])) as e:
+        info = e.plan(visited="bitmap", dedup="bucket", bucket_min_work=1)
+        for _ in range(3):
+            assert e.run().layer_sizes == fx["layers"]
+    assert info["dedup"] == "bucket" and info["shards"] == int(case.split("mod")[1])
+
+
+def test_large_radix_bitmaps_route_by_default():
+    """GL(2,211): 1.97e9 states, a 236 MB radix bitmap (above 64 MiB, so the
+    planner routes its large layers by the top entry)."""
+    from multigpubfs_b200.engine import NativeGraph
+    p = 211
+    with NativeGraph(_gl2(p)) as e:
+        info = e.plan()
+        r = e.run()
+    assert info["visited"] == "bitmap" and info["dedup"] == "bucket" and info["shards"] == p
+    assert r.complete and r.states == (p * p - 1) * (p * p - p)
