@@ -78,7 +78,7 @@ WORKLOADS = {
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
-    "gl2-211-matrix": dict(matrix_p=211, visited="bitmap", dedup="atomic",
+    "gl2-211-matrix": dict(matrix_p=211, visited="bitmap", dedup="auto",
                            desc="GL(2,211) on 2x2 int64 matrices mod 211 from the identity, 6 generators: "
                                 "1,972,681,200 states, 99.5 % of the certified entry-space bound 211^4; packed "
                                 "8-bit entries, mixed-radix bitmap"),

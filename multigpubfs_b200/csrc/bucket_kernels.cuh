@@ -43,7 +43,7 @@ constexpr uint32_t kAcceptChunk = 4096;               // bucket entries per acce
 // Template N of the route / accept kernels for packed modular matrices: shard
 // = the top entry (the most significant digit of the radix rank), so shard s
 // owns the rank range [s * m^(E-1), (s + 1) * m^(E-1)).
-constexpr int kRadixDomain = -1;
+constexpr int kRadixDomain = kMatrixN;
 
 struct RouteParams {
   const unsigned long long* frontier;
@@ -190,7 +190,9 @@ __global__ void __launch_bounds__(kBlock, 3) route_lehmer(RouteParams p) {
         for (int k = 0; k < 4; ++k) {
           if (k >= static_cast<int>(p.ppt)) break;
           if (val[k] && g != skip[k]) {
-            const uint64_t c = p.mat.mod ? apply_matrix(p.mat, par[k], terms, tb, te) : apply_terms(par[k], terms, tb, te);
+            uint64_t c;
+            if constexpr (N == kRadixDomain) c = apply_matrix(p.mat, par[k], terms, tb, te);
+            else c = apply_terms(par[k], terms, tb, te);
             const uint32_t s = route_shard<N, K>(p, c);
             const uint32_t slot = live * kBlock + tid;
             sm.state[slot] = c | gtag;
@@ -311,8 +313,9 @@ __global__ void __launch_bounds__(kBlock) count_lehmer(RouteParams p) {
     const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
     for (uint32_t g = 0; g < p.gens; ++g)
       if (g != skip) {
-        const uint64_t c = p.mat.mod ? apply_matrix(p.mat, w, terms, tbegin[g], tbegin[g + 1])
-                                     : apply_terms(w, terms, tbegin[g], tbegin[g + 1]);
+        uint64_t c;
+        if constexpr (N == kRadixDomain) c = apply_matrix(p.mat, w, terms, tbegin[g], tbegin[g + 1]);
+        else c = apply_terms(w, terms, tbegin[g], tbegin[g + 1]);
         atomicAdd(&hist[route_shard<N, K>(p, c)], 1u);
       }
   }

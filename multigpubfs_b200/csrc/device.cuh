@@ -323,6 +323,9 @@ __host__ __device__ constexpr bool bitmap_kind(int v) {
 // over the whole canonical entry space (the reference's certified bound,
 // workload_geometry.py:21-36).
 constexpr uint32_t kMatrixCopy = 1u << 31;
+// Template N of the fused, route and count kernels for packed matrices: the
+// action is compiled in, so permutation kernels carry none of its code.
+constexpr int kMatrixN = -1;
 constexpr uint32_t kMatrixMaxCols = 8;
 
 struct MatrixAction {

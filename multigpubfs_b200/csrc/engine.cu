@@ -987,7 +987,21 @@ static ExpandFn pick_sorted(int visit, uint32_t n) {
   }
 }
 
-static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
+static ExpandFn pick_expand(int visit, bool warp, uint32_t n, bool matrix) {
+  if (matrix) {
+    switch (visit) {
+      case V_RADIX:
+        return warp ? expand_packed<V_RADIX, kMatrixN, true> : expand_packed<V_RADIX, kMatrixN, false>;
+      case V_HASH:
+        return expand_packed<V_HASH, kMatrixN, false>;
+      case V_HASHQ:
+        return expand_packed<V_HASHQ, kMatrixN, false>;
+      case V_HASH3:
+        return expand_packed<V_HASH3, kMatrixN, false>;
+      default:
+        return nullptr;
+    }
+  }
   switch (visit) {
     case V_LEHMER:
       return warp ? pick_lehmer<V_LEHMER, true>(n) : pick_lehmer<V_LEHMER, false>(n);
@@ -995,8 +1009,6 @@ static ExpandFn pick_expand(int visit, bool warp, uint32_t n) {
       return warp ? expand_packed<V_MULTISET, 0, true> : expand_packed<V_MULTISET, 0, false>;
     case V_PRODUCT:
       return warp ? expand_packed<V_PRODUCT, 0, true> : expand_packed<V_PRODUCT, 0, false>;
-    case V_RADIX:
-      return warp ? expand_packed<V_RADIX, 0, true> : expand_packed<V_RADIX, 0, false>;
     case V_HASH:
       return expand_packed<V_HASH, 0, false>;
     case V_HASHQ:
@@ -1673,7 +1685,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   const int visit = visit_kind();
   const bool warp = plan.dedup == MGBFS2_DEDUP_WARP;
   const bool sorted = plan.dedup == MGBFS2_DEDUP_SORT;
-  ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements);
+  ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements, packed_matrix);
   if (!fn) return MGBFS2_UNSUPPORTED;
   // Bucketed layers for large frontiers; small layers use the fused kernel.
   const bool bucketed =

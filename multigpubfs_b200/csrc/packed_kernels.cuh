@@ -73,10 +73,16 @@ struct ExpandParams {
 };
 
 // The child of packed state s under generator g (terms [tb, te) of the
-// program): permutation displacement terms, or a modular matrix product.
+// program): permutation displacement terms, or (N = kMatrixN) a modular
+// matrix product.
+template <int N>
 __device__ __forceinline__ uint64_t apply_action(const ExpandParams& p, uint64_t s, const Term* terms, uint32_t tb,
                                                  uint32_t te) {
-  return p.mat.mod ? apply_matrix(p.mat, s, terms, tb, te) : apply_terms(s, terms, tb, te);
+  if constexpr (N == kMatrixN) {
+    return apply_matrix(p.mat, s, terms, tb, te);
+  } else {
+    return apply_terms(s, terms, tb, te);
+  }
 }
 
 // Visited test-and-set of candidate c.  Must be reached by all 32 lanes (the
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
   #pragma unroll
           for (int k = 0; k < 4; ++k) {
             live[k] = k < static_cast<int>(p.ppt) && val[k] && g != skip[k];
-            ch[k] = live[k] ? apply_action(p, par[k], terms, tb, te) : 0;
+            ch[k] = live[k] ? apply_action<N>(p, par[k], terms, tb, te) : 0;
             first[k] = live[k] ? qhash_first(p.q, ch[k]) : 0u;
           }
   #pragma unroll
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
           for (int k = 0; k < 4; ++k) {
             if (k >= static_cast<int>(p.ppt)) break;
             const bool v = val[k] && g != skip[k];
-            const uint64_t c = v ? apply_action(p, par[k], terms, tb, te) : 0;
+            const uint64_t c = v ? apply_action<N>(p, par[k], terms, tb, te) : 0;
             const bool won = claim<V, N, WARP>(p, c, v);
             const unsigned m = __ballot_sync(kFullMask, won);
             if (m) {
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(kSortThreads) expand_sorted(ExpandParams p) {
       const uint32_t skip = tag ? inverse[tag - 1] : 0xffffffffu;
       for (uint32_t g = 0; g < p.gens; ++g) {
         if (g == skip) continue;
-        const uint64_t c = apply_action(p, par, terms, begin[g], begin[g + 1]);
+        const uint64_t c = apply_action<N>(p, par, terms, begin[g], begin[g + 1]);
         s.keys[g * per_tile + j] = c | (p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull);
       }
     }
