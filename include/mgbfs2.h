@@ -98,14 +98,17 @@ typedef struct {
    * memory allow).  They change speed only. */
   uint32_t group_chunk;
   uint32_t blocks_per_sm;
-  uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 4 up to
-                                  4 generators, else 2) */
+  uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 2 for
+                                  quotient-slot hash layers, else 4 up to 4 generators and 2 above) */
   uint32_t reserved;
 } mgbfs2_plan_request;
 
-/* Inverse-closed packed graphs tag every frontier state with the generator
- * that produced it and skip that generator's inverse (the edge back to the
- * previous layer) without a visited test; this option turns that off. */
+/* Packed graphs tag every frontier state with the generator that produced it
+ * and skip that generator's inverse (the edge back to the previous layer)
+ * without a visited test, when there are spare bits above the state and the
+ * generators come in inverse pairs (permutations: an inverse-closed set;
+ * modular matrices: any generator whose inverse mod m is in the set); this
+ * option turns that off. */
 #define MGBFS2_OPTION_NO_PARENT_SKIP 1u
 /* Plans whose frontier buffers and visited set are sized up front (the fused
  * bitmap or all-visited hash layers, no limits or callback) run the whole BFS
@@ -126,13 +129,15 @@ typedef struct {
 
 typedef struct {
   uint32_t visited, dedup;
-  uint32_t packed;          /* 1 = states are one packed uint64 word */
-  uint32_t bits_per_symbol; /* packed symbol width */
+  uint32_t packed;          /* 1 = states are one packed uint64 word (permutation codes, or the entries of
+                               a modular matrix) */
+  uint32_t bits_per_symbol; /* packed symbol or matrix-entry width */
   uint32_t key_words;       /* uint64 words per state */
   uint32_t history_layers;  /* 1 = all visited retained, 3 = three-layer banks */
   uint64_t capacity;        /* frontier capacity bound (states) */
   uint64_t table_slots;     /* hash slots (all-visited table) */
-  uint64_t bitmap_bits;     /* rank-domain size of the bitmap */
+  uint64_t bitmap_bits;     /* rank-domain size of the bitmap: n!, the multinomial, the product of the
+                               position components' domains, or m^entries for modular matrices */
   uint64_t device_bytes;    /* fixed device allocation of the plan */
   uint64_t state_bound;     /* certified orbit bound, 0 = unknown */
   uint32_t shards, block;
