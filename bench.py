@@ -78,6 +78,9 @@ WORKLOADS = {
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
                          desc="S11 LRX full BFS (39,916,800 states), exact-key open-addressing hash of all visited states"),
+    "s10-coxeter": dict(n=10, gens=coxeter(10), visited="bitmap", dedup="auto",
+                        desc="S10 adjacent transpositions full BFS (3,628,800 states), Lehmer bitmap; beside it the "
+                             "reference's own GPU BFS of the same graph (gpu/cayley_bfs.cu) on the same B200"),
     "gl2-211-matrix": dict(matrix_p=211, visited="bitmap", dedup="auto",
                            desc="GL(2,211) on 2x2 int64 matrices mod 211 from the identity, 6 generators: "
                                 "1,972,681,200 states, 99.5 % of the certified entry-space bound 211^4; packed "
@@ -106,7 +109,7 @@ def golden(name):
 def expected_layers(name, n):
     if name == "s13-lrx":
         return golden("lrx13_layers.json")["layers"]
-    if name == "s13-coxeter":
+    if name in ("s13-coxeter", "s10-coxeter"):
         sizes = [1]
         for i in range(1, n + 1):
             out, window = [], 0
@@ -687,11 +690,34 @@ def bench_single(args, rank, world, local):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_sample(args.workload)
+        if args.workload == "s10-coxeter":
+            line["same_box_reference_gpu"] = reference_gpu_leg(w["n"], expect, succ, args)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def reference_gpu_leg(n, expect, succ, args):
+    """The reference's own GPU BFS of S_n under adjacent transpositions
+    (gpu/cayley_bfs.cu, built into oracle/_ref), timed on this B200: its
+    warp-aggregated variant, one host-driven step per layer, tables checked."""
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libmgbfs_ref_gpu.so not built (reference sources absent at build)"}
+    with ref_gpu.CayleyBfs(n) as ref:
+        for _ in range(args.warmup):
+            sizes, _, _ = ref.run(1, 0)
+            assert sizes == expect, "reference GPU table differs"
+        runs = [ref.run(1, 0) for _ in range(args.steps)]
+    assert all(r[0] == expect for r in runs)
+    kernel_s = sum(r[1] for r in runs) / len(runs) * 1e-3
+    wall_s = sum(r[2] for r in runs) / len(runs)
+    return {"value": succ / wall_s, "unit": "successors/s", "kernel_only_value": succ / kernel_s,
+            "ms_per_bfs": wall_s * 1e3, "kernel_ms_per_bfs": kernel_s * 1e3,
+            "code": "reference gpu/cayley_bfs.cu expand_kernel (warp-aggregated variant, one step per layer), "
+                    "compiled for sm_100a from the reference sources"}
 
 
 def bench_sharded(args, rank, world, local):

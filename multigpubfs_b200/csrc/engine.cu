@@ -949,12 +949,18 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
 
 using ExpandFn = void (*)(ExpandParams);
 
-template <int V, bool W>
+// Bitmap graphs with at least this many generators take the kernels with the
+// candidate-parallel small-layer mode (S10 Coxeter, 9 generators: 1.38 ->
+// 1.10 ms per BFS); with fewer a thread's generators are few enough that the
+// mode does not pay (S11 LRX, 3 generators: 2.15 -> 2.31 ms with it).
+constexpr uint32_t kCandidateMinGens = 5;
+
+template <int V, bool W, bool C>
 static ExpandFn pick_lehmer(uint32_t n) {
   switch (n) {
 #define MG_CASE(K) \
   case K:          \
-    return expand_packed<V, K, W>;
+    return expand_packed<V, K, W, C>;
     MG_CASE(2) MG_CASE(3) MG_CASE(4) MG_CASE(5) MG_CASE(6) MG_CASE(7) MG_CASE(8) MG_CASE(9) MG_CASE(10)
     MG_CASE(11) MG_CASE(12) MG_CASE(13) MG_CASE(14) MG_CASE(15) MG_CASE(16)
 #undef MG_CASE
@@ -987,34 +993,39 @@ static ExpandFn pick_sorted(int visit, uint32_t n) {
   }
 }
 
-static ExpandFn pick_expand(int visit, bool warp, uint32_t n, bool matrix) {
+// Bitmap kernels with many generators (cand) carry the candidate-parallel
+// mode for small layers; hash and matrix kernels always do.
+static ExpandFn pick_expand(int visit, bool warp, uint32_t n, bool matrix, bool cand) {
   if (matrix) {
     switch (visit) {
       case V_RADIX:
-        return warp ? expand_packed<V_RADIX, kMatrixN, true> : expand_packed<V_RADIX, kMatrixN, false>;
+        return warp ? expand_packed<V_RADIX, kMatrixN, true, true> : expand_packed<V_RADIX, kMatrixN, false, true>;
       case V_HASH:
-        return expand_packed<V_HASH, kMatrixN, false>;
+        return expand_packed<V_HASH, kMatrixN, false, true>;
       case V_HASHQ:
-        return expand_packed<V_HASHQ, kMatrixN, false>;
+        return expand_packed<V_HASHQ, kMatrixN, false, true>;
       case V_HASH3:
-        return expand_packed<V_HASH3, kMatrixN, false>;
+        return expand_packed<V_HASH3, kMatrixN, false, true>;
       default:
         return nullptr;
     }
   }
   switch (visit) {
     case V_LEHMER:
-      return warp ? pick_lehmer<V_LEHMER, true>(n) : pick_lehmer<V_LEHMER, false>(n);
+      if (cand) return warp ? pick_lehmer<V_LEHMER, true, true>(n) : pick_lehmer<V_LEHMER, false, true>(n);
+      return warp ? pick_lehmer<V_LEHMER, true, false>(n) : pick_lehmer<V_LEHMER, false, false>(n);
     case V_MULTISET:
-      return warp ? expand_packed<V_MULTISET, 0, true> : expand_packed<V_MULTISET, 0, false>;
+      if (cand) return warp ? expand_packed<V_MULTISET, 0, true, true> : expand_packed<V_MULTISET, 0, false, true>;
+      return warp ? expand_packed<V_MULTISET, 0, true, false> : expand_packed<V_MULTISET, 0, false, false>;
     case V_PRODUCT:
-      return warp ? expand_packed<V_PRODUCT, 0, true> : expand_packed<V_PRODUCT, 0, false>;
+      if (cand) return warp ? expand_packed<V_PRODUCT, 0, true, true> : expand_packed<V_PRODUCT, 0, false, true>;
+      return warp ? expand_packed<V_PRODUCT, 0, true, false> : expand_packed<V_PRODUCT, 0, false, false>;
     case V_HASH:
-      return expand_packed<V_HASH, 0, false>;
+      return expand_packed<V_HASH, 0, false, true>;
     case V_HASHQ:
-      return expand_packed<V_HASHQ, 0, false>;
+      return expand_packed<V_HASHQ, 0, false, true>;
     default:
-      return expand_packed<V_HASH3, 0, false>;
+      return expand_packed<V_HASH3, 0, false, true>;
   }
 }
 
@@ -1685,7 +1696,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   const int visit = visit_kind();
   const bool warp = plan.dedup == MGBFS2_DEDUP_WARP;
   const bool sorted = plan.dedup == MGBFS2_DEDUP_SORT;
-  ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements, packed_matrix);
+  ExpandFn fn = sorted ? pick_sorted(visit, elements) : pick_expand(visit, warp, elements, packed_matrix, gens >= kCandidateMinGens);
   if (!fn) return MGBFS2_UNSUPPORTED;
   // Bucketed layers for large frontiers; small layers use the fused kernel.
   const bool bucketed =

@@ -15,6 +15,12 @@ namespace mgbfs2 {
 
 
 constexpr uint32_t kOutCap = 4096;  // shared-memory winners per block (32 KiB)
+// Layers of at most this many (parent, generator) candidates per thread of the
+// grid run candidate-parallel in the expand_packed<..., CAND = true> kernels
+// (measured: 4 waves beat 1 and 2 on S10 Coxeter and S11 LRX hash).  The
+// mode's code is compiled only where the host selects it: present in a kernel
+// it slowed the parent path of the Lehmer kernels (S12 LRX 17.2 -> 22.3 ms).
+constexpr unsigned long long kCandidateWaves = 4;
 // The quotient-hash kernel runs six blocks per SM (its registers allow six)
 // with a 16 KB stage, so that 6 x 17 KB stays in the 132 KB shared-memory
 // configuration and leaves about 100 KB of L1 (a 32 KB stage pushed it to the
@@ -202,7 +208,7 @@ __device__ __forceinline__ uint32_t loop_step(LoopState* s, Control* c) {
   return stop;
 }
 
-template <int V, int N, bool WARP>
+template <int V, int N, bool WARP, bool CAND>
 __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) expand_packed(ExpandParams p) {
   constexpr uint32_t out_cap = V == V_HASHQ ? kOutCapHashQ : kOutCap;
   extern __shared__ __align__(16) unsigned char program_smem[];
@@ -234,7 +240,55 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
     // block flushes once per tile and skips the room check (two barriers)
     // after every generator.
     const bool one_flush = tile * p.gens <= out_cap;
-    for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    // A small layer runs one thread per (parent, generator) candidate
+    // instead (CAND kernels), so its generators are tested in parallel rather
+    // than one after another by each thread: at most kCandidateWaves
+    // candidates per thread of the grid (uniform across the grid; counted in
+    // 32 bits).
+    const bool by_candidate =
+        CAND && count * p.gens <= kCandidateWaves * static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+    if (by_candidate) {
+      const uint32_t candidates = static_cast<uint32_t>(count * p.gens);
+      const uint32_t ctiles = (candidates + blockDim.x - 1) / blockDim.x;
+      for (uint32_t t = blockIdx.x; t < ctiles; t += gridDim.x) {
+        const uint32_t q = t * blockDim.x + threadIdx.x;
+        bool v = q < candidates;
+        uint64_t c = 0;
+        unsigned long long gtag = 0;
+        if (v) {
+          const uint32_t pi = q / p.gens, g = q - pi * p.gens;
+          const uint64_t par = frontier[pi];
+          const uint32_t tag = p.gen_shift ? static_cast<uint32_t>(par >> p.gen_shift) : 0u;
+          if (tag && inverse[tag - 1] == g) {
+            v = false;
+          } else {
+            c = apply_action<N>(p, par, terms, begin[g], begin[g + 1]);
+            gtag = p.gen_shift ? static_cast<unsigned long long>(g + 1) << p.gen_shift : 0ull;
+          }
+        }
+        bool won;
+        if constexpr (V == V_HASHQ) {
+          won = false;
+          if (v) {
+            const int rc = qhash_insert(p.q, c);
+            if (rc < 0) raise_error(&p.control->error, ERR_TABLE_FULL);
+            won = rc == 1;
+          }
+        } else {
+          won = claim<V, N, WARP>(p, c, v);
+        }
+        const unsigned m = __ballot_sync(kFullMask, won);
+        if (m) {
+          const int leader = __ffs(m) - 1;
+          uint32_t wb = 0;
+          if (static_cast<int>(lane) == leader) wb = atomicAdd(&out_count, static_cast<uint32_t>(__popc(m)));
+          wb = __shfl_sync(kFullMask, wb, leader);
+          if (won) out[wb + __popc(m & lanemask_lt())] = c | gtag;
+        }
+        flush_block(p, next, out, &out_count, &out_base);
+      }
+    }
+    for (unsigned long long t = by_candidate ? tiles : blockIdx.x; t < tiles; t += gridDim.x) {
       const unsigned long long base = t * tile;
       uint64_t par[4];
       bool val[4];
