@@ -188,3 +188,13 @@ def test_matrix_oracle_matches_the_reference_sl2_table():
     fx = golden("matrix_groups.json")["cases"]["sl2_mod31"]
     assert G.layer_sizes(fx["graph"]) == fx["layers"]
     assert sum(fx["layers"]) == 31 * (31 * 31 - 1)
+
+
+@pytest.mark.parametrize("p", [5, 7, 11])
+def test_gl2_workload_is_the_whole_group(p):
+    """GL(2, p) from the identity under the workload's six generators: the
+    oracle's orbit is (p^2 - 1)(p^2 - p), the certified bound p^4 above it."""
+    from multigpubfs_b200 import workloads
+    g = workloads.gl2_graph(p)
+    assert workloads.primitive_root(p) == min(r for r in range(2, p) if len({pow(r, k, p) for k in range(1, p)}) == p - 1)
+    assert sum(G.layer_sizes(g)) == (p * p - 1) * (p * p - p) < p ** 4
