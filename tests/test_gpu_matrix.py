@@ -44,7 +44,7 @@ def _gl2(p):
     return GraphDefinition.from_dict(gl2_graph(p))
 
 
-@pytest.mark.parametrize("visited", ["bitmap", "hash", "auto"])
+@pytest.mark.parametrize("visited", ["bitmap", "hash", "hash3", "auto"])
 def test_packed_matrices_match_the_reference_on_every_visited_set(visited):
     from multigpubfs_b200 import GraphDefinition
     from multigpubfs_b200.engine import NativeGraph
@@ -125,3 +125,21 @@ def test_large_radix_bitmaps_route_by_default():
         r = e.run()
     assert info["visited"] == "bitmap" and info["dedup"] == "bucket" and info["shards"] == p
     assert r.complete and r.states == (p * p - 1) * (p * p - p)
+
+
+def test_packed_matrix_checkpoint_resumes_exactly(tmp_path):
+    """A radix-bitmap BFS stopped at a layer limit, checkpointed and resumed in
+    a fresh handle ends with the reference's table."""
+    from multigpubfs_b200 import GraphDefinition, archive
+    from multigpubfs_b200.engine import NativeGraph
+    fx = golden("matrix_groups.json")["cases"]["sl2_mod101"]
+    g = GraphDefinition.from_dict(fx["graph"])
+    with NativeGraph(g) as e:
+        e.plan(visited="bitmap")
+        part = e.run(max_layers=12)
+        assert part.layer_sizes == fx["layers"][:12]
+        archive.save_checkpoint(e, tmp_path / "ck", part)
+    with NativeGraph(g) as e:
+        e.plan(visited="bitmap")
+        archive.load_checkpoint(e, tmp_path / "ck")
+        assert e.run().layer_sizes == fx["layers"]
