@@ -1006,8 +1006,8 @@ int mgbfs2_batch_run(mgbfs2_batch* batch, const mgbfs2_batch_options* options, m
   if (tile != kBatchBlock && tile != 2 * kBatchBlock && tile != 4 * kBatchBlock) return MGBFS2_INVALID_ARGUMENT;
   const uint32_t tile_ppt = tile / kBatchBlock;
   MG_CHECK_BATCH(cudaSetDevice(b->device));
-  size_t free_bytes = 0, total_bytes = 0;
-  MG_CHECK_BATCH(cudaMemGetInfo(&free_bytes, &total_bytes));
+  size_t free_bytes = 0;
+  if (int frc = device_free_bytes(b->device, &free_bytes)) return frc;
   free_bytes += pool_idle_bytes(b->device) + device_cache_bytes(b->device) + b->arena.bytes;
   const uint64_t reserve = o.reserve_bytes ? o.reserve_bytes : (2ull << 30);
   uint64_t budget = o.memory_bytes ? o.memory_bytes : (free_bytes > reserve ? free_bytes - reserve : 0);

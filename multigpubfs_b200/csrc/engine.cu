@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -708,6 +709,97 @@ int retain_pool_memory(int device) {
 }
 
 // Bytes the pool holds reserved but unused: allocatable without new mappings.
+// Free device memory, as cudaMemGetInfo reports it.  On shared hosts the call
+// itself sometimes takes tens of milliseconds (44-98 ms seen in a sequence of
+// 30 plans), which a plan per handle would pay at random.  So the first query
+// of a device is synchronous; afterwards plans read the last answer, corrected
+// by the change in this process's pool reservation since it was taken (the
+// memory the library itself allocated or gave back in between), and an answer
+// older than two seconds is refreshed by a background thread.
+namespace {
+
+struct FreeMemory {
+  std::chrono::steady_clock::time_point when;
+  size_t free = 0;
+  uint64_t reserved = 0;
+  bool valid = false;
+};
+
+std::mutex free_memory_lock;
+std::map<int, FreeMemory> free_memory;
+bool free_memory_refreshing = false;  // one refresh at a time, any device
+
+uint64_t pool_reserved_bytes(int device) {
+  cudaMemPool_t pool;
+  uint64_t reserved = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return reserved;
+}
+
+// The refresher thread of the process; joined at exit (a query in flight
+// ends first).
+struct FreeMemoryRefresher {
+  std::thread worker;
+  ~FreeMemoryRefresher() {
+    if (worker.joinable()) worker.join();
+  }
+};
+FreeMemoryRefresher free_memory_refresher;
+
+void refresh_free_memory(int device) {
+  size_t free_now = 0, total = 0;
+  const bool ok = cudaSetDevice(device) == cudaSuccess && cudaMemGetInfo(&free_now, &total) == cudaSuccess;
+  const uint64_t reserved = pool_reserved_bytes(device);
+  if (!ok) cudaGetLastError();
+  std::lock_guard<std::mutex> hold(free_memory_lock);
+  FreeMemory& e = free_memory[device];
+  if (ok) {
+    e.when = std::chrono::steady_clock::now();
+    e.free = free_now;
+    e.reserved = reserved;
+    e.valid = true;
+  }
+  free_memory_refreshing = false;
+}
+
+}  // namespace
+
+int device_free_bytes(int device, size_t* free_bytes) {
+  const uint64_t reserved = pool_reserved_bytes(device);
+  {
+    std::lock_guard<std::mutex> hold(free_memory_lock);
+    FreeMemory& e = free_memory[device];
+    if (e.valid) {
+      const int64_t grown = static_cast<int64_t>(reserved) - static_cast<int64_t>(e.reserved);
+      const int64_t est = static_cast<int64_t>(e.free) - grown;
+      *free_bytes = est > 0 ? static_cast<size_t>(est) : 0;
+      if (!free_memory_refreshing && std::chrono::steady_clock::now() - e.when > std::chrono::seconds(2)) {
+        free_memory_refreshing = true;
+        // The previous refresh has cleared the flag, its last use of the
+        // lock: joining it here cannot wait on this lock.
+        if (free_memory_refresher.worker.joinable()) free_memory_refresher.worker.join();
+        free_memory_refresher.worker = std::thread(refresh_free_memory, device);
+      }
+      return MGBFS2_OK;
+    }
+  }
+  size_t free_now = 0, total = 0;
+  const cudaError_t err = cudaMemGetInfo(&free_now, &total);
+  if (err != cudaSuccess) return cuda_status(err);
+  std::lock_guard<std::mutex> hold(free_memory_lock);
+  FreeMemory& e = free_memory[device];
+  e.when = std::chrono::steady_clock::now();
+  e.free = free_now;
+  e.reserved = reserved;
+  e.valid = true;
+  *free_bytes = free_now;
+  return MGBFS2_OK;
+}
+
 uint64_t pool_idle_bytes(int device) {
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return 0;
@@ -728,8 +820,8 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (r.visited > MGBFS2_VISITED_HASH3 || r.dedup > MGBFS2_DEDUP_GROUPED || r.planner > MGBFS2_PLANNER_LEARNED)
     return MGBFS2_INVALID_ARGUMENT;
   MG_CHECK(cudaSetDevice(device));
-  size_t free_bytes = 0, total_bytes = 0;
-  MG_CHECK(cudaMemGetInfo(&free_bytes, &total_bytes));
+  size_t free_bytes = 0;
+  if (int rc = device_free_bytes(device, &free_bytes)) return rc;
   free_bytes += pool_idle_bytes(device) + device_cache_bytes(device);
   const uint64_t reserve = r.reserve_bytes ? r.reserve_bytes : (2ull << 30);
   if (free_bytes <= reserve) return MGBFS2_OUT_OF_MEMORY;

@@ -53,6 +53,9 @@ int retain_pool_memory(int device);
 int pinned_take(size_t bytes, void** out);
 void pinned_give(void* ptr);
 uint64_t pool_idle_bytes(int device);
+// Free device memory (cudaMemGetInfo), reused for up to two seconds per device and
+// corrected by the change in this process's pool reservation since.
+int device_free_bytes(int device, size_t* free_bytes);
 
 struct WideState;     // int64-key arena path (wide.cu)
 struct ExpandParams;  // packed_kernels.cuh
