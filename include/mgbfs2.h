@@ -98,7 +98,7 @@ typedef struct {
    * memory allow).  They change speed only. */
   uint32_t group_chunk;
   uint32_t blocks_per_sm;
-  uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 2 for
+  uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 1 for
                                   quotient-slot hash layers, else 4 up to 4 generators and 2 above) */
   uint32_t reserved;
 } mgbfs2_plan_request;

@@ -94,7 +94,7 @@ def shape_candidates(plan: dict, resolved: dict) -> list[dict]:
         out += [dict(plan, bucket_margin=m) for m in (1024, 16384)]
     elif visited == "hash":
         out += [dict(plan, hash_load_percent=f) for f in (35, 70)]
-        out.append(dict(plan, parents_per_thread=4 if resolved.get("parents_per_thread") == 2 else 2))
+        out.append(dict(plan, parents_per_thread=2 if resolved.get("parents_per_thread", 4) in (1, 4) else 1))
         out += [dict(plan, blocks_per_sm=b) for b in (4, 8)]
     elif visited == "bitmap":
         out += [dict(plan, blocks_per_sm=b) for b in (3, 6)]

@@ -996,10 +996,11 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     p.table_slots = slots;
     p.table_slot_bytes = hash_quotient ? 4 : 8;
     p.hash_load_percent = load;
-    // Quotient-slot layers stage a tile's children in 2048 entries: two
-    // parents per thread fit one flush per tile (S11 LRX: 4.25 ms against
-    // 4.78 ms with four parents and a flush per generator).
-    if (hash_quotient && !parents_per_thread) parents_per_thread = p.parents_per_thread = 2;
+    // Quotient-slot layers stage a tile's children in 2048 entries: one
+    // parent per thread fits a tile in one flush with the most tiles in
+    // flight (S11 LRX: 3.85 ms; 3.96 ms with two parents; 4.78 ms with four
+    // and a flush per generator).
+    if (hash_quotient && !parents_per_thread) parents_per_thread = p.parents_per_thread = 1;
   }
   if (hash_routed) {
     // Hash-routed layers: shard = table region of a key's home slot, regions

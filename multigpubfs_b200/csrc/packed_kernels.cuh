@@ -296,7 +296,15 @@ __global__ void __launch_bounds__(kBlock, V == V_HASHQ ? kHashQBlocksPerSM : 1) 
       for (int j = 0; j < 2; ++j) {
         par[2 * j] = par[2 * j + 1] = 0;
         val[2 * j] = val[2 * j + 1] = false;
-        if (2 * j < static_cast<int>(p.ppt)) {
+        if (p.ppt == 1) {
+          // One parent per thread: parent base + tid (the pair loads below
+          // would cover two tiles' worth of positions).
+          const unsigned long long i0 = base + threadIdx.x;
+          if (j == 0 && i0 < count) {
+            par[0] = frontier[i0];
+            val[0] = true;
+          }
+        } else if (2 * j < static_cast<int>(p.ppt)) {
           const unsigned long long i0 = base + 2ull * (j * blockDim.x + threadIdx.x);
           if (i0 + 1 < count) {
             const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(frontier + i0);

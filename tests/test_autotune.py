@@ -66,8 +66,11 @@ def test_shape_candidates_vary_the_kept_path_only():
     assert hashed[0] == autotune.DEFAULT and {"visited": "auto", "dedup": "auto", "hash_load_percent": 70} in hashed
     assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 2} in hashed
     quotient = autotune.shape_candidates(dict(autotune.DEFAULT),
-                                         {"visited": "hash", "dedup": "atomic", "parents_per_thread": 2})
-    assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 4} in quotient
+                                         {"visited": "hash", "dedup": "atomic", "parents_per_thread": 1})
+    assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 2} in quotient
+    two = autotune.shape_candidates(dict(autotune.DEFAULT),
+                                    {"visited": "hash", "dedup": "atomic", "parents_per_thread": 2})
+    assert {"visited": "auto", "dedup": "auto", "parents_per_thread": 1} in two
     bucket = autotune.shape_candidates({"visited": "bitmap", "dedup": "bucket", "shards": 1},
                                        {"visited": "bitmap", "dedup": "bucket"})
     assert [p.get("bucket_margin") for p in bucket] == [None, 1024, 16384]

@@ -312,3 +312,20 @@ def test_bfs_through_cayleypy_boundary(tmp_path, monkeypatch):
     assert result.layer_sizes == [len(x) for x in exact]
     assert result.diameter() == len(exact) - 1
     assert result.last_layer().tolist() == exact[-1]
+
+
+@pytest.mark.parametrize("ppt", [1, 2, 4])
+@pytest.mark.parametrize("plan", [dict(visited="bitmap", dedup="atomic"), dict(visited="bitmap", dedup="warp"),
+                                  dict(visited="hash"), dict(visited="hash", wide_slots=True),
+                                  dict(visited="bitmap", dedup="atomic", host_loop=True)])
+def test_every_parents_per_thread_shape_is_exact(ppt, plan):
+    """The fused kernels' tile shapes (1, 2 or 4 parents per thread), device
+    and host loops, on LRX S10 and Coxeter S9 against the reference's tables."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    for gens, n, expect in ((G.lrx_generators(10), 10, golden("lrx_layers.json")["layers"]["10"]),
+                            (G.coxeter_generators(9), 9, G.coxeter_layers(9))):
+        with NativeGraph(GraphDefinition.permutation(gens, list(range(n)))) as e:
+            info = e.plan(parents_per_thread=ppt, **plan)
+            assert info["parents_per_thread"] == ppt
+            assert e.run().layer_sizes == expect, (n, ppt, plan)
