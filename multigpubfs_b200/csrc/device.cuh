@@ -326,7 +326,7 @@ constexpr uint32_t kMatrixCopy = 1u << 31;
 // Template N of the fused, route and count kernels for packed matrices: the
 // action is compiled in, so permutation kernels carry none of its code.
 constexpr int kMatrixN = -1;
-constexpr uint32_t kMatrixMaxCols = 8;
+constexpr uint32_t kMatrixMaxCols = 4;
 
 struct MatrixAction {
   uint32_t rows, cols, bits, mod;  // mod = 0: permutation terms instead

@@ -329,3 +329,28 @@ def test_every_parents_per_thread_shape_is_exact(ppt, plan):
             info = e.plan(parents_per_thread=ppt, **plan)
             assert info["parents_per_thread"] == ppt
             assert e.run().layer_sizes == expect, (n, ppt, plan)
+
+
+@pytest.mark.parametrize("shape", [dict(group_chunk=256), dict(group_chunk=1 << 20), dict(group_chunk=2048, blocks_per_sm=4),
+                                   dict(blocks_per_sm=8), dict(bucket_margin=0)])
+def test_grouped_shapes_are_exact(shape):
+    """Every grouped layer (bucket_min_work 1) under the tuner's shapes, on
+    S11 LRX against the reference's table."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    with NativeGraph(GraphDefinition.permutation(G.lrx_generators(11), list(range(11)))) as e:
+        info = e.plan(visited="bitmap", dedup="grouped", bucket_min_work=1, **shape)
+        assert info["dedup"] == "grouped"
+        assert e.run().layer_sizes == golden("lrx_layers.json")["layers"]["11"]
+
+
+@pytest.mark.parametrize("blocks", [1, 2, 8, 16])
+def test_fused_blocks_per_sm_are_exact(blocks):
+    """Resident-block shapes of the fused bitmap and hash kernels on S10
+    Coxeter against the Mahonian layer sizes."""
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    for plan in (dict(visited="bitmap", dedup="atomic"), dict(visited="hash")):
+        with NativeGraph(GraphDefinition.permutation(G.coxeter_generators(10), list(range(10)))) as e:
+            e.plan(blocks_per_sm=blocks, **plan)
+            assert e.run().layer_sizes == G.coxeter_layers(10), plan
