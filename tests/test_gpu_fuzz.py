@@ -1,0 +1,105 @@
+"""Seeded random parity sweep: random permutation graphs (distinct and
+repeated labels, directed and inverse-closed generator sets, 2 to 7
+generators on 5 to 10 points) and random modular-matrix graphs, each run
+under a random choice of the plan shapes a caller or the autotuner can ask
+for (visited set, claim mode, parents per thread, resident blocks, host or
+device loop, parent-edge skip), against the oracle's layer tables and
+samples.  The seed is fixed, so a failure names a reproducible case."""
+import random
+
+import pytest
+
+from oracle import graph_oracle as G
+from oracle import packed_oracle as P
+
+pytestmark = pytest.mark.gpu
+
+SEED = 20261204
+CASES = 128
+
+
+def _permutation_case(rng):
+    n = rng.randint(5, 10)
+    gens = [rng.sample(range(n), n) for _ in range(rng.randint(2, 4))]
+    if rng.random() < 0.5:
+        gens = G.add_inverses(gens)
+    labels = list(range(n))
+    if rng.random() < 0.35:
+        labels = [rng.randint(0, max(1, n // 2)) for _ in range(n)]
+        labels[0] = 0
+    return gens, labels
+
+
+def _plan(rng, distinct, closed):
+    choices = [dict(visited="auto")]
+    choices += [dict(visited="bitmap", dedup=d) for d in ("atomic", "warp")]
+    choices += [dict(visited="hash"), dict(visited="hash", wide_slots=True)]
+    if closed:
+        choices.append(dict(visited="hash3"))
+    if distinct:
+        choices.append(dict(visited="bitmap", dedup="bucket", bucket_min_work=1))
+    plan = dict(rng.choice(choices))
+    if plan.get("dedup") in (None, "atomic", "warp") and plan.get("visited") != "hash3":
+        plan["parents_per_thread"] = rng.choice([0, 1, 2, 4])
+    plan["blocks_per_sm"] = rng.choice([0, 0, 2, 8])
+    plan["host_loop"] = rng.random() < 0.3
+    plan["parent_skip"] = rng.random() < 0.8
+    return plan
+
+
+@pytest.mark.parametrize("case", range(CASES))
+def test_random_permutation_graph_under_a_random_plan(case):
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    from multigpubfs_b200.native import NativeError
+    rng = random.Random(SEED * 1000 + case)
+    gens, labels = _permutation_case(rng)
+    distinct = len(set(labels)) == len(labels)
+    closed = G.inverse_closed(G.permutation_graph(gens, labels))
+    plan = _plan(rng, distinct, closed)
+    expect, last, prev = P.packed_bfs(gens, labels, use_bitmap=False, sample=1000)
+    with NativeGraph(GraphDefinition.permutation(gens, labels)) as e:
+        try:
+            e.plan(**plan)
+        except NativeError as exc:
+            assert exc.code == 5, (gens, labels, plan)  # UNSUPPORTED for this graph: nothing ran
+            return
+        r = e.run()
+        got_last, got_prev = e.sample(0, 1000), e.sample(1, 1000)
+    assert r.complete and r.layer_sizes == expect, (gens, labels, plan)
+    # A layer of at most 1000 states is sampled whole; a larger one gives
+    # 1000 of its states (frontier order), which must all belong to it.
+    if expect[-1] <= 1000:
+        assert got_last == last, (gens, labels, plan)
+    else:
+        assert len(got_last) == 1000 and got_last == sorted(got_last)
+        if expect[-1] <= 20000:
+            _, whole, _ = P.packed_bfs(gens, labels, use_bitmap=False, sample=expect[-1])
+            members = {tuple(x) for x in whole}
+            assert all(tuple(x) in members for x in got_last), (gens, labels, plan)
+    if len(expect) > 1 and expect[-2] < 1000:
+        assert got_prev == prev, (gens, labels, plan)
+
+
+@pytest.mark.parametrize("case", range(24))
+def test_random_matrix_graph_under_a_random_plan(case):
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.engine import NativeGraph
+    rng = random.Random(SEED * 7 + case)
+    rows, cols = rng.choice([(2, 2), (2, 1), (3, 1), (2, 3)])
+    p = rng.choice([q for q in (3, 5, 7, 11, 13) if q ** (rows * cols) <= 1 << 17])
+    gens = []
+    for _ in range(rng.randint(2, 4)):
+        m = [rng.randint(-2, p + 2) for _ in range(rows * rows)]
+        gens.append((m, p))
+    start = [rng.randint(0, p - 1) for _ in range(rows * cols)]
+    graph = G.matrix_graph(rows, cols, gens, start)
+    expect = G.layer_sizes(graph, 1 << 17)
+    plan = dict(rng.choice([dict(visited="auto"), dict(visited="bitmap"), dict(visited="hash"),
+                            dict(visited="bitmap", dedup="bucket", bucket_min_work=1)]))
+    plan["host_loop"] = rng.random() < 0.3
+    with NativeGraph(GraphDefinition.matrix(rows, cols, gens, start)) as e:
+        info = e.plan(**plan)
+        r = e.run()
+    assert info["packed"] == 1
+    assert r.complete and r.layer_sizes == expect, (rows, cols, gens, start, plan)
