@@ -36,8 +36,10 @@ def _plan(rng, distinct, closed):
     choices += [dict(visited="hash"), dict(visited="hash", wide_slots=True)]
     if closed:
         choices.append(dict(visited="hash3"))
+    choices.append(dict(visited="bitmap", dedup="sort"))
     if distinct:
         choices.append(dict(visited="bitmap", dedup="bucket", bucket_min_work=1))
+        choices.append(dict(visited="bitmap", dedup="grouped", bucket_min_work=1))
     plan = dict(rng.choice(choices))
     if plan.get("dedup") in (None, "atomic", "warp") and plan.get("visited") != "hash3":
         plan["parents_per_thread"] = rng.choice([0, 1, 2, 4])
