@@ -105,3 +105,31 @@ def test_random_matrix_graph_under_a_random_plan(case):
         r = e.run()
     assert info["packed"] == 1
     assert r.complete and r.layer_sizes == expect, (rows, cols, gens, start, plan)
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_random_batched_sweep_under_random_shapes(case):
+    """64 random instances in one batched run under random tile sizes,
+    resident blocks, layer loops, memory budgets (several waves) and
+    predicted capacities between a third of and twice each instance's true
+    peak layer (under-predictions redo layers inside the launch)."""
+    from multigpubfs_b200 import workloads
+    from multigpubfs_b200.batch import BatchSweep
+    rng = random.Random(SEED * 13 + case)
+    graphs, expect = [], []
+    while len(graphs) < 64:
+        gens, labels = _permutation_case(rng)
+        if len(labels) > 9:
+            continue
+        labels = list(range(len(labels)))  # the batched path takes distinct labels
+        graphs.append(workloads.permutation_graph(gens, labels))
+        expect.append(P.packed_bfs(gens, labels)[0])
+    opts = dict(tile_entries=rng.choice([256, 512, 1024]), blocks_per_sm=rng.choice([0, 2, 3]),
+                memory_bytes=rng.choice([None, 64 << 20, 256 << 20]))
+    loop = rng.choice(["persistent", "host", "graph"])
+    caps = [max(1, int(max(t) * rng.uniform(0.34, 2.0))) for t in expect] if rng.random() < 0.6 else None
+    with BatchSweep(graphs, 0) as sweep:
+        status = sweep.run(capacities=caps, host_loop=loop == "host", graph_loop=loop == "graph", **opts)
+        tables = sweep.layer_tables()
+    assert status["complete_instances"] == 64 and not status["fatal"], (opts, loop, status)
+    assert tables == expect, (opts, loop)
