@@ -133,3 +133,18 @@ def test_random_batched_sweep_under_random_shapes(case):
         tables = sweep.layer_tables()
     assert status["complete_instances"] == 64 and not status["fatal"], (opts, loop, status)
     assert tables == expect, (opts, loop)
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_random_graph_split_over_random_ranks(case):
+    """The owner-partitioned path (every rank's shard in one process) on
+    random graphs of distinct labels, 1 to 9 ranks, random route chunks."""
+    from multigpubfs_b200 import GraphDefinition, sharded
+    rng = random.Random(SEED * 17 + case)
+    gens, labels = _permutation_case(rng)
+    labels = list(range(len(labels)))
+    expect = P.packed_bfs(gens, labels)[0]
+    world = rng.randint(1, 9)
+    chunk = rng.choice([32, 1000, 1 << 25])
+    got = sharded.run_emulated(GraphDefinition.permutation(gens, labels), world, chunk_parents=chunk)
+    assert got == expect, (gens, world, chunk)
