@@ -100,7 +100,9 @@ typedef struct {
   uint32_t blocks_per_sm;
   uint32_t parents_per_thread; /* fused layers: 1, 2 or 4 frontier states per thread and tile (0 = 1 for
                                   quotient-slot hash layers, else 4 up to 4 generators and 2 above) */
-  uint32_t reserved;
+  uint32_t route_chunk;    /* routed (BUCKET) layers: parents routed and accepted per pass, a multiple of
+                              1024 (0 = the whole layer, or the largest chunk whose buckets fit the device
+                              memory left beside the bitmap and both frontiers, e.g. S14 under LRX) */
 } mgbfs2_plan_request;
 
 /* Packed graphs tag every frontier state with the generator that produced it

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/mgbfs2.h"
 #include "bucket_kernels.cuh"
 #include "engine.h"
@@ -39,9 +41,26 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr uint64_t kRouteChunkAlign = 1024;  // parents: route chunks start 8 KB apart
+
 void set_message(char* error, size_t capacity, const std::string& text) {
   if (!error || !capacity) return;
   std::snprintf(error, capacity, "%s", text.c_str());
+}
+
+// Grouped layers' prefix length K for degree n: N - 10 (10!-bit, 454 KB
+// groups, whose working set of target groups stays in L2) within 1..4, the
+// largest K <= 4 with at most kMaxGroups = 14!/10! groups above that (K = 3
+// for degrees 15 and 16).
+uint32_t group_prefix_for(uint32_t n) {
+  uint32_t K = n > 10 ? std::min<uint32_t>(4, n - 10) : 1;
+  const auto groups = [n](uint32_t k) {
+    uint64_t g = 1;
+    for (uint32_t i = 0; i < k; ++i) g *= n - i;
+    return g;
+  };
+  while (K > 1 && groups(K) > kMaxGroups) --K;
+  return K;
 }
 
 uint64_t next_pow2(uint64_t x) {
@@ -532,18 +551,244 @@ void Graph::release() {
   front_grouped = false;
 }
 
+// Mapped buffers.  On a B200 a stream-ordered pool allocation of tens of GB
+// took 0.07-1.8 s (8-64 GB, at random), giving it back up to 1 s, and a freed
+// block that the pool keeps is no use to the next, larger one; creating and
+// mapping 32 GB of physical memory took 27 ms, releasing it 22 ms.  So buffers
+// from kMappedMin bytes up reserve a virtual range of the device's size once
+// and grow in place by mapping the missing tail (a BFS near the memory's
+// limit maps each byte once), give memory back at once when freed, and are
+// kept mapped for the next handle when their handle is destroyed.  The
+// driver's calls come through cudaGetDriverEntryPoint (no link against the
+// driver library).
+namespace {
+constexpr size_t kMappedMin = 1ull << 30;
+
+struct MappedApi {
+  bool ok = false;
+  size_t granularity = 0, total = 0;  // mapping granularity, device memory
+  CUmemAllocationProp prop{};
+  CUresult (*create)(CUmemGenericAllocationHandle*, size_t, const CUmemAllocationProp*, unsigned long long) = nullptr;
+  CUresult (*reserve)(CUdeviceptr*, size_t, size_t, CUdeviceptr, unsigned long long) = nullptr;
+  CUresult (*map)(CUdeviceptr, size_t, size_t, CUmemGenericAllocationHandle, unsigned long long) = nullptr;
+  CUresult (*access)(CUdeviceptr, size_t, const CUmemAccessDesc*, size_t) = nullptr;
+  CUresult (*unmap)(CUdeviceptr, size_t) = nullptr;
+  CUresult (*release)(CUmemGenericAllocationHandle) = nullptr;
+  CUresult (*address_free)(CUdeviceptr, size_t) = nullptr;
+  CUresult (*granule)(size_t*, const CUmemAllocationProp*, CUmemAllocationGranularity_flags) = nullptr;
+};
+
+std::mutex mapped_lock;
+std::map<int, MappedApi> mapped_apis;
+std::map<int, uint64_t> mapped_total;  // physical bytes mapped by this process, per device
+
+template <typename F>
+bool entry_point(const char* name, F* fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &found) != cudaSuccess ||
+      found != cudaDriverEntryPointSuccess || !p) {
+    cudaGetLastError();
+    return false;
+  }
+  *fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+const MappedApi& mapped_api(int device) {
+  std::lock_guard<std::mutex> hold(mapped_lock);
+  auto it = mapped_apis.find(device);
+  if (it != mapped_apis.end()) return it->second;
+  MappedApi& a = mapped_apis[device];
+  a.prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  a.prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  a.prop.location.id = device;
+  a.ok = entry_point("cuMemCreate", &a.create) && entry_point("cuMemAddressReserve", &a.reserve) &&
+         entry_point("cuMemMap", &a.map) && entry_point("cuMemSetAccess", &a.access) &&
+         entry_point("cuMemUnmap", &a.unmap) && entry_point("cuMemRelease", &a.release) &&
+         entry_point("cuMemAddressFree", &a.address_free) &&
+         entry_point("cuMemGetAllocationGranularity", &a.granule) &&
+         a.granule(&a.granularity, &a.prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED) == CUDA_SUCCESS &&
+         a.granularity > 0;
+  size_t free_now = 0;
+  if (a.ok && cudaMemGetInfo(&free_now, &a.total) != cudaSuccess) {
+    cudaGetLastError();
+    a.ok = false;
+  }
+  return a;
+}
+
+uint64_t mapped_bytes(int device) {
+  std::lock_guard<std::mutex> hold(mapped_lock);
+  auto it = mapped_total.find(device);
+  return it == mapped_total.end() ? 0 : it->second;
+}
+
+void mapped_add(int device, int64_t delta) {
+  std::lock_guard<std::mutex> hold(mapped_lock);
+  mapped_total[device] += static_cast<uint64_t>(delta);
+}
+
+size_t round_up(size_t x, size_t g) { return (x + g - 1) / g * g; }
+}  // namespace
+
+namespace {
+// Mapped buffers given back by destroyed handles, per device, still mapped: a
+// new handle takes one (the smallest that holds its request, else the largest,
+// grown in place) without a driver call.  Beyond kMappedCacheEntries the
+// smallest is unmapped.
+constexpr size_t kMappedCacheEntries = 16;
+std::map<int, std::vector<DeviceBuffer>> mapped_cache;  // under mapped_lock
+std::map<int, uint64_t> mapped_cache_total;
+
+// Unmaps and releases a mapped buffer with no work in flight.
+void unmap_buffer(DeviceBuffer* b) {
+  const MappedApi& a = mapped_api(b->device);
+  CUdeviceptr at = reinterpret_cast<CUdeviceptr>(b->ptr);
+  for (const auto& c : b->chunks) {
+    a.unmap(at, c.second);
+    a.release(c.first);
+    at += c.second;
+  }
+  a.address_free(reinterpret_cast<CUdeviceptr>(b->ptr), b->span);
+  mapped_add(b->device, -static_cast<int64_t>(b->bytes));
+  b->chunks.clear();
+  b->span = 0;
+  b->ptr = nullptr;
+  b->bytes = 0;
+}
+
+bool mapped_cache_take(int device, size_t want, DeviceBuffer* b) {
+  std::lock_guard<std::mutex> hold(mapped_lock);
+  std::vector<DeviceBuffer>& v = mapped_cache[device];
+  if (v.empty()) return false;
+  size_t pick = 0;
+  for (size_t i = 1; i < v.size(); ++i) {
+    const bool fits = v[i].bytes >= want, best_fits = v[pick].bytes >= want;
+    if (fits ? (!best_fits || v[i].bytes < v[pick].bytes) : (!best_fits && v[i].bytes > v[pick].bytes)) pick = i;
+  }
+  b->ptr = v[pick].ptr;
+  b->bytes = v[pick].bytes;
+  b->span = v[pick].span;
+  b->device = v[pick].device;
+  b->chunks.swap(v[pick].chunks);
+  mapped_cache_total[device] -= b->bytes;
+  v.erase(v.begin() + static_cast<std::ptrdiff_t>(pick));
+  return true;
+}
+
+void mapped_cache_give(DeviceBuffer* b) {
+  DeviceBuffer evicted;
+  {
+    std::lock_guard<std::mutex> hold(mapped_lock);
+    std::vector<DeviceBuffer>& v = mapped_cache[b->device];
+    v.push_back(*b);
+    mapped_cache_total[b->device] += b->bytes;
+    if (v.size() > kMappedCacheEntries) {
+      size_t small = 0;
+      for (size_t i = 1; i < v.size(); ++i)
+        if (v[i].bytes < v[small].bytes) small = i;
+      evicted = v[small];
+      mapped_cache_total[b->device] -= evicted.bytes;
+      v.erase(v.begin() + static_cast<std::ptrdiff_t>(small));
+    }
+  }
+  b->chunks.clear();
+  b->span = 0;
+  b->ptr = nullptr;
+  b->bytes = 0;
+  if (evicted.span) unmap_buffer(&evicted);
+}
+
+uint64_t mapped_cache_bytes(int device) {
+  std::lock_guard<std::mutex> hold(mapped_lock);
+  auto it = mapped_cache_total.find(device);
+  return it == mapped_cache_total.end() ? 0 : it->second;
+}
+
+// Unmaps every cached mapped buffer of `device` (none has work in flight).
+void mapped_cache_drain(int device) {
+  std::vector<DeviceBuffer> v;
+  {
+    std::lock_guard<std::mutex> hold(mapped_lock);
+    v.swap(mapped_cache[device]);
+    mapped_cache_total[device] = 0;
+  }
+  for (DeviceBuffer& b : v) unmap_buffer(&b);
+}
+}  // namespace
+
+// Maps the tail [bytes, target) of a mapped buffer.  A buffer that is not yet
+// mapped first gives back its pool block and takes a cached mapped buffer, or
+// reserves a virtual range of the device's size.  The mapped part keeps its
+// contents.  A chunk that finds no free memory is retried once after the
+// device caches and the pool's idle memory are given back.
+static int grow_mapped(DeviceBuffer* b, int device, size_t want, bool exact) {
+  const MappedApi& a = mapped_api(device);
+  if (!b->span) {
+    b->free();
+    if (!mapped_cache_take(device, want, b)) {
+      const size_t span = round_up(std::max(want, a.total), a.granularity);
+      CUdeviceptr va = 0;
+      if (a.reserve(&va, span, 0, 0, 0) != CUDA_SUCCESS) return MGBFS2_OUT_OF_MEMORY;
+      b->ptr = reinterpret_cast<void*>(va);
+      b->span = span;
+      b->device = device;
+    }
+    if (want <= b->bytes) return MGBFS2_OK;
+  }
+  size_t target = round_up(want, a.granularity);
+  if (!exact) target = std::max(target, round_up(b->bytes + b->bytes / 4, a.granularity));
+  if (target > b->span) return MGBFS2_OUT_OF_MEMORY;
+  const size_t delta = target - b->bytes;
+  CUmemGenericAllocationHandle h = 0;
+  CUresult r = a.create(&h, delta, &a.prop, 0);
+  if (r == CUDA_ERROR_OUT_OF_MEMORY) {
+    cudaMemPool_t pool;
+    device_cache_drain(device, b->stream);
+    if (cudaStreamSynchronize(b->stream) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+        cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+      r = a.create(&h, delta, &a.prop, 0);
+    cudaGetLastError();
+  }
+  if (r != CUDA_SUCCESS) return r == CUDA_ERROR_OUT_OF_MEMORY ? MGBFS2_OUT_OF_MEMORY : MGBFS2_CUDA_BASE + static_cast<int>(r);
+  const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(b->ptr) + b->bytes;
+  CUmemAccessDesc rw{};
+  rw.location = a.prop.location;
+  rw.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+  if ((r = a.map(at, delta, 0, h, 0)) != CUDA_SUCCESS) {
+    a.release(h);
+    return MGBFS2_CUDA_BASE + static_cast<int>(r);
+  }
+  if ((r = a.access(at, delta, &rw, 1)) != CUDA_SUCCESS) {
+    a.unmap(at, delta);
+    a.release(h);
+    return MGBFS2_CUDA_BASE + static_cast<int>(r);
+  }
+  b->chunks.emplace_back(h, delta);
+  b->bytes = target;
+  mapped_add(device, static_cast<int64_t>(delta));
+  return MGBFS2_OK;
+}
+
 // Stream-ordered allocations from the device's default memory pool, which
 // keeps freed memory reserved (release threshold = max) so that regrowing a
 // buffer, or a new graph handle in the same process, reuses it without device
 // synchronisation.  Growth is geometric (x1.5) so a BFS regrows O(log) times.
+// From kMappedMin bytes on, mapped buffers (grow_mapped).
 int DeviceBuffer::ensure(size_t want, bool exact) {
   if (want <= bytes) return MGBFS2_OK;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return MGBFS2_CUDA_BASE;
+  }
+  if (span || (want >= kMappedMin && mapped_api(device).ok)) return grow_mapped(this, device, want, exact);
   const size_t grown = exact ? want : std::max(want, bytes + bytes / 2);
   free();
   void* p = nullptr;
-  int device = 0;
   size_t cached = 0;
-  if (cudaGetDevice(&device) == cudaSuccess && device_cache_take(device, grown, &p, &cached)) {
+  if (device_cache_take(device, grown, &p, &cached)) {
     ptr = p;
     bytes = cached;
     return MGBFS2_OK;
@@ -556,6 +801,16 @@ int DeviceBuffer::ensure(size_t want, bool exact) {
     device_cache_drain(device, stream);
     e = cudaMallocAsync(&p, grown, stream);
   }
+  cudaMemPool_t pool;
+  if (e == cudaErrorMemoryAllocation && pool_idle_bytes(device) &&
+      cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    // The pool keeps what it was given back (release threshold: all), in
+    // blocks that may each be too small for this one: once the frees in
+    // flight are done, hand the idle memory to the driver and retry.
+    cudaGetLastError();
+    if (cudaStreamSynchronize(stream) == cudaSuccess && cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+      e = cudaMallocAsync(&p, grown, stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? MGBFS2_OUT_OF_MEMORY : cuda_status(e);
@@ -566,12 +821,19 @@ int DeviceBuffer::ensure(size_t want, bool exact) {
 }
 
 void DeviceBuffer::free() {
-  if (ptr) cudaFreeAsync(ptr, stream);
+  if (span) {
+    // Work in flight may still use the range: unmap once the stream is done.
+    cudaStreamSynchronize(stream);
+    unmap_buffer(this);
+  } else if (ptr) {
+    cudaFreeAsync(ptr, stream);
+  }
   ptr = nullptr;
   bytes = 0;
 }
 
 void DeviceBuffer::release_to_cache(int device) {
+  if (span) mapped_cache_give(this);
   if (ptr) device_cache_give(device, ptr, bytes);
   ptr = nullptr;
   bytes = 0;
@@ -616,9 +878,10 @@ void device_cache_give(int device, void* ptr, size_t bytes) {
 }
 
 uint64_t device_cache_bytes(int device) {
+  uint64_t mapped = mapped_cache_bytes(device);
   std::lock_guard<std::mutex> lock(device_cache_mutex);
   auto it = device_cache_total.find(device);
-  return it == device_cache_total.end() ? 0 : it->second;
+  return mapped + (it == device_cache_total.end() ? 0 : it->second);
 }
 
 // Frees every cached buffer of `device` into its pool, in the order of
@@ -631,6 +894,7 @@ void device_cache_drain(int device, cudaStream_t stream) {
     device_cache_total[device] = 0;
   }
   for (auto& kv : entries) cudaFreeAsync(kv.second, stream);
+  mapped_cache_drain(device);
 }
 
 // Frees every cached buffer of `device` and returns the pool's unused memory
@@ -648,6 +912,7 @@ int device_cache_release(int device) {
   for (auto& kv : entries)
     if (e == cudaSuccess) e = cudaFreeAsync(kv.second, 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) mapped_cache_drain(device);
   cudaMemPool_t pool;
   if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&pool, device);
   if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
@@ -729,15 +994,17 @@ std::mutex free_memory_lock;
 std::map<int, FreeMemory> free_memory;
 bool free_memory_refreshing = false;  // one refresh at a time, any device
 
+// Device memory this process holds through the library: the pool's
+// reservation and the mapped buffers.
 uint64_t pool_reserved_bytes(int device) {
   cudaMemPool_t pool;
   uint64_t reserved = 0;
   if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess ||
       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess) {
     cudaGetLastError();
-    return 0;
+    reserved = 0;
   }
-  return reserved;
+  return reserved + mapped_bytes(device);
 }
 
 // The refresher thread of the process; joined at exit (a query in flight
@@ -826,6 +1093,7 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   const uint64_t reserve = r.reserve_bytes ? r.reserve_bytes : (2ull << 30);
   if (free_bytes <= reserve) return MGBFS2_OUT_OF_MEMORY;
   const uint64_t budget = free_bytes - reserve;
+  memory_reserve = reserve;
   mgbfs2_plan_info p{};
   p.packed = packed;
   p.bits_per_symbol = packed ? bits : 64;
@@ -848,6 +1116,8 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
   if (r.parents_per_thread && r.parents_per_thread != 1 && r.parents_per_thread != 2 && r.parents_per_thread != 4)
     return MGBFS2_INVALID_ARGUMENT;
   parents_per_thread = r.parents_per_thread;
+  if (r.route_chunk % kRouteChunkAlign) return MGBFS2_INVALID_ARGUMENT;
+  route_chunk = r.route_chunk;
   group_chunk = r.group_chunk ? r.group_chunk : kGroupChunk;
   blocks_per_sm = static_cast<int>(r.blocks_per_sm);
   p.group_chunk = group_chunk;
@@ -882,8 +1152,8 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     // whatever the generators.
     dedup = MGBFS2_DEDUP_ATOMIC;
     if (visited == MGBFS2_VISITED_BITMAP && lehmer && !use_product && bitmap_bytes > (64ull << 20) && elements <= 16) {
-      const uint32_t n = elements, K = n > 10 ? std::min<uint32_t>(3, n - 10) : 1;
-      bool local = n <= 13;
+      const uint32_t n = elements, K = group_prefix_for(n);
+      bool local = n <= 14;
       for (uint32_t k = 0; k < gens && local; ++k) {
         uint32_t outside = 0;
         for (uint32_t i = 0; i < K; ++i) outside += perms[static_cast<size_t>(k) * n + i] >= K ? 1 : 0;
@@ -934,14 +1204,12 @@ int Graph::make_plan(const mgbfs2_plan_request* req, mgbfs2_plan_info* out) {
     bucket_min_work = r.bucket_min_work ? r.bucket_min_work : (1ull << 22);
   }
   if (dedup == MGBFS2_DEDUP_GROUPED) {
-    // Groups = states sharing their first K symbols; K = N - 10 (10!-bit,
-    // 454 KB groups) within 1..3 and at most kMaxGroups groups.
+    // Groups = states sharing their first K symbols (group_prefix_for).
     const uint32_t n = elements;
     if (n < 2 || n > 16) return MGBFS2_UNSUPPORTED;
     uint64_t fact[17] = {1};
     for (uint32_t i = 1; i <= 16; ++i) fact[i] = fact[i - 1] * i;
-    uint32_t K = n > 10 ? std::min<uint32_t>(3, n - 10) : 1;
-    while (K > 1 && fact[n] / fact[n - K] > kMaxGroups) --K;
+    const uint32_t K = group_prefix_for(n);
     if (fact[n] / fact[n - K] > kMaxGroups) return MGBFS2_UNSUPPORTED;
     group_prefix = K;
     groups = static_cast<uint32_t>(fact[n] / fact[n - K]);
@@ -1144,6 +1412,7 @@ static void pick_bucket(uint32_t n, uint32_t prefix, RouteFn* route, AcceptFn* a
 using GroupedFn = void (*)(GroupedParams);
 
 static GroupedFn pick_grouped(uint32_t n, uint32_t prefix) {
+  if (prefix == 4) return n == 14 ? expand_grouped<14, 4, false> : nullptr;
   switch (n) {
 #define MG_CASE(K)                                                                               \
   case K:                                                                                        \
@@ -1287,7 +1556,11 @@ static size_t group_meta_bytes(uint32_t groups) {
 // Lays out the next frontier of a grouped layer and uploads the layer's meta.
 // Group regions get the current layer's distribution of `count` scaled by the
 // last growth ratio, plus 25 % and bucket_margin; the spill region gets the exact
-// bound `cap`, so every winner has a place.
+// bound `cap`, so every winner has a place, where the device memory holds it
+// with room to spare; else at least half the group regions, as far as the memory
+// goes (S14 under LRX: the exact bound of its 4.6e9-state layer would need 74 GB
+// of spill beside two 46 GB frontiers).  A winner that finds no place raises
+// ERR_FRONTIER_OVERFLOW: the run ends, no state is lost.
 int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void** fn, size_t* smem_total,
                          size_t smem, uint64_t* items, uint32_t* grid) {
   const uint32_t G = groups, R = groups + 1;
@@ -1333,12 +1606,32 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
     nc[g] = next_cap[g] = c;
     total += c;
   }
+  constexpr uint64_t W = sizeof(unsigned long long);
+  uint64_t spill = cap;
+  if ((total + spill + 2) * W > next.bytes) {
+    // Growing `next` frees it first: its bytes count as free here.
+    size_t free_bytes = 0;
+    if ((rc = device_free_bytes(device, &free_bytes))) return rc;
+    const uint64_t avail = free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes;
+    const uint64_t room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
+    if ((total + spill + 2) / 2 * 3 <= room) {
+      if ((rc = next.ensure((total + spill + 2) * W))) return rc;
+    } else {
+      // Memory-bounded: a spill of at least half the group regions (or the
+      // bound), the buffer grown with 25 % headroom within the memory, so
+      // that it is reallocated every few layers rather than every layer.
+      if (room < total + bucket_margin + 2) return MGBFS2_OUT_OF_MEMORY;
+      const uint64_t least = total + std::min<uint64_t>(cap, total / 2) + 2;
+      if (next.bytes / W < least && (rc = next.ensure(std::min<uint64_t>(room, least + least / 4) * W, true)))
+        return rc;
+      spill = std::min<uint64_t>(cap, next.bytes / W - total - 2);
+    }
+  }
   nb[G] = next_begin[G] = total;
-  nc[G] = next_cap[G] = cap;
-  total += cap;
+  nc[G] = next_cap[G] = spill;
+  total += spill;
   for (uint32_t r = 0; r < R; ++r) ncount[r] = 0;
   ncount[R] = 0;  // work counter
-  if ((rc = next.ensure((total + 2) * sizeof(unsigned long long)))) return rc;
   MG_CHECK(cudaMemcpyAsync(group_meta.ptr, host_group, bytes, cudaMemcpyHostToDevice, stream));
   GroupedFn f = group_transp ? pick_grouped_transp(elements, group_prefix) : pick_grouped(elements, group_prefix);
   if (!f) return MGBFS2_UNSUPPORTED;
@@ -1426,7 +1719,8 @@ int Graph::bucket_setup(uint64_t work, bool exact) {
     cap[s] = c;
     total += c;
   }
-  if ((rc = buckets.ensure(total * sizeof(unsigned long long)))) return rc;
+  bucket_work = work;
+  if ((rc = buckets.ensure(total * sizeof(unsigned long long), bucket_alloc_exact))) return rc;
   MG_CHECK(cudaMemcpyAsync(shard_meta.ptr, host_meta, 2 * kMaxShards * sizeof(unsigned long long),
                            cudaMemcpyHostToDevice, stream));
   // Zero the shard counts and the accept work counter.
@@ -1491,6 +1785,94 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
   reinterpret_cast<AcceptFn>(const_cast<void*>(accept_fn))<<<grid_for(accept_fn, 0, UINT32_MAX), kBlock, 0, stream>>>(ap);
   ++launches;
   MG_CHECK(cudaGetLastError());
+  return MGBFS2_OK;
+}
+
+// Sizes a routed layer's next frontier (up to the exact bound `*cap`) and its
+// shard buckets (the estimate of bucket_setup: the last distribution + 20 %,
+// or x2 uniform, plus bucket_margin per shard) together.  Where both fit the
+// device memory with room to spare the layer is one route and one accept
+// pass, with the buffers' usual geometric growth.  Otherwise, and for the
+// rest of the run, both grow only to sizes chosen here, with 25 % headroom so
+// that a run near the memory's limit reallocates them every few layers, not
+// every layer: the next frontier takes up to `*cap` (lowered to what the
+// memory holds: a layer larger than that ends the run with
+// ERR_FRONTIER_OVERFLOW), the buckets what is left, and a layer whose buckets
+// do not fit them is routed in parent chunks of `*chunk`.  S14 under LRX needs
+// this: its 4.6e9-state layer has 13.8e9 successors, 110 GB of buckets, on a
+// 180 GB GPU.
+int Graph::routed_setup(uint64_t count, uint64_t* cap, uint64_t* chunk) {
+  const uint64_t margin = static_cast<uint64_t>(bucket_shards) * bucket_margin;
+  const double per_parent = static_cast<double>(gens) * (shard_history_total ? 1.2 : 2.0);
+  const auto bucket_words = [&](uint64_t parents) {
+    return static_cast<uint64_t>(per_parent * static_cast<double>(parents)) + margin + 1;
+  };
+  constexpr uint64_t W = sizeof(unsigned long long);
+  *chunk = count;
+  if (route_chunk && route_chunk < count) {
+    *chunk = route_chunk;
+    return next.ensure((*cap + 2) * W);
+  }
+  const uint64_t need_next = *cap + 2, need_buckets = bucket_words(count);
+  if (need_next * W <= next.bytes && need_buckets * W <= buckets.bytes) return MGBFS2_OK;
+  size_t free_bytes = 0;
+  if (int rc = device_free_bytes(device, &free_bytes)) return rc;
+  const uint64_t avail =
+      free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes + buckets.bytes;
+  const uint64_t room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
+  if (!bucket_alloc_exact && (need_next + need_buckets) / 2 * 3 <= room) return next.ensure(need_next * W);
+  bucket_alloc_exact = true;
+  const uint64_t least = bucket_words(std::min<uint64_t>(count, kRouteChunkAlign));
+  if (room < least + 2 + bucket_margin) return MGBFS2_OUT_OF_MEMORY;
+  if (need_next * W > next.bytes) {
+    const uint64_t target = std::min<uint64_t>(need_next + need_next / 4, room - least);
+    if (target + buckets.bytes / W > room) buckets.free();
+    if (int rc = next.ensure(target * W, true)) return rc;
+  }
+  *cap = std::min<uint64_t>(*cap, next.bytes / W - 2);
+  const uint64_t left = room > next.bytes / W ? room - next.bytes / W : 0;
+  if (need_buckets * W > buckets.bytes && (need_buckets <= left || buckets.bytes / W < left / 2)) {
+    // The whole layer's buckets where they fit, else all that is left (an
+    // older block is kept while it holds at least half of that).
+    const uint64_t target = need_buckets <= left ? std::min<uint64_t>(need_buckets + need_buckets / 4, left) : left;
+    buckets.free();
+    if (int rc = buckets.ensure(target * W, true)) return rc;
+  }
+  const uint64_t have = buckets.bytes / W;
+  if (need_buckets <= have) return MGBFS2_OK;
+  const uint64_t parents =
+      have > margin + 1 ? static_cast<uint64_t>(static_cast<double>(have - margin - 1) / per_parent) : 0;
+  // Chunks start on 16-byte boundaries: the route kernels read parents in pairs.
+  *chunk = std::max<uint64_t>(kRouteChunkAlign, parents / kRouteChunkAlign * kRouteChunkAlign);
+  return MGBFS2_OK;
+}
+
+// A routed layer in parent chunks (routed_setup): route and accept one chunk at
+// a time, each redone once with its exact shard counts when its buckets
+// overflowed (the bitmap untouched, the next frontier's count kept).  The
+// next frontier's count runs on across the chunks.
+int Graph::bucket_chunks(const void* route_fn, const void* accept_fn, const ExpandParams& p, size_t smem,
+                         uint64_t chunk, uint32_t* redo) {
+  unsigned int* error = &static_cast<Control*>(control_buf.ptr)->error;
+  unsigned long long* counts = static_cast<unsigned long long*>(shard_meta.ptr) + 2 * kMaxShards;
+  for (uint64_t off = 0; off < p.count; off += chunk) {
+    ExpandParams q = p;
+    q.frontier = p.frontier + off;
+    q.count = std::min<uint64_t>(chunk, p.count - off);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      int rc = bucket_setup(q.count * gens, attempt == 1);
+      if (!rc) rc = bucket_launch(route_fn, accept_fn, q, smem);
+      if (rc) return rc;
+      MG_CHECK(cudaMemcpyAsync(host_control, control_buf.ptr, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+      MG_CHECK(cudaMemcpyAsync(host_meta + 2 * kMaxShards, counts, bucket_shards * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, stream));
+      MG_CHECK(cudaStreamSynchronize(stream));
+      if (host_control->error != ERR_BUCKET_OVERFLOW) break;
+      ++*redo;
+      MG_CHECK(cudaMemsetAsync(error, 0, sizeof(unsigned int), stream));
+    }
+    if (host_control->error) break;
+  }
   return MGBFS2_OK;
 }
 
@@ -1810,6 +2192,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
   }
   shard_history.assign(bucket_shards, 0);
   shard_history_total = 0;
+  bucket_alloc_exact = false;
   const bool grouped_mode = plan.dedup == MGBFS2_DEDUP_GROUPED && visit == V_LEHMER;
   if (grouped_mode && !pick_grouped(elements, group_prefix)) return MGBFS2_UNSUPPORTED;
   front_grouped = false;
@@ -1956,16 +2339,21 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     }
     const auto layer_start = Clock::now();
     const uint64_t bound = next_bound(depth, count, visited);
-    const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(bound, 1), plan.capacity);
+    uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(bound, 1), plan.capacity);
     const bool group_layer = grouped_mode && count * gens >= bucket_min_work;
+    const uint64_t work = count * gens;
+    const bool routed = bucketed && work >= bucket_min_work;
     if (!group_layer && front_grouped && (rc = gather_front(count))) break;
     void* group_fn = nullptr;
     size_t group_smem = 0;
     uint32_t group_grid = 1;
     uint64_t group_items = 0;
+    uint64_t route_chunk = count;
     if (group_layer) {
       const uint64_t prev_count = depth ? layer_sizes[depth - 1] : 0;
       if ((rc = grouped_setup(count, prev_count, cap, &group_fn, &group_smem, smem, &group_items, &group_grid))) break;
+    } else if (routed) {
+      if ((rc = routed_setup(count, &cap, &route_chunk))) break;
     } else if ((rc = next.ensure((cap + 2) * 8))) {
       break;
     }
@@ -2036,17 +2424,20 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
       p.look1 = depth >= 1 ? static_cast<const unsigned long long*>(bank[prev].ptr) : nullptr;
       p.look1_mask = depth >= 1 ? bank_slots[prev] - 1 : 0;
     }
-    const uint64_t work = count * gens;
-    const bool routed = bucketed && work >= bucket_min_work;
     TraceRange layer_range(routed ? "layer.bucket" : group_layer ? "layer.grouped" : sorted ? "layer.sorted"
                                                                                          : "layer.fused");
     // One attempt; a routed layer whose shard buckets overflowed left the
     // bitmap untouched and is redone once with the exact shard counts.
     for (int attempt = 0; attempt < 2; ++attempt) {
       MG_CHECK(cudaMemsetAsync(control_buf.ptr, 0, sizeof(Control), stream));
-      if (routed && (rc = bucket_setup(work, attempt == 1))) break;
+      const bool chunked = routed && route_chunk < count;
+      if (routed && !chunked && (rc = bucket_setup(work, attempt == 1))) break;
       MG_CHECK(cudaEventRecord(ev_kernel[0], stream));
-      if (routed) {
+      if (chunked) {
+        if ((rc = bucket_chunks(reinterpret_cast<const void*>(route_fn), reinterpret_cast<const void*>(accept_fn), p,
+                                smem, route_chunk, &st.redo_layers)))
+          break;
+      } else if (routed) {
         if ((rc = bucket_launch(reinterpret_cast<const void*>(route_fn), reinterpret_cast<const void*>(accept_fn), p,
                                 smem)))
           break;
@@ -2107,7 +2498,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
     if (rc) break;
     if (routed && !host_control->error) {
       shard_history.assign(host_meta + 2 * kMaxShards, host_meta + 2 * kMaxShards + bucket_shards);
-      shard_history_total = work;
+      shard_history_total = bucket_work;
     }
     st.successors += count * gens;
     // Every tagged parent (all but the start) skips exactly one generator.

@@ -27,6 +27,12 @@ struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
   cudaStream_t stream = nullptr;
+  // Mapped buffers (kMappedMin bytes and up): a reserved virtual range of
+  // `span` bytes (0 = a pool allocation) that grows in place, one physical
+  // chunk per growth, through the driver's virtual memory calls.
+  size_t span = 0;
+  int device = 0;                                             // of a mapped buffer
+  std::vector<std::pair<unsigned long long, size_t>> chunks;  // physical handle, bytes
   int ensure(size_t want, bool exact = false);  // exact: no geometric headroom
   void free();
   // Hands the buffer to the process-wide device cache instead of the pool.
@@ -127,9 +133,11 @@ struct Graph {
   bool hash_quotient = false;
   uint32_t hash_load = 50;  // growth threshold, percent
   uint64_t learned_peak = 0;  // learned plan: predicted largest layer (pre-sizes the frontier buffers)
+  uint64_t memory_reserve = 2ull << 30;  // plan: device bytes left free for others
   uint32_t group_chunk = 4096;  // plan shape: parents per grouped work item
   int blocks_per_sm = 0;        // plan shape: resident layer-kernel blocks per SM, 0 = defaults
   uint32_t parents_per_thread = 0;  // plan shape: fused layers' states per thread, 0 = by generators
+  uint64_t route_chunk = 0;         // plan shape: parents per routed pass, 0 = by memory
   int want_blocks(int kernel_default) const { return blocks_per_sm ? blocks_per_sm : kernel_default; }
   QuotientSlots quotient_slots(uint64_t slots) const;
   Control* host_control = nullptr;
@@ -145,6 +153,11 @@ struct Graph {
   uint64_t shard_history_total = 0;
   int bucket_setup(uint64_t work, bool exact);
   int bucket_launch(const void* route, const void* accept, const ExpandParams& p, size_t smem);
+  int routed_setup(uint64_t count, uint64_t* cap, uint64_t* chunk);
+  int bucket_chunks(const void* route, const void* accept, const ExpandParams& p, size_t smem, uint64_t chunk,
+                    uint32_t* redo);
+  bool bucket_alloc_exact = false;  // memory-bounded routed layer: buckets grow without headroom
+  uint64_t bucket_work = 0;         // successors the current shard buckets were sized for
 
   // Grouped layers (claim, then route the winners): the frontier is kept in
   // per-group regions (states sharing their first group_prefix symbols) plus a

@@ -37,7 +37,7 @@ namespace mgbfs2 {
 
 constexpr uint32_t kGroupStage = 1024;  // staged winners per block (one pass of 256 x 4 parents)
 constexpr int kGroupBlocksPerSM = 8;    // resident blocks the shared-memory carveout is sized for
-constexpr uint32_t kMaxGroups = 1728;   // region tables: 13!/10! = 1716 groups at most
+constexpr uint32_t kMaxGroups = 24024;  // region tables: 14!/10! groups at most (S13: 1,716)
 constexpr uint32_t kGroupChunk = 4096;  // parents per work item unless the plan chooses another size
 constexpr uint32_t kMaxTranspGens = 32;  // adjacent-transposition generators of the incremental-rank path
 static_assert(kGroupStage >= kBlock * 4, "a pass stages up to kBlock * ppt winners, ppt <= 4");

@@ -93,7 +93,8 @@ class NativeGraph:
     def plan(self, *, visited="auto", dedup="auto", capacity=None, reserve_bytes=None, shards=None,
              planner="plain", bucket_margin=None, bucket_min_work=None, parent_skip=True, host_loop=False,
              full_rank=False, wide_slots=False, hash_load_percent=None, predicted_states=None,
-             predicted_peak=None, group_chunk=None, blocks_per_sm=None, parents_per_thread=None) -> dict:
+             predicted_peak=None, group_chunk=None, blocks_per_sm=None, parents_per_thread=None,
+             route_chunk=None) -> dict:
         """Plans the run (mgbfs2_plan).  planner="learned" needs
         `predicted_states` (and optionally `predicted_peak`), e.g. from
         planner.predict_graph."""
@@ -103,6 +104,7 @@ class NativeGraph:
         req.group_chunk = int(group_chunk or 0)
         req.blocks_per_sm = int(blocks_per_sm or 0)
         req.parents_per_thread = int(parents_per_thread or 0)
+        req.route_chunk = int(route_chunk or 0)
         req.options = ((0 if parent_skip else native.OPTION_NO_PARENT_SKIP) |
                        (native.OPTION_HOST_LOOP if host_loop else 0) | (native.OPTION_FULL_RANK if full_rank else 0) |
                        (native.OPTION_WIDE_SLOTS if wide_slots else 0))

@@ -52,7 +52,7 @@ class PlanRequest(C.Structure):
                 ("planner", C.c_uint32), ("bucket_margin", C.c_uint32), ("bucket_min_work", C.c_uint64),
                 ("options", C.c_uint32), ("hash_load_percent", C.c_uint32), ("predicted_states", C.c_uint64),
                 ("predicted_peak", C.c_uint64), ("group_chunk", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("parents_per_thread", C.c_uint32), ("reserved", C.c_uint32)]
+                ("parents_per_thread", C.c_uint32), ("route_chunk", C.c_uint32)]
 
 
 OPTION_NO_PARENT_SKIP = 1

@@ -102,14 +102,15 @@ def test_unpackable_matrices_stay_on_the_wide_path():
 
 
 @pytest.mark.parametrize("case", ["sl2_mod31", "sl2_mod101"])
-def test_routed_radix_layers_match_the_reference(case):
+@pytest.mark.parametrize("route_chunk", [None, 1024])
+def test_routed_radix_layers_match_the_reference(case, route_chunk):
     """Every layer routed by the top entry (m shards of the radix bitmap),
-    then claimed shard by shard."""
+    then claimed shard by shard; whole layers, or 1024 parents per pass."""
     from multigpubfs_b200 import GraphDefinition
     from multigpubfs_b200.engine import NativeGraph
     fx = golden("matrix_groups.json")["cases"][case]
     with NativeGraph(GraphDefinition.from_dict(fx["graph"])) as e:
-        info = e.plan(visited="bitmap", dedup="bucket", bucket_min_work=1)
+        info = e.plan(visited="bitmap", dedup="bucket", bucket_min_work=1, route_chunk=route_chunk)
         for _ in range(3):
             assert e.run().layer_sizes == fx["layers"]
     assert info["dedup"] == "bucket" and info["shards"] == int(case.split("mod")[1])

@@ -66,6 +66,12 @@ VARIANTS = {
     # hash with every layer routed to table regions, then inserted per region
     "hash_bucket": dict(visited="hash", dedup="bucket", bucket_min_work=1),
     "hash_bucket_tight": dict(visited="hash", dedup="bucket", bucket_min_work=1, bucket_margin=0),
+    # routed layers in parent chunks (as when a layer's buckets exceed the
+    # device memory), one chunk at a time; tight: chunks overflow and are redone
+    "bitmap_bucket_chunked": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, route_chunk=1 << 14),
+    "bitmap_bucket_chunked_tight": dict(visited="bitmap", dedup="bucket", bucket_min_work=1, bucket_margin=0,
+                                        route_chunk=1 << 10),
+    "hash_bucket_chunked": dict(visited="hash", dedup="bucket", bucket_min_work=1, route_chunk=1 << 12),
     # host-driven layer loop instead of the one-graph device loop
     "bitmap_atomic_hostloop": dict(visited="bitmap", dedup="atomic", host_loop=True),
     "hash_hostloop": dict(visited="hash", host_loop=True),
@@ -146,7 +152,8 @@ def test_parent_skip_accounting(lrx_layers):
                                      "bitmap_bucket_tight", "bitmap_bucket_noskip", "hash3_noskip", "bitmap_sort",
                                      "bitmap_sort_noskip", "hash_sort", "hash3_sort", "bitmap_grouped",
                                      "bitmap_grouped_tight", "bitmap_grouped_noskip", "hash_bucket",
-                                     "hash_bucket_tight"])
+                                     "hash_bucket_tight", "bitmap_bucket_chunked", "bitmap_bucket_chunked_tight",
+                                     "hash_bucket_chunked"])
 def test_lrx_small(lrx_layers, variant):
     redo = 0
     for n in range(3, 12):
@@ -154,7 +161,7 @@ def test_lrx_small(lrx_layers, variant):
         assert out is not None
         assert out[1].layer_sizes == lrx_layers[n], (n, variant)
         redo += out[1].redo_layers
-    if variant in ("bitmap_bucket_tight", "hash_bucket_tight"):
+    if variant in ("bitmap_bucket_tight", "hash_bucket_tight", "bitmap_bucket_chunked_tight"):
         assert redo > 0  # the exact redo path ran and changed nothing
 
 
@@ -354,3 +361,36 @@ def test_fused_blocks_per_sm_are_exact(blocks):
         with NativeGraph(GraphDefinition.permutation(G.coxeter_generators(10), list(range(10)))) as e:
             e.plan(blocks_per_sm=blocks, **plan)
             assert e.run().layer_sizes == G.coxeter_layers(10), plan
+
+
+def test_route_chunk_must_be_a_multiple_of_1024():
+    from multigpubfs_b200 import GraphDefinition
+    from multigpubfs_b200.native import NativeError
+    g = GraphDefinition.from_dict(G.permutation_graph(G.lrx_generators(8), list(range(8))))
+    with _engine()(g) as e:
+        with pytest.raises(NativeError) as exc:
+            e.plan(visited="bitmap", dedup="bucket", route_chunk=1000)
+        assert exc.value.code == 1
+        e.plan(visited="bitmap", dedup="bucket", bucket_min_work=1, route_chunk=2048)
+        assert e.run().layer_sizes == G.layer_sizes(G.permutation_graph(G.lrx_generators(8), list(range(8))))
+
+
+@pytest.mark.parametrize("dedup", ["grouped", "bucket"])
+def test_s14_lrx_first_layers_match_the_oracle(dedup):
+    """Degree 14, every layer from the first through the large-bitmap layers:
+    grouped with 4-symbol groups (24,024 regions of 10! bits), or owner-routed
+    in 65,536-parent chunks; the first 24 layers equal the oracle's."""
+    from multigpubfs_b200 import GraphDefinition
+    n = 14
+    gens = G.lrx_generators(n)
+    expect, _, _ = P.packed_bfs(gens, list(range(n)), use_bitmap=False, max_layers=24, partial=True,
+                                max_states=1 << 27)
+    g = GraphDefinition.from_dict(G.permutation_graph(gens, list(range(n))))
+    plan = dict(visited="bitmap", dedup=dedup, bucket_min_work=1)
+    if dedup == "bucket":
+        plan["route_chunk"] = 1 << 16
+    with _engine()(g) as e:
+        info = e.plan(**plan)
+        r = e.run(max_layers=24)
+    assert info["shards"] == (24024 if dedup == "grouped" else 182)
+    assert len(expect) == 24 and r.layer_sizes == expect
