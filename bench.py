@@ -10,6 +10,9 @@ Workloads (one step = one pass of the workload):
   from the identity: 13! = 6,227,020,800 states, 79 layers, 18,681,062,400
   successors, exact Lehmer-rank bitmap.  Every BFS's table is checked against
   the reference's shipped table.
+* ``s14-lrx``: the same graph on 14 symbols, 14! = 87,178,291,200 states in 92
+  layers (peak 4,595,217,203), on one GPU: grouped layers of 24,024 prefix
+  groups; checked by its total and the reference's first 24 layers.
 * ``s13-coxeter``: S13 under the adjacent transpositions s1..s12 (inverse-closed),
   checked against the Mahonian layer certificate.
 * ``s11-lrx-hash``: S11 LRX through the exact-key open-addressing hash of all
@@ -74,6 +77,9 @@ def coxeter(n):
 WORKLOADS = {
     "s13-lrx": dict(n=13, gens=lrx(13), visited="bitmap", dedup="grouped",
                     desc="S13 LRX full BFS (L, R, X from identity; 6,227,020,800 states), exact Lehmer-rank bitmap"),
+    "s14-lrx": dict(n=14, gens=lrx(14), visited="bitmap", dedup="auto",
+                    desc="S14 LRX full BFS (87,178,291,200 states, 4.6e9 in the peak layer), exact Lehmer-rank "
+                         "bitmap, grouped layers with 24,024 prefix groups and a memory-bounded spill"),
     "s13-coxeter": dict(n=13, gens=coxeter(13), visited="bitmap", dedup="grouped",
                         desc="S13 adjacent transpositions s1..s12 full BFS (6,227,020,800 states), exact bitmap"),
     "s11-lrx-hash": dict(n=11, gens=lrx(11), visited="hash", dedup="atomic",
@@ -91,7 +97,10 @@ BATCHED = ("sweep512", "planner-s12", "s13-lrx-sharded")
 # Bounded CPU samples (about 10-30 s of C-oracle work on a 16-core host): the
 # layers run of each workload's sample; s11-lrx-hash runs whole, and sweep512
 # runs its first 128 instances whole.
-CPU_SAMPLE_LAYERS = {"s13-lrx": 32, "s13-coxeter": 20, "planner-s12": 17}
+CPU_SAMPLE_LAYERS = {"s13-lrx": 32, "s13-coxeter": 20, "planner-s12": 17, "s14-lrx": 32}
+# Past 13 symbols the oracle's bitmap (n!/8 bytes of host memory) gives way to
+# its exact hash, sized for the sample.
+CPU_SAMPLE_HASH_STATES = {"s14-lrx": 1 << 27}
 
 
 def measured_peak():
@@ -252,9 +261,10 @@ def cpu_sample(name, threads=None):
     elif name in WORKLOADS:
         w = WORKLOADS[name]
         layers = CPU_SAMPLE_LAYERS.get(name)
-        bitmap = w["visited"] == "bitmap"
+        bitmap = w["visited"] == "bitmap" and name not in CPU_SAMPLE_HASH_STATES
         sizes, _, _ = P.packed_bfs(w["gens"], list(range(w["n"])), use_bitmap=bitmap, threads=threads,
-                                   max_layers=layers or (1 << 16), partial=bool(layers))
+                                   max_layers=layers or (1 << 16), partial=bool(layers),
+                                   max_states=CPU_SAMPLE_HASH_STATES.get(name))
         states, succ = sum(sizes), len(w["gens"]) * sum(sizes)
         what = (f"{name} layers 0-{len(sizes) - 1}" if layers else f"{name} full BFS") + \
                f" ({'Lehmer bitmap' if bitmap else 'exact hash set'})"
@@ -555,7 +565,14 @@ def bench_single(args, rank, world, local):
     dedup = args.dedup or w["dedup"]
     graph = workload_graph(args.workload)
     expect = expected_layers(args.workload, w.get("n"))
-    if expect is None:
+    if args.workload == "s14-lrx":
+        # No whole S14 table ships with the reference: 14! states in all, and
+        # the first 24 layers of the reference's own CPU search.
+        prefix = golden("lrx14_prefix.json")["layers"]
+
+        def table_ok(sizes):
+            return sum(sizes) == math.factorial(14) and sizes[:len(prefix)] == prefix
+    elif expect is None:
         # GL(2, p): the group order, and the oracle's first layers.
         p = w["matrix_p"]
         order = (p * p - 1) * (p * p - p)

@@ -394,3 +394,25 @@ def test_s14_lrx_first_layers_match_the_oracle(dedup):
         r = e.run(max_layers=24)
     assert info["shards"] == (24024 if dedup == "grouped" else 182)
     assert len(expect) == 24 and r.layer_sizes == expect
+
+
+def test_s14_lrx_full_bfs_on_one_gpu():
+    """The whole S14 LRX BFS (14! = 87,178,291,200 states, 4.6e9 in the peak
+    layer) under the default plan (grouped layers with 24,024 prefix groups and
+    a memory-bounded spill) and owner-routed in parent chunks sized by the free
+    memory: both settle 14! states, agree layer by layer, and start with the
+    reference's first 24 layers."""
+    from multigpubfs_b200 import GraphDefinition
+    n = 14
+    fx = golden("lrx14_prefix.json")
+    g = GraphDefinition.from_dict(G.permutation_graph(G.lrx_generators(n), list(range(n))))
+    tables = {}
+    for dedup in ("auto", "bucket"):
+        with _engine()(g) as e:
+            info = e.plan(visited="bitmap", dedup=dedup)
+            r = e.run()
+        tables[dedup] = (info["dedup"], r.layer_sizes)
+    assert tables["auto"][0] == "grouped" and tables["bucket"][0] == "bucket"
+    sizes = tables["auto"][1]
+    assert sum(sizes) == math.factorial(n) and sizes[:24] == fx["layers"]
+    assert tables["bucket"][1] == sizes

@@ -31,6 +31,16 @@ def test_c_oracle_lrx_matches_reference_packed_search(n, lrx_layers):
     assert sizes_hash == lrx_layers[n]
 
 
+def test_c_oracle_s14_prefix_matches_the_reference_search():
+    """The first 24 layers of S14 LRX: the oracle's partial search against
+    the reference's CPU search cancelled at the same depth."""
+    from tests.conftest import golden
+    fx = golden("lrx14_prefix.json")
+    sizes, _, _ = P.packed_bfs(G.lrx_generators(14), list(range(14)), use_bitmap=False, max_layers=24,
+                               partial=True, max_states=1 << 27)
+    assert sizes == fx["layers"] and fx["states"] == math.factorial(14)
+
+
 def test_c_oracle_s13_full_table(lrx13):
     # The whole 13! search takes ~10 minutes on 8 cores, so it runs only on
     # request; the GPU suite checks the engine against the same table.
