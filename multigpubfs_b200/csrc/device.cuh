@@ -547,6 +547,24 @@ __device__ __forceinline__ unsigned int atomic_or_hinted32(unsigned int* address
   return old;
 }
 
+// Generators from which the grouped layers' claims test before they set
+// (claim_bit32): with g generators about (g - 2) / (g - 1) of an inverse-
+// closed graph's tests find a visited state, and a work item's children fall
+// into a few 454 KB group slices, so the load often hits L1.  Measured on the
+// B200: S13 Coxeter (12 generators) 544 -> 414 ms, S13 LRX (3) 145 -> 150 ms.
+// The fused and batched layers scatter their claims over the whole bitmap;
+// there the load lost (S10 Coxeter 1.15 -> 1.39 ms, S12 planner instances
+// 2.41 -> 2.81 s), so they keep the plain atomic.
+constexpr uint32_t kTestFirstGens = 5;
+
+// Test, then set: a bit that a plain load sees set is set for good (a run
+// only ever sets bits, and a launch starts with no stale L1 lines), so only a
+// bit seen clear costs an L2 atomic.  True when this call set it.
+__device__ __forceinline__ bool claim_bit32(unsigned int* word, unsigned int bit, unsigned long long policy) {
+  if (*word & bit) return false;
+  return !(atomic_or_hinted32(word, bit, policy) & bit);
+}
+
 __device__ __forceinline__ unsigned long long atomic_or_hinted(unsigned long long* address, unsigned long long bits,
                                                                unsigned long long policy) {
   unsigned long long old;

@@ -1035,9 +1035,9 @@ void refresh_free_memory(int device) {
 
 }  // namespace
 
-int device_free_bytes(int device, size_t* free_bytes) {
+int device_free_bytes(int device, size_t* free_bytes, bool fresh) {
   const uint64_t reserved = pool_reserved_bytes(device);
-  {
+  if (!fresh) {
     std::lock_guard<std::mutex> hold(free_memory_lock);
     FreeMemory& e = free_memory[device];
     if (e.valid) {
@@ -1609,11 +1609,16 @@ int Graph::grouped_setup(uint64_t count, uint64_t prev_count, uint64_t cap, void
   constexpr uint64_t W = sizeof(unsigned long long);
   uint64_t spill = cap;
   if ((total + spill + 2) * W > next.bytes) {
-    // Growing `next` frees it first: its bytes count as free here.
-    size_t free_bytes = 0;
-    if ((rc = device_free_bytes(device, &free_bytes))) return rc;
-    const uint64_t avail = free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes;
-    const uint64_t room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
+    // Growing `next` frees it first: its bytes count as free here.  Before a
+    // memory-bounded layout the device is asked afresh.
+    uint64_t room = 0;
+    for (bool fresh : {false, true}) {
+      size_t free_bytes = 0;
+      if ((rc = device_free_bytes(device, &free_bytes, fresh))) return rc;
+      const uint64_t avail = free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes;
+      room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
+      if ((total + spill + 2) / 2 * 3 <= room) break;
+    }
     if ((total + spill + 2) / 2 * 3 <= room) {
       if ((rc = next.ensure((total + spill + 2) * W))) return rc;
     } else {
@@ -1815,12 +1820,15 @@ int Graph::routed_setup(uint64_t count, uint64_t* cap, uint64_t* chunk) {
   }
   const uint64_t need_next = *cap + 2, need_buckets = bucket_words(count);
   if (need_next * W <= next.bytes && need_buckets * W <= buckets.bytes) return MGBFS2_OK;
-  size_t free_bytes = 0;
-  if (int rc = device_free_bytes(device, &free_bytes)) return rc;
-  const uint64_t avail =
-      free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes + buckets.bytes;
-  const uint64_t room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
-  if (!bucket_alloc_exact && (need_next + need_buckets) / 2 * 3 <= room) return next.ensure(need_next * W);
+  uint64_t room = 0;
+  for (bool fresh : {false, true}) {
+    size_t free_bytes = 0;
+    if (int rc = device_free_bytes(device, &free_bytes, fresh)) return rc;
+    const uint64_t avail =
+        free_bytes + pool_idle_bytes(device) + device_cache_bytes(device) + next.bytes + buckets.bytes;
+    room = avail > memory_reserve ? (avail - memory_reserve) / W : 0;
+    if (!bucket_alloc_exact && (need_next + need_buckets) / 2 * 3 <= room) return next.ensure(need_next * W);
+  }
   bucket_alloc_exact = true;
   const uint64_t least = bucket_words(std::min<uint64_t>(count, kRouteChunkAlign));
   if (room < least + 2 + bucket_margin) return MGBFS2_OUT_OF_MEMORY;
@@ -2465,6 +2473,7 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         gp.next_count = meta + 5 * R + 1;
         gp.work = meta + 6 * R + 1;
         gp.chunk = group_chunk;
+        gp.test_first = gens >= kTestFirstGens ? 1u : 0u;
         gp.control = p.control;
         gp.transp = static_cast<const uint32_t*>(transp_buf.ptr);
         reinterpret_cast<GroupedFn>(group_fn)<<<group_grid, kBlock, group_smem,

@@ -60,8 +60,10 @@ int pinned_take(size_t bytes, void** out);
 void pinned_give(void* ptr);
 uint64_t pool_idle_bytes(int device);
 // Free device memory (cudaMemGetInfo), reused for up to two seconds per device and
-// corrected by the change in this process's pool reservation since.
-int device_free_bytes(int device, size_t* free_bytes);
+// corrected by the change in this process's pool reservation since; `fresh`
+// queries the device now (memory taken by others, e.g. another allocator of
+// the process, is seen only then).
+int device_free_bytes(int device, size_t* free_bytes, bool fresh = false);
 
 struct WideState;     // int64-key arena path (wide.cu)
 struct ExpandParams;  // packed_kernels.cuh

@@ -61,6 +61,10 @@ struct GroupedParams {
   unsigned long long* next_count;        // regions: winners reserved per region (may pass a group's cap)
   unsigned long long* work;              // work-item counter, zero at launch
   uint32_t chunk;                        // parents per work item
+  // Claims load the bitmap word first and skip the atomic when the bit is
+  // set (claim_bit32), from kTestFirstGens generators up; the incremental-
+  // rank path (adjacent transpositions) always tests first.
+  uint32_t test_first;
   Control* control;
   // Incremental-rank path (every generator swaps positions t-1 and t): per
   // generator t and the weights of digits t-1 and t in the group part and in
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
               const uint32_t bit = 1u << (inner & 31);
               unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
                                    (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
-              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+              won = claim_bit32(word, bit, l2_policy_evict_last());
             } else {
               raise_error(&p.control->error, ERR_RANK_RANGE);
             }
@@ -290,7 +294,8 @@ __global__ void __launch_bounds__(kBlock, TRANSP ? 5 : kGroupBlocksPerSM) expand
               const uint32_t bit = 1u << (inner & 31);
               unsigned int* word = reinterpret_cast<unsigned int*>(p.bitmap) +
                                    (static_cast<unsigned long long>(grp) * kGroupWords32 + (inner >> 5));
-              won = !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
+              won = p.test_first ? claim_bit32(word, bit, l2_policy_evict_last())
+                                 : !(atomic_or_hinted32(word, bit, l2_policy_evict_last()) & bit);
             } else {
               const uint64_t r = lehmer_rank4<N>(c);
               const unsigned long long bit = 1ull << (r & 63);

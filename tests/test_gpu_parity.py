@@ -396,22 +396,50 @@ def test_s14_lrx_first_layers_match_the_oracle(dedup):
     assert len(expect) == 24 and r.layer_sizes == expect
 
 
+_S14_CHILD = """
+import json, sys
+sys.path.insert(0, sys.argv[1])
+from multigpubfs_b200 import GraphDefinition
+from multigpubfs_b200.engine import NativeGraph
+n = 14
+left = [(i + 1) % n for i in range(n)]
+right = [(i - 1) % n for i in range(n)]
+x = list(range(n)); x[0], x[1] = 1, 0
+g = GraphDefinition.permutation([left, right, x], list(range(n)))
+out = {}
+for dedup in ("auto", "bucket"):
+    with NativeGraph(g, 0) as e:
+        info = e.plan(visited="bitmap", dedup=dedup)
+        r = e.run()
+    out[dedup] = [info["dedup"], r.layer_sizes]
+print(json.dumps(out))
+"""
+
+
 def test_s14_lrx_full_bfs_on_one_gpu():
     """The whole S14 LRX BFS (14! = 87,178,291,200 states, 4.6e9 in the peak
     layer) under the default plan (grouped layers with 24,024 prefix groups and
     a memory-bounded spill) and owner-routed in parent chunks sized by the free
     memory: both settle 14! states, agree layer by layer, and start with the
-    reference's first 24 layers."""
-    from multigpubfs_b200 import GraphDefinition
+    reference's first 24 layers.  It needs about 130 GB of the device, so it
+    runs in a fresh process, beside none of the earlier tests' buffers."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    import torch
+    from multigpubfs_b200 import native
     n = 14
     fx = golden("lrx14_prefix.json")
-    g = GraphDefinition.from_dict(G.permutation_graph(G.lrx_generators(n), list(range(n))))
-    tables = {}
-    for dedup in ("auto", "bucket"):
-        with _engine()(g) as e:
-            info = e.plan(visited="bitmap", dedup=dedup)
-            r = e.run()
-        tables[dedup] = (info["dedup"], r.layer_sizes)
+    root = str(Path(__file__).resolve().parents[1])
+    # This process's cached buffers and tensors go back to the device first.
+    native.trim_memory(0)
+    torch.cuda.empty_cache()
+    free, total = torch.cuda.mem_get_info()
+    child = subprocess.run([sys.executable, "-c", _S14_CHILD, root], capture_output=True, text=True, timeout=600)
+    assert child.returncode == 0, f"free before: {free / 2**30:.1f} of {total / 2**30:.1f} GiB\n" + child.stderr[-2000:]
+    tables = json.loads(child.stdout.strip().splitlines()[-1])
     assert tables["auto"][0] == "grouped" and tables["bucket"][0] == "bucket"
     sizes = tables["auto"][1]
     assert sum(sizes) == math.factorial(n) and sizes[:24] == fx["layers"]
