@@ -658,15 +658,24 @@ void unmap_buffer(DeviceBuffer* b) {
   b->bytes = 0;
 }
 
+// The smallest cached buffer that holds `want` without holding more than
+// twice it (a larger one would keep memory the request does not use), else
+// the largest smaller one, to be grown.
 bool mapped_cache_take(int device, size_t want, DeviceBuffer* b) {
   std::lock_guard<std::mutex> hold(mapped_lock);
   std::vector<DeviceBuffer>& v = mapped_cache[device];
-  if (v.empty()) return false;
-  size_t pick = 0;
-  for (size_t i = 1; i < v.size(); ++i) {
-    const bool fits = v[i].bytes >= want, best_fits = v[pick].bytes >= want;
-    if (fits ? (!best_fits || v[i].bytes < v[pick].bytes) : (!best_fits && v[i].bytes > v[pick].bytes)) pick = i;
+  size_t pick = v.size();
+  for (size_t i = 0; i < v.size(); ++i) {
+    const size_t have = v[i].bytes;
+    if (have >= want && have / 2 > want) continue;
+    if (pick == v.size()) {
+      pick = i;
+      continue;
+    }
+    const bool fits = have >= want, best_fits = v[pick].bytes >= want;
+    if (fits ? (!best_fits || have < v[pick].bytes) : (!best_fits && have > v[pick].bytes)) pick = i;
   }
+  if (pick == v.size()) return false;
   b->ptr = v[pick].ptr;
   b->bytes = v[pick].bytes;
   b->span = v[pick].span;

@@ -408,6 +408,7 @@ x = list(range(n)); x[0], x[1] = 1, 0
 g = GraphDefinition.permutation([left, right, x], list(range(n)))
 out = {}
 for dedup in ("auto", "bucket"):
+    print("dedup", dedup, file=sys.stderr, flush=True)
     with NativeGraph(g, 0) as e:
         info = e.plan(visited="bitmap", dedup=dedup)
         r = e.run()
