@@ -61,7 +61,7 @@ enum { MGBFS2_VISITED_AUTO = 0, MGBFS2_VISITED_BITMAP = 1, MGBFS2_VISITED_HASH =
 /* SORT: per-tile radix sort + unique of the children before the visited test.
  * BUCKET: route successors to rank-range shard buckets, then claim per shard.
  * GROUPED: claim first, route only the winners into a frontier grouped by its
- * first N-10 symbols (Lehmer bitmaps of degree 11..13). */
+ * first N-10 symbols (Lehmer bitmaps of degree 11..14). */
 enum { MGBFS2_DEDUP_AUTO = 0, MGBFS2_DEDUP_ATOMIC = 1, MGBFS2_DEDUP_WARP = 2, MGBFS2_DEDUP_SORT = 3,
        MGBFS2_DEDUP_BUCKET = 4, MGBFS2_DEDUP_GROUPED = 5 };
 enum { MGBFS2_PLANNER_PLAIN = 0, MGBFS2_PLANNER_LEARNED = 1 };
@@ -245,9 +245,10 @@ MGBFS2_API int mgbfs2_table_probes(mgbfs2_graph* graph, double* mean_probes, uin
 MGBFS2_API const char* mgbfs2_status_string(int code);
 
 /* Destroying a handle keeps its device buffers in a per-device cache of the
- * library (and the stream-ordered pool keeps freed memory reserved), so the
- * next handle on the device allocates nothing.  This returns both to the
- * device: it frees the cached buffers and trims the pool.  Call it with no
+ * library (buffers from 1 GB stay mapped; the stream-ordered pool keeps freed
+ * smaller ones reserved), so the next handle on the device allocates nothing.
+ * This returns both to the device: it frees the cached buffers and trims the
+ * pool.  Call it with no
  * handle or batch of the device running.  No reference counterpart: the
  * reference runs each graph in a CLI process whose exit frees everything
  * (crates/mgbfs-cli/src/main.rs:191-200). */

@@ -55,6 +55,9 @@ def main(argv=None) -> int:
     ap.add_argument("--planner", default="plain", choices=["plain", "learned"])
     ap.add_argument("--capacity", type=int, default=None)
     ap.add_argument("--shards", type=int, default=None)
+    ap.add_argument("--route-chunk", type=int, default=None,
+                    help="routed (bucket) layers: parents per route-and-accept pass, a multiple of 1024 "
+                         "(default: the whole layer, or what the free memory holds)")
     ap.add_argument("--max-layers", type=int, default=None)
     ap.add_argument("--max-seconds", type=int, default=None)
     ap.add_argument("--repeat", type=int, default=1)
@@ -77,7 +80,7 @@ def main(argv=None) -> int:
         learned = choose_path(graph.to_dict(), device=a.device)
     with NativeGraph(graph, a.device) as engine:
         plan = engine.plan(visited=a.visited, dedup=a.dedup, capacity=a.capacity, shards=a.shards,
-                           host_loop=a.host_loop, **learned)
+                           host_loop=a.host_loop, route_chunk=a.route_chunk, **learned)
         if a.verb == "plan":
             print(json.dumps({"graph": graph.name, "digest": graph.digest(), "plan": plan}))
             return 0
