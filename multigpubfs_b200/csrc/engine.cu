@@ -658,16 +658,18 @@ void unmap_buffer(DeviceBuffer* b) {
   b->bytes = 0;
 }
 
-// The smallest cached buffer that holds `want` without holding more than
-// twice it (a larger one would keep memory the request does not use), else
-// the largest smaller one, to be grown.
-bool mapped_cache_take(int device, size_t want, DeviceBuffer* b) {
+// The smallest cached buffer that holds `want`, else the largest smaller
+// one, to be grown.  With `tight` (little free device memory) a buffer of
+// more than twice `want` is left in the cache: it would keep memory that the
+// request does not use, where other buffers of the run need it (a grouped
+// S14 BFS followed by a routed one in the same process).
+bool mapped_cache_take(int device, size_t want, DeviceBuffer* b, bool tight) {
   std::lock_guard<std::mutex> hold(mapped_lock);
   std::vector<DeviceBuffer>& v = mapped_cache[device];
   size_t pick = v.size();
   for (size_t i = 0; i < v.size(); ++i) {
     const size_t have = v[i].bytes;
-    if (have >= want && have / 2 > want) continue;
+    if (tight && have >= want && have / 2 > want) continue;
     if (pick == v.size()) {
       pick = i;
       continue;
@@ -736,7 +738,10 @@ static int grow_mapped(DeviceBuffer* b, int device, size_t want, bool exact) {
   const MappedApi& a = mapped_api(device);
   if (!b->span) {
     b->free();
-    if (!mapped_cache_take(device, want, b)) {
+    // Tight: under a quarter of the device free outside the caches.
+    size_t free_bytes = 0;
+    const bool tight = device_free_bytes(device, &free_bytes) == MGBFS2_OK && free_bytes < a.total / 4;
+    if (!mapped_cache_take(device, want, b, tight)) {
       const size_t span = round_up(std::max(want, a.total), a.granularity);
       CUdeviceptr va = 0;
       if (a.reserve(&va, span, 0, 0, 0) != CUDA_SUCCESS) return MGBFS2_OUT_OF_MEMORY;
