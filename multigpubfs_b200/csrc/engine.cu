@@ -2487,7 +2487,14 @@ int Graph::run(const mgbfs2_run_limits* limits, mgbfs2_layer_callback cb, void* 
         gp.next_count = meta + 5 * R + 1;
         gp.work = meta + 6 * R + 1;
         gp.chunk = group_chunk;
-        gp.test_first = gens >= kTestFirstGens ? 1u : 0u;
+        // Test first where most tests will find a visited state: many
+        // generators, or a layer whose parents won under 40 % of their tests
+        // (LRX past its peak layer).
+        {
+          const uint64_t tested = depth ? layer_sizes[depth - 1] * (parent_skip && depth > 1 ? gens - 1 : gens) : 0;
+          const bool lean = tested && static_cast<double>(count) < 0.4 * static_cast<double>(tested);
+          gp.test_first = gens >= kTestFirstGens || lean ? 1u : 0u;
+        }
         gp.control = p.control;
         gp.transp = static_cast<const uint32_t*>(transp_buf.ptr);
         reinterpret_cast<GroupedFn>(group_fn)<<<group_grid, kBlock, group_smem,
