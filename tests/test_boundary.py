@@ -318,3 +318,41 @@ def test_no_cpu_fallback_without_device(tmp_path):
     g = GraphDefinition.permutation([[1, 2, 0]], [0, 1, 2])
     with pytest.raises(native.NativeUnavailable):
         run_graph(g, tmp_path / "out")
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Every ctypes structure of multigpubfs_b200.native has the size and the
+    field offsets of its struct in include/mgbfs2.h, as gcc lays it out (a
+    field renamed or moved in one and not the other fails here, on CPU)."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    from pathlib import Path
+
+    from multigpubfs_b200 import native
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    pairs = {"mgbfs2_graph_desc": native.GraphDesc, "mgbfs2_plan_request": native.PlanRequest,
+             "mgbfs2_plan_info": native.PlanInfo, "mgbfs2_run_limits": native.RunLimits,
+             "mgbfs2_status": native.RunStatus, "mgbfs2_batch_options": native.BatchOptions,
+             "mgbfs2_batch_status": native.BatchStatus}
+    root = Path(__file__).resolve().parents[1]
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "mgbfs2.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(root / "include"), str(src), "-o", str(exe)], check=True,
+                   capture_output=True, text=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, field, value = line.split()
+        got[(cname, field)] = int(value)
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
