@@ -445,3 +445,28 @@ def test_s14_lrx_full_bfs_on_one_gpu():
     sizes = tables["auto"][1]
     assert sum(sizes) == math.factorial(n) and sizes[:24] == fx["layers"]
     assert tables["bucket"][1] == sizes
+
+
+def test_routed_layers_under_a_memory_budget_keep_the_table():
+    """S12 Coxeter (11 generators, the certified Mahonian table) routed on a
+    device budget of 1.2 GB: its peak layer's buckets alone would need about
+    2.6 GB. Its routed layers therefore go in parent chunks sized by the free
+    memory. That takes more route/accept launches than the same BFS
+    unbounded, and gives the certified table."""
+    import torch
+    from multigpubfs_b200 import GraphDefinition, native
+    n = 12
+    g = GraphDefinition.from_dict(G.permutation_graph(G.coxeter_generators(n), list(range(n))))
+    expect = G.coxeter_layers(n)
+    native.trim_memory(0)
+    torch.cuda.empty_cache()
+    with _engine()(g) as e:
+        e.plan(visited="bitmap", dedup="bucket")
+        free = e.run()
+    native.trim_memory(0)
+    free_bytes, _ = torch.cuda.mem_get_info()
+    with _engine()(g) as e:
+        e.plan(visited="bitmap", dedup="bucket", reserve_bytes=free_bytes - (1200 << 20))
+        bounded = e.run()
+    assert free.layer_sizes == expect and bounded.layer_sizes == expect
+    assert bounded.kernel_launches > free.kernel_launches
