@@ -1817,9 +1817,9 @@ int Graph::bucket_launch(const void* route_fn, const void* accept_fn, const Expa
 // every layer: the next frontier takes up to `*cap` (lowered to what the
 // memory holds: a layer larger than that ends the run with
 // ERR_FRONTIER_OVERFLOW), the buckets what is left, and a layer whose buckets
-// do not fit them is routed in parent chunks of `*chunk`.  S14 under LRX needs
-// this: its 4.6e9-state layer has 13.8e9 successors, 110 GB of buckets, on a
-// 180 GB GPU.
+// do not fit them is routed in parent chunks of `*chunk`.  S14 under LRX with
+// routed layers needs this: its 4.6e9-state layer has 13.8e9 successors, 110
+// GB of buckets, on a 180 GB GPU.
 int Graph::routed_setup(uint64_t count, uint64_t* cap, uint64_t* chunk) {
   const uint64_t margin = static_cast<uint64_t>(bucket_shards) * bucket_margin;
   const double per_parent = static_cast<double>(gens) * (shard_history_total ? 1.2 : 2.0);
