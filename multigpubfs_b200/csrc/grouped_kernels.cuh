@@ -62,7 +62,8 @@ struct GroupedParams {
   unsigned long long* work;              // work-item counter, zero at launch
   uint32_t chunk;                        // parents per work item
   // Claims load the bitmap word first and skip the atomic when the bit is
-  // set (claim_bit32), from kTestFirstGens generators up; the incremental-
+  // set (claim_bit32).  The host sets it from kTestFirstGens generators up and
+  // in layers whose parents won under 40 % of their tests; the incremental-
   // rank path (adjacent transpositions) always tests first.
   uint32_t test_first;
   Control* control;
